@@ -1,0 +1,340 @@
+#!/usr/bin/env python3
+"""Headline benchmark of the CKKS evaluation core on B200.
+
+Metric: relinearised homomorphic multiplies + rescales per second at
+N = 2^12, L = 3 45-bit RNS primes + 1 special prime (hybrid keyswitch,
+dnum = 3), 256 ciphertext pairs per step (the ct-mult workload the
+reference's metric is quoted on).  A step is one call of the batched
+ct-mult + relin + rescale over 256 pairs resident in HBM; four distinct input
+batches rotate between steps (400 MB > the 126 MB L2).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank processes its own 256 pairs (weak scaling, no
+data-path collective); the step time is the max over ranks.
+`--impl reference` times the CPU restatement of the same path on all host
+cores (the reference project has no CPU or GPU implementation of the RNS path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT / "cipher-pu_b200"))
+
+METRIC = "ct-mult+relin+rescale/s @N=2^12 L=3"
+UNIT = "ct-mult/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=30)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--log-n", type=int, default=12)
+    ap.add_argument("--levels", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config(a) -> dict:
+    return {"workload": f"ct-mult+relin+rescale, N=2^{a.log_n}, L={a.levels} x 45-bit + 1 special "
+                        f"prime, dnum={a.levels}, {a.batch} ciphertext pairs per step per GPU",
+            "log_n": a.log_n, "levels": a.levels, "special_primes": 1, "dnum": a.levels,
+            "batch_per_gpu": a.batch, "global_batch": a.batch * max(1, a.gpus),
+            "l2": "inputs larger than L2: 4 distinct input batches rotate between steps",
+            "parallelism": f"replicas x{max(1, a.gpus)} (ciphertext batch sharded, no collective)"}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ------------------------------------------------------------------ reference arm
+def run_reference(a) -> int:
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    from oracle import cpu_baseline
+    steps, warm = a.steps, a.warmup
+    per_step = max(1.0, min(6.0, 150.0 / max(1, steps + warm)))
+    total_done, total_wall = 0, 0.0
+    with cpu_baseline.CpuPool(a.log_n, a.levels) as pool:
+        for i in range(warm + steps):
+            done, wall = pool.step(per_step)
+            if i >= warm:
+                total_done += done
+                total_wall += wall
+        cores = pool.cores
+        sample = pool.sample(total_done, per_step)
+    v = total_done / total_wall
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": a.gpus,
+            "steps": steps, "warmup": warm, "ms_per_step": 1000.0 * a.batch / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic uniform residues", "config": config(a),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    def __init__(self, gpu_index: int):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        self.gpu = gpu_index
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu),
+                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            rows = []
+        sm = []
+        smax = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                smax = float(r[2])
+            except Exception:
+                continue
+            for nm, val in zip(names, r[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ ours
+def stage_bytes(stage: int, n: int, level: int) -> int:
+    """Algorithmic HBM bytes per CTA-unit of each ct-mult kernel, times units per ciphertext.
+    Returned per ciphertext pair."""
+    w = 8 * n
+    if stage == 0:   # tensor: read a0,a1,b0,b1 ; write d0,d1,d2(eval),d2(coef) -- per limb
+        return level * 8 * w
+    if stage == 1:   # modup: per target prime: read `level` digits, 2 key rows of (value, shoup)
+        # per digit, write 2 accumulators
+        return (level + 1) * (level * w + level * 2 * 2 * w + 2 * w)
+    # down: per poly k: read accp, d_t, acc_t, then per limb i<t: d_i, acc_i ; write t limbs
+    t = level - 1
+    return 2 * (3 * w + t * 2 * w + t * w)
+
+
+def run_ours(a) -> int:
+    import torch
+    ws, rank, local = dist_env()
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    import ckks_b200.ops as ops
+    from ckks_b200 import _lib
+    from ckks_b200.context import Context
+    from ckks_b200.params import CkksParams
+    import ctypes as C
+
+    P = CkksParams.standard(a.log_n, a.levels)
+    ctx = Context.get(a.log_n, P.primes, n_special=1)
+    n, L, B = P.n, a.levels, a.batch
+    g = torch.Generator(device=dev)
+    g.manual_seed(1234 + rank)
+
+    def rnd(shape, basis):
+        x = torch.empty(shape, dtype=torch.int64, device=dev)
+        for i, q in enumerate(basis):
+            x[..., i, :] = torch.randint(0, q, x[..., i, :].shape, generator=g, device=dev,
+                                         dtype=torch.int64)
+        return x.view(torch.uint64)
+
+    NB = 4
+    cts = [(rnd((B, 2, L, n), P.q), rnd((B, 2, L, n), P.q)) for _ in range(NB)]
+    ksk = rnd((L, 2, L + 1, n), list(P.q) + [P.special]).contiguous()
+    key = ops.relin_key_prepare(ctx, ksk)
+    scratch = torch.empty((ops.ct_mul_scratch_bytes(ctx, B, L) + 7) // 8, dtype=torch.uint64, device=dev)
+    out = torch.empty((B, 2, L - 1, n), dtype=torch.uint64, device=dev)
+
+    def step(i):
+        x, y = cts[i % NB]
+        ops.ct_mul_relin_rescale(ctx, x, y, key, scratch=scratch, out=out)
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if ws == 1:
+            return v
+        import torch.distributed as dist
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for i in range(a.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    lib = _lib.load()
+    lib.ckks_profile_reset()
+    lib.ckks_profile_enable(1)
+    barrier()
+    torch.cuda.synchronize()
+    with Clocks(local if ws > 1 else 0) as clk:
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(a.steps):
+            step(i)
+        e1.record()
+        torch.cuda.synchronize()
+    barrier()
+    lib.ckks_profile_enable(0)
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = ws * B * a.steps / (ms / 1000.0)
+    stages = []
+    for s in range(3):
+        tot = C.c_double()
+        cnt = C.c_longlong()
+        lib.ckks_profile_read(s, C.byref(tot), C.byref(cnt))
+        stages.append((tot.value, cnt.value))
+    clocks = clk.summary()
+
+    # ---------------- end to end: pinned host buffers, H2D + call + D2H each step
+    ha = cts[0][0].cpu().pin_memory()
+    hb = cts[0][1].cpu().pin_memory()
+    hout = torch.empty(out.shape, dtype=torch.uint64).pin_memory()
+    da = torch.empty_like(cts[0][0])
+    db = torch.empty_like(cts[0][1])
+    for _ in range(2):
+        da.copy_(ha, non_blocking=True)
+        db.copy_(hb, non_blocking=True)
+        ops.ct_mul_relin_rescale(ctx, da, db, key, scratch=scratch, out=out)
+        hout.copy_(out, non_blocking=True)
+    torch.cuda.synchronize()
+    barrier()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2_steps = max(3, a.steps // 2)
+    e2.record()
+    for _ in range(e2_steps):
+        da.copy_(ha, non_blocking=True)
+        db.copy_(hb, non_blocking=True)
+        ops.ct_mul_relin_rescale(ctx, da, db, key, scratch=scratch, out=out)
+        hout.copy_(out, non_blocking=True)
+    e3.record()
+    torch.cuda.synchronize()
+    barrier()
+    ms_e2e = max_over_ranks(e2.elapsed_time(e3))
+    e2e_value = ws * B * e2_steps / (ms_e2e / 1000.0)
+
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(ROOT / "MEASURED_PEAKS.json"))
+        except Exception:
+            pass
+        hbm = peaks.get("hbm_gbs")
+        peak_src = "measured" if hbm else "fallback"
+        hbm = hbm or 6650.0
+        dom = max(range(3), key=lambda s: stages[s][0])
+        names = ["k_cm_tensor", "k_cm_modup", "k_cm_down"]
+        per_launch_ms = stages[dom][0] / max(1, stages[dom][1])
+        alg = stage_bytes(dom, n, L) * B
+        achieved = alg / (per_launch_ms / 1000.0) / 1e9
+        traffic = None
+        try:
+            tr = json.load(open(ROOT / "profiles" / "ncu_traffic.json"))
+            rec = tr.get(names[dom])
+            if rec:
+                traffic = rec["bytes_per_pair"] * B
+        except Exception:
+            pass
+        tot_ms = sum(s[0] for s in stages)
+        cpu = None
+        if ws == 1 and not a.no_cpu_baseline:
+            from oracle import cpu_baseline
+            info = cpu_baseline.measure(a.log_n, a.levels, seconds=a.cpu_seconds)
+            cpu = {"value": info["value"], "unit": UNIT, "cores": info["cores"], "kind": "port",
+                   "sample": info["sample"]}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: uniform residues mod each prime (fresh-ciphertext distribution), random key",
+            "config": config(a),
+            "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm,
+                         "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
+                         "peak_source": f"{peak_src} hbm_gbs",
+                         "algorithmic_bytes_per_launch": alg,
+                         "avg_launch_ms": per_launch_ms},
+            "stage_ms_per_step": {names[s]: stages[s][0] / max(1, a.steps) for s in range(3)},
+            "stage_share": {names[s]: (stages[s][0] / tot_ms if tot_ms else None) for s in range(3)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT,
+                    "h2d_bytes_per_step": int(ha.numel() * 8 + hb.numel() * 8),
+                    "d2h_bytes_per_step": int(hout.numel() * 8)},
+            "gpu_launches": 3 * a.steps,
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main() -> int:
+    a = parse()
+    ws, _, _ = dist_env()
+    if ws > 1:
+        a.gpus = ws
+    if a.impl == "reference":
+        return run_reference(a)
+    return run_ours(a)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

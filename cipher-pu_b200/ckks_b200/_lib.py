@@ -1,0 +1,87 @@
+"""ctypes binding of libckks_b200.so (the C ABI declared in include/ckks_b200.h).
+
+The library is built in tree (``python cipher-pu_b200/build.py``).  Loading
+fails loudly when it is missing: there is no CPU fallback on the product path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libckks_b200.so"
+
+_u64p = C.c_void_p  # device pointers are passed as plain addresses
+_vp = C.c_void_p
+_i32 = C.c_int
+_i64 = C.c_int64
+_u64 = C.c_uint64
+_sz = C.c_size_t
+
+# name -> (restype, argtypes); must mirror include/ckks_b200.h
+SIGNATURES: dict[str, tuple] = {
+    "ckks_abi_version": (_i32, []),
+    "ckks_last_error": (C.c_char_p, []),
+    "ckks_ctx_create": (_i32, [_i32, _i32, _i32, C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64),
+                               C.POINTER(_vp)]),
+    "ckks_ctx_destroy": (_i32, [_vp]),
+    "ckks_ntt": (_i32, [_vp, _u64p, _i32, _i32, _i32, _i32, _i32, _vp]),
+    "ckks_bitrev_permute": (_i32, [_vp, _u64p, _u64p, _i32, _vp]),
+    "ckks_pointwise_mul": (_i32, [_vp, _u64p, _u64p, _u64p, _i32, _i32, _i32, _vp]),
+    "ckks_vec_addsub": (_i32, [_u64p, _u64p, _u64p, _i64, _u64, _i32, _vp]),
+    "ckks_poly_mul": (_i32, [_vp, _u64p, _u64p, _u64p, _i32, _i32, _i32, _i32, _vp]),
+    "ckks_poly_mul_anyq": (_i32, [_vp, _u64p, _u64p, _u64p, _i32, _u64, _i32, _vp]),
+    "ckks_relin_single": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _u64p, _u64p, _u64p, _i32, _i32,
+                                 _vp]),
+    "ckks_rescale_exact": (_i32, [_u64p, _u64p, _i64, _u64, _u64, _vp]),
+    "ckks_rescale_scaled": (_i32, [_u64p, _u64p, _i64, _u64, _u64, _i32, _vp]),
+    "ckks_rescale_rns": (_i32, [_vp, _u64p, _u64p, _i32, _i32, _vp]),
+    "ckks_relin_key_prepare": (_i32, [_vp, _u64p, _u64p, _vp]),
+    "ckks_ct_mul_scratch_bytes": (_sz, [_vp, _i32, _i32]),
+    "ckks_ct_mul_relin_rescale": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _i32, _i32, _vp, _sz,
+                                         _vp]),
+    "ckks_profile_enable": (_i32, [_i32]),
+    "ckks_profile_reset": (_i32, []),
+    "ckks_profile_read": (_i32, [_i32, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),
+}
+
+
+class CkksError(RuntimeError):
+    def __init__(self, fn: str, code: int, msg: str):
+        super().__init__(f"{fn} failed (status {code}): {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load the shared library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build it with `python cipher-pu_b200/build.py` "
+            "(the CKKS core has no CPU fallback)")
+    lib = C.CDLL(str(LIB_PATH), mode=os.RTLD_LOCAL if hasattr(os, "RTLD_LOCAL") else 0)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def call(name: str, *args) -> int:
+    lib = load()
+    rc = getattr(lib, name)(*args)
+    if rc != 0:
+        msg = lib.ckks_last_error().decode(errors="replace")
+        raise CkksError(name, rc, msg)
+    return rc
+
+
+def raw(name: str):
+    return getattr(load(), name)

@@ -1,0 +1,84 @@
+// common.cuh - shared types and exact 64-bit modular arithmetic for the
+// CKKS evaluation core (sm_100a).
+//
+// Moduli are NTT-friendly primes below 2^50 (the production chain is 45-bit).
+// Twiddle multiplications use Shoup's precomputed quotient
+// (w' = floor(w * 2^64 / q)), variable x variable products use Montgomery
+// multiplication with R = 2^64 followed by a Shoup multiply by (R mod q).
+// All lazy ranges stay below 4q < 2^52, far inside 64 bits.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+typedef unsigned long long u64;
+typedef long long i64;
+
+struct TwPair {
+  u64 w;   // twiddle
+  u64 ws;  // floor(w * 2^64 / q)
+};
+
+// Per-prime constants, one record per prime of a context.
+struct PrimeInfo {
+  u64 q, q2, q4;
+  u64 mont_qinv;  // -q^{-1} mod 2^64
+  u64 r_mod;      // 2^64 mod q
+  u64 r_mod_s;    // Shoup companion of r_mod
+  u64 one_s;      // floor(2^64 / q): Shoup companion of 1
+  u64 ninv;       // N^{-1} mod q
+  u64 ninv_s;
+  u64 half;       // (q - 1) / 2 : centred representative boundary
+  double qd;      // (double) q
+  double qinv_d;  // 1.0 / q
+};
+
+// ------------------------------------------------------------------ modular
+__device__ __forceinline__ u64 mulhi64(u64 a, u64 b) { return __umul64hi(a, b); }
+
+// Shoup multiply, lazy: any y < 2^64, w < q, ws = floor(w 2^64 / q) -> [0, 2q)
+__device__ __forceinline__ u64 shoup_lazy(u64 y, u64 w, u64 ws, u64 q) {
+  const u64 qt = mulhi64(y, ws);
+  return y * w - qt * q;
+}
+
+__device__ __forceinline__ u64 csub(u64 x, u64 m) { return x >= m ? x - m : x; }
+
+__device__ __forceinline__ u64 shoup(u64 y, u64 w, u64 ws, u64 q) {
+  return csub(shoup_lazy(y, w, ws, q), q);
+}
+
+// Montgomery product a*b*2^-64 mod q, lazy result in [0, 2q) when a*b < q*2^64.
+__device__ __forceinline__ u64 mont_lazy(u64 a, u64 b, u64 q, u64 qinv_neg) {
+  const u64 lo = a * b;
+  const u64 hi = mulhi64(a, b);
+  const u64 m = lo * qinv_neg;
+  const u64 mqh = mulhi64(m, q);
+  return hi + mqh + (lo != 0ull ? 1ull : 0ull);
+}
+
+// Exact a*b mod q for a, b < 2q (var x var) -> [0, q)
+__device__ __forceinline__ u64 mulmod(u64 a, u64 b, const PrimeInfo& P) {
+  const u64 t = mont_lazy(a, b, P.q, P.mont_qinv);      // a b R^-1, [0, 2q)
+  return shoup(t, P.r_mod, P.r_mod_s, P.q);              // * R  -> a b
+}
+
+__device__ __forceinline__ u64 addmod(u64 a, u64 b, u64 q) { return csub(a + b, q); }
+__device__ __forceinline__ u64 submod(u64 a, u64 b, u64 q) { return a >= b ? a - b : a + q - b; }
+
+// Reduce any x < 2^64 to [0, q) (Shoup multiply by 1).
+__device__ __forceinline__ u64 reduce_any(u64 x, const PrimeInfo& P) {
+  return csub(shoup_lazy(x, 1ull, P.one_s, P.q), P.q);
+}
+
+// Reduce [0, 4q) -> [0, q)
+__device__ __forceinline__ u64 reduce4(u64 x, u64 q, u64 q2) { return csub(csub(x, q2), q); }
+
+__device__ __forceinline__ TwPair ldtw(const TwPair* p) {
+  const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(p));
+  TwPair t;
+  t.w = v.x;
+  t.ws = v.y;
+  return t;
+}
+
+__device__ __forceinline__ PrimeInfo ldpi(const PrimeInfo* p) { return *p; }

@@ -1,0 +1,215 @@
+// ctx.cu - context creation (prime constants, twiddle tables) and the
+// thread-local error channel of the C ABI.
+#include <cstring>
+#include <mutex>
+
+#include "ctx.hpp"
+
+static thread_local std::string g_last_error;
+
+int ckks_set_error(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_last_error = buf;
+  return code;
+}
+
+int ckks_check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    return ckks_set_error(CKKS_ECUDA, "%s: %s", what, cudaGetErrorString(e));
+  return CKKS_OK;
+}
+
+extern "C" int ckks_abi_version(void) { return 1; }
+
+extern "C" const char* ckks_last_error(void) { return g_last_error.c_str(); }
+
+static int bitrev(int i, int bits) {
+  int r = 0;
+  for (int b = 0; b < bits; ++b) {
+    r = (r << 1) | (i & 1);
+    i >>= 1;
+  }
+  return r;
+}
+
+static bool is_prime_u64(u64 n) {
+  if (n < 2) return false;
+  static const u64 bases[] = {2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37};
+  for (u64 p : bases)
+    if (n % p == 0) return n == p;
+  u64 d = n - 1;
+  int s = 0;
+  while ((d & 1) == 0) {
+    d >>= 1;
+    ++s;
+  }
+  for (u64 a : bases) {
+    u64 x = h_powmod(a, d, n);
+    if (x == 1 || x == n - 1) continue;
+    bool comp = true;
+    for (int r = 1; r < s; ++r) {
+      x = h_mulmod(x, x, n);
+      if (x == n - 1) {
+        comp = false;
+        break;
+      }
+    }
+    if (comp) return false;
+  }
+  return true;
+}
+
+static void free_ctx(ckks_ctx* c) {
+  if (!c) return;
+  cudaFree(c->d_pi);
+  cudaFree(c->d_tw);
+  cudaFree(c->d_pinv);
+  cudaFree(c->d_qtinv);
+  delete c;
+}
+
+extern "C" int ckks_ctx_create(int log_n, int n_primes, int n_special, const uint64_t* primes,
+                               const uint64_t* psi, const uint64_t* omega, ckks_ctx** out) {
+  CKKS_REQUIRE(out != nullptr, "ckks_ctx_create: out is NULL");
+  *out = nullptr;
+  CKKS_REQUIRE(log_n >= 1 && log_n <= 14, "ckks_ctx_create: log_n=%d outside [1, 14]", log_n);
+  CKKS_REQUIRE(n_primes >= 1 && n_primes <= 64, "ckks_ctx_create: n_primes=%d outside [1, 64]",
+               n_primes);
+  CKKS_REQUIRE(n_special >= 0 && n_special <= 1 && n_special < n_primes,
+               "ckks_ctx_create: n_special=%d (must be 0 or 1 and < n_primes)", n_special);
+  CKKS_REQUIRE(primes != nullptr && psi != nullptr, "ckks_ctx_create: NULL primes/psi");
+  const int n = 1 << log_n;
+  ckks_ctx* c = new ckks_ctx();
+  c->log_n = log_n;
+  c->n = n;
+  c->n_primes = n_primes;
+  c->n_special = n_special;
+  c->n_q = n_primes - n_special;
+  cudaGetDevice(&c->device);
+  std::vector<TwPair> tw((size_t)n_primes * 4 * n);
+  for (int i = 0; i < n_primes; ++i) {
+    const u64 q = primes[i];
+    if (q < 3 || q >= (1ull << 50) || !is_prime_u64(q)) {
+      free_ctx(c);
+      return ckks_set_error(CKKS_EINVAL, "ckks_ctx_create: primes[%d]=%llu is not a prime in [3, 2^50)",
+                            i, (unsigned long long)q);
+    }
+    if ((q - 1) % (u64)n != 0) {
+      free_ctx(c);
+      return ckks_set_error(CKKS_EINVAL, "ckks_ctx_create: N=%d does not divide primes[%d]-1", n, i);
+    }
+    u64 ps = psi[i] % q;
+    bool nega = ps != 0;
+    if (nega) {
+      if (h_powmod(ps, (u64)n, q) != q - 1) {
+        free_ctx(c);
+        return ckks_set_error(CKKS_EINVAL, "ckks_ctx_create: psi[%d] is not a primitive 2N-th root", i);
+      }
+    }
+    u64 om = (omega && omega[i]) ? omega[i] % q : (nega ? h_mulmod(ps, ps, q) : 0);
+    if (om == 0 || h_powmod(om, (u64)n, q) != 1 || (n > 1 && h_powmod(om, (u64)n / 2, q) == 1)) {
+      free_ctx(c);
+      return ckks_set_error(CKKS_EINVAL, "ckks_ctx_create: omega[%d] is not a primitive N-th root", i);
+    }
+    c->primes.push_back(q);
+    c->psi.push_back(ps);
+    c->omega.push_back(om);
+    c->has_nega.push_back(nega ? 1 : 0);
+    PrimeInfo P;
+    std::memset(&P, 0, sizeof(P));
+    P.q = q;
+    P.q2 = 2 * q;
+    P.q4 = 4 * q;
+    u64 inv = 1;  // q^{-1} mod 2^64 by Newton
+    for (int k = 0; k < 7; ++k) inv *= 2 - q * inv;
+    P.mont_qinv = (u64)0 - inv;
+    P.r_mod = (u64)(((unsigned __int128)1 << 64) % q);
+    P.r_mod_s = h_shoup(P.r_mod, q);
+    P.one_s = h_shoup(1, q);
+    P.ninv = h_invmod((u64)n % q, q);
+    P.ninv_s = h_shoup(P.ninv, q);
+    P.half = (q - 1) / 2;
+    P.qd = (double)q;
+    P.qinv_d = 1.0 / (double)q;
+    c->h_pi.push_back(P);
+    TwPair* t = tw.data() + (size_t)i * 4 * n;
+    TwPair zero;
+    zero.w = 0;
+    zero.ws = 0;
+    for (int k = 0; k < 4 * n; ++k) t[k] = zero;
+    if (nega) {
+      const u64 pinv = h_invmod(ps, q);
+      for (int k = 1; k < n; ++k) {
+        const int e = bitrev(k, log_n);
+        t[TW_FWD * n + k] = h_twp(h_powmod(ps, e, q), q);
+        t[TW_INV * n + k] = h_twp(h_powmod(pinv, e, q), q);
+      }
+    }
+    const u64 oinv = h_invmod(om, q);
+    for (int m = 1; m < n; m <<= 1)
+      for (int ii = 0; ii < m; ++ii) {
+        const int e = (bitrev(m + ii, log_n) - n / (2 * m)) / 2;
+        t[TW_FWD_CYC * n + m + ii] = h_twp(h_powmod(om, e, q), q);
+        t[TW_INV_CYC * n + m + ii] = h_twp(h_powmod(oinv, e, q), q);
+      }
+  }
+  // keyswitch / rescale constants
+  const int nq = c->n_q;
+  std::vector<TwPair> pinv(nq), qtinv((size_t)nq * nq);
+  c->h_pinv.assign(nq, 0);
+  c->h_qtinv.assign(nq, std::vector<u64>(nq, 0));
+  for (int i = 0; i < nq; ++i) {
+    TwPair z;
+    z.w = 0;
+    z.ws = 0;
+    pinv[i] = z;
+    if (n_special) {
+      const u64 p = c->primes[nq];
+      const u64 v = h_invmod(p % c->primes[i], c->primes[i]);
+      pinv[i] = h_twp(v, c->primes[i]);
+      c->h_pinv[i] = v;
+    }
+  }
+  for (int t = 0; t < nq; ++t)
+    for (int i = 0; i < nq; ++i) {
+      TwPair z;
+      z.w = 0;
+      z.ws = 0;
+      qtinv[(size_t)t * nq + i] = z;
+      if (i < t && c->primes[t] % c->primes[i] != 0) {
+        const u64 v = h_invmod(c->primes[t] % c->primes[i], c->primes[i]);
+        qtinv[(size_t)t * nq + i] = h_twp(v, c->primes[i]);
+        c->h_qtinv[t][i] = v;
+      }
+    }
+  cudaError_t e = cudaSuccess;
+  e = cudaMalloc(&c->d_pi, sizeof(PrimeInfo) * n_primes);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_tw, sizeof(TwPair) * tw.size());
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_pinv, sizeof(TwPair) * nq);
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_qtinv, sizeof(TwPair) * (size_t)nq * nq);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c->d_pi, c->h_pi.data(), sizeof(PrimeInfo) * n_primes, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c->d_tw, tw.data(), sizeof(TwPair) * tw.size(), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c->d_pinv, pinv.data(), sizeof(TwPair) * nq, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(c->d_qtinv, qtinv.data(), sizeof(TwPair) * (size_t)nq * nq,
+                   cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    free_ctx(c);
+    return ckks_set_error(CKKS_ECUDA, "ckks_ctx_create: %s", cudaGetErrorString(e));
+  }
+  *out = c;
+  return CKKS_OK;
+}
+
+extern "C" int ckks_ctx_destroy(ckks_ctx* ctx) {
+  free_ctx(ctx);
+  return CKKS_OK;
+}

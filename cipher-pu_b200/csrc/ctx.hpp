@@ -1,0 +1,69 @@
+// ctx.hpp - host-side context of the CKKS evaluation core: the prime basis of
+// one ring dimension with its device-resident twiddle tables and constants.
+#pragma once
+#include <cstdarg>
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/ckks_b200.h"
+#include "common.cuh"
+
+struct ckks_ctx {
+  int log_n = 0;
+  int n = 0;
+  int n_primes = 0;
+  int n_special = 0;  // trailing special primes (0 or 1)
+  int n_q = 0;        // n_primes - n_special
+  int device = 0;
+  std::vector<u64> primes, psi, omega;
+  std::vector<int> has_nega;
+  std::vector<PrimeInfo> h_pi;
+  PrimeInfo* d_pi = nullptr;  // [n_primes]
+  TwPair* d_tw = nullptr;     // [n_primes][4][n]: fwd, inv, fwd cyclic, inv cyclic
+  TwPair* d_pinv = nullptr;   // [n_q]: special^-1 mod q_i (zeros when n_special == 0)
+  TwPair* d_qtinv = nullptr;  // [n_q][n_q]: q_t^-1 mod q_i at [t][i], i < t
+  TwPair* d_misc = nullptr;   // [n_primes][4]: (1, one_s) helpers; slot 1: R mod q
+  std::vector<std::vector<u64>> h_qtinv;  // host copies
+  std::vector<u64> h_pinv;
+
+  const TwPair* tw(int prime, int which) const {
+    return d_tw + ((size_t)prime * 4 + which) * (size_t)n;
+  }
+};
+
+enum { TW_FWD = 0, TW_INV = 1, TW_FWD_CYC = 2, TW_INV_CYC = 3 };
+
+// ---------------------------------------------------------------- errors
+int ckks_set_error(int code, const char* fmt, ...);
+int ckks_check_launch(const char* what);
+
+#define CKKS_REQUIRE(cond, ...)                                  \
+  do {                                                           \
+    if (!(cond)) return ckks_set_error(CKKS_EINVAL, __VA_ARGS__); \
+  } while (0)
+
+// ---------------------------------------------------------------- host math
+static inline u64 h_mulmod(u64 a, u64 b, u64 q) {
+  return (u64)(((unsigned __int128)a * b) % q);
+}
+static inline u64 h_powmod(u64 b, u64 e, u64 q) {
+  u64 r = 1 % q;
+  b %= q;
+  while (e) {
+    if (e & 1) r = h_mulmod(r, b, q);
+    b = h_mulmod(b, b, q);
+    e >>= 1;
+  }
+  return r;
+}
+static inline u64 h_invmod(u64 a, u64 q) { return h_powmod(a % q, q - 2, q); }  // q prime
+static inline u64 h_shoup(u64 w, u64 q) { return (u64)(((unsigned __int128)w << 64) / q); }
+static inline TwPair h_twp(u64 w, u64 q) {
+  TwPair t;
+  t.w = w % q;
+  t.ws = h_shoup(t.w, q);
+  return t;
+}
+
+static inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }

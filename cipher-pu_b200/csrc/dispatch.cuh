@@ -1,0 +1,47 @@
+// dispatch.cuh - compile-time dispatch over the ring dimension and launch
+// helpers shared by the kernel files.
+#pragma once
+#include "ctx.hpp"
+#include "ntt.cuh"
+
+// K (log2 coefficients per thread) used for a given log N.
+template <int LOGN>
+struct DefaultK {
+  static constexpr int value = LOGN < 4 ? LOGN : 4;
+};
+
+// Calls F.template operator()<LOGN, K>() for the runtime log_n.
+template <typename F>
+static int dispatch_logn(int log_n, F&& f) {
+  switch (log_n) {
+#define CKKS_CASE(L) \
+  case L:            \
+    return f.template operator()<L, DefaultK<L>::value>();
+    CKKS_CASE(1)
+    CKKS_CASE(2)
+    CKKS_CASE(3)
+    CKKS_CASE(4)
+    CKKS_CASE(5)
+    CKKS_CASE(6)
+    CKKS_CASE(7)
+    CKKS_CASE(8)
+    CKKS_CASE(9)
+    CKKS_CASE(10)
+    CKKS_CASE(11)
+    CKKS_CASE(12)
+    CKKS_CASE(13)
+    CKKS_CASE(14)
+#undef CKKS_CASE
+    default:
+      return ckks_set_error(CKKS_EUNSUPPORTED, "log_n=%d unsupported", log_n);
+  }
+}
+
+// Opt a kernel into > 48 KB of dynamic shared memory once per process/device.
+template <typename KernelT>
+static cudaError_t ensure_smem(KernelT kernel, int bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+static inline unsigned grid1d(long long blocks) { return (unsigned)blocks; }

@@ -1,0 +1,28 @@
+// profile.hpp - stage ids and the RAII span used by instrumented launches.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "ctx.hpp"
+
+enum {
+  CKKS_STAGE_CM_TENSOR = 0,  // ct-mult: tensor product + d2 INTT
+  CKKS_STAGE_CM_MODUP = 1,   // ct-mult: ModUp NTTs + key inner product
+  CKKS_STAGE_CM_DOWN = 2,    // ct-mult: ModDown + rescale
+  CKKS_STAGE_NTT = 3,        // standalone batched NTT
+  CKKS_STAGE_OTHER = 4,
+  CKKS_PROFILE_STAGES = 8
+};
+
+bool prof_on();
+
+class ProfSpan {
+ public:
+  ProfSpan(int stage, cudaStream_t s);
+  ~ProfSpan();
+
+ private:
+  int stage_;
+  cudaStream_t s_;
+  cudaEvent_t a_ = nullptr, b_ = nullptr;
+  bool active_ = false;
+};

@@ -1,0 +1,212 @@
+"""Generate golden vectors by running the reference's own Python functions.
+
+Run in a container that has the reference checkout (read-only) at
+REFERENCE_ROOT (default /root/reference):
+
+    python tests/golden/make_golden.py
+
+It imports the reference's golden-model functions by path (never copying
+their source), runs them on seeded inputs and writes the inputs/outputs to
+tests/golden/*.npz / *.json.  The committed outputs are what the tests compare
+the oracle and the GPU path against; the reference itself is not needed at
+test time.  tb/ref/gen_ntt_reference.py executes file-writing code at import,
+so it is executed in a temporary copy of its directory and its .mem outputs
+are read back.
+"""
+from __future__ import annotations
+
+import hashlib
+import importlib.util
+import json
+import os
+import random
+import shutil
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+REF = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
+OUT = Path(__file__).resolve().parent
+
+
+def load(relpath: str, name: str):
+    spec = importlib.util.spec_from_file_location(name, REF / relpath)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def sha(vals) -> str:
+    h = hashlib.sha256()
+    for v in vals:
+        h.update(int(v).to_bytes(16, "little", signed=True))
+    return h.hexdigest()
+
+
+def read_hex(relpath: str) -> list[int]:
+    with open(REF / relpath) as f:
+        return [int(l, 16) for l in f if l.strip()]
+
+
+def main() -> int:
+    arrays: dict[str, np.ndarray] = {}
+    meta: dict = {"reference": "YI-HAIBO/cipher-pu", "generator": "tests/golden/make_golden.py"}
+
+    # ---------------------------------------------------------------- 1 gen_ntt_reference (N=16, q=113)
+    with tempfile.TemporaryDirectory() as td:
+        tdir = Path(td) / "tbref"
+        tdir.mkdir()
+        shutil.copy(REF / "tb/ref/gen_ntt_reference.py", tdir / "gen_ntt_reference.py")
+        subprocess.run([sys.executable, "gen_ntt_reference.py"], cwd=tdir, check=True,
+                       capture_output=True)
+        ins, outs = [], []
+        for v in range(10):
+            ins.append([int(l) for l in open(tdir / "ref" / f"ntt_input_{v}.mem") if l.strip()])
+            outs.append([int(l) for l in open(tdir / "ref" / f"ntt_output_{v}.mem") if l.strip()])
+    arrays["toy_ntt_in"] = np.array(ins, dtype=np.uint64)
+    arrays["toy_ntt_out"] = np.array(outs, dtype=np.uint64)
+    meta["toy"] = {"N": 16, "q": 113, "omega": 40, "omega_inv": 65, "n_inv": 106,
+                   "source": "tb/ref/gen_ntt_reference.py:78 ntt (seeds 42+v)"}
+
+    # ---------------------------------------------------------------- 2 gen_omega_tables on q3 / N=4096
+    got = load("scripts/gen_omega_tables.py", "ref_got")
+    q3 = 17592186175489
+    tw = read_hex("rtl/m5/tw/tw_omega_q3_n4096.hex")
+    twi = read_hex("rtl/m5/tw/tw_omegainv_q3_n4096.hex")
+    omega = tw[1]
+    omega_inv = twi[1]
+    n = 4096
+    tab = got.generate_table(omega, q3, n)
+    assert tab == tw, "generate_table disagrees with committed hex"
+    rng = random.Random(0xC77)
+    a = [rng.randint(0, q3 - 1) for _ in range(n)]
+    ah = got._ntt_dit(a, omega, q3)
+    rec = got._intt_dif(ah, omega_inv, pow(n, -1, q3), q3)
+    assert rec == a
+    arrays["q3_ntt_in"] = np.array(a, dtype=np.uint64)
+    arrays["q3_ntt_out"] = np.array(ah, dtype=np.uint64)
+    meta["q3"] = {"q": q3, "N": n, "omega": omega, "omega_inv": omega_inv,
+                  "n_inv": pow(n, -1, q3), "tw_sha": sha(tw), "twinv_sha": sha(twi),
+                  "tw_len": len(tw), "source": "scripts/gen_omega_tables.py:96,154,188; rtl/m5/tw/tw_omega*_q3_n4096.hex"}
+    errs = got.verify(n, q3, omega, omega_inv, tab, got.generate_table(omega_inv, q3, n))
+    meta["q3"]["verify_errors"] = errs
+
+    # committed chain4 fixtures: constants + table digests
+    chain = json.load(open(REF / "rtl/m2/modulus_chain_chain4.json"))
+    meta["chain4"] = []
+    for i, rec in enumerate(chain):
+        t = read_hex(f"rtl/m2/omega_table_chain4_q{i}.hex")
+        ti = read_hex(f"rtl/m2/omega_inv_table_chain4_q{i}.hex")
+        meta["chain4"].append({k: rec[k] for k in ("q", "primitive_root", "omega", "omega_inv", "N", "N_INV")}
+                              | {"tw_sha": sha(t), "twinv_sha": sha(ti), "tw_len": len(t),
+                                 "tw_head": t[:4], "twinv_head": ti[:4]})
+    # RNS p1/p2/p3 tables (N=16, 4096): digests + head
+    meta["rns_tw"] = {}
+    for tag in ("p1", "p2", "p3", "q3", "toy"):
+        for nn in (8, 16, 4096, 16384):
+            for kind in ("omega", "omegainv"):
+                rel = f"rtl/m5/tw/tw_{kind}_{tag}_n{nn}.hex"
+                if (REF / rel).exists():
+                    t = read_hex(rel)
+                    meta["rns_tw"][f"{kind}_{tag}_n{nn}"] = {"sha": sha(t), "len": len(t), "head": t[:4]}
+
+    # ---------------------------------------------------------------- 3 gen_poly_mult_vectors_n12 (cyclic)
+    pm = load("tb/ref/gen_poly_mult_vectors_n12.py", "ref_pm12")
+    vecs = pm.build_vectors()
+    pm_meta = []
+    for i, (tag, a, b) in enumerate(vecs):
+        c = pm.poly_mult_via_ntt(a, b, pm.N, pm.Q, pm.OMEGA, pm.OMEGA_INV)
+        pm_meta.append({"tag": tag, "c_sha": sha(c), "c_head": c[:4]})
+        if tag in ("rand0", "sparse"):
+            arrays[f"pm12_{tag}_a"] = np.array(a, dtype=np.uint64)
+            arrays[f"pm12_{tag}_b"] = np.array(b, dtype=np.uint64)
+            arrays[f"pm12_{tag}_c"] = np.array(c, dtype=np.uint64)
+    meta["pm12"] = {"q": pm.Q, "N": pm.N, "psi": pm.PSI, "omega": pm.OMEGA, "omega_inv": pm.OMEGA_INV,
+                    "n_inv": pm.N_INV, "vectors": pm_meta,
+                    "source": "tb/ref/gen_poly_mult_vectors_n12.py:103,149"}
+
+    # ---------------------------------------------------------------- 4 verify_keyswitch (negacyclic)
+    vk = load("scripts/verify_keyswitch.py", "ref_vk")
+    q0 = vk.load_chain()[0]["q"]
+    rng = random.Random(42)
+    cases = []
+    for n_toy in (16, 64):
+        for t in range(3):
+            e0, e1, e2, ka = ([rng.randrange(q0) for _ in range(n_toy)] for _ in range(4))
+            s = [rng.randrange(q0) for _ in range(n_toy)]
+            e_ks = [rng.randrange(100) for _ in range(n_toy)]
+            kb = vk.poly_add(vk.poly_mult(ka, s, q0), e_ks, q0)
+            f0, f1 = vk.relin(e0, e1, e2, ka, kb, q0)
+            cases.append([e0, e1, e2, ka, kb, f0, f1])
+    arrays["relin16"] = np.array([c for c in cases[:3]], dtype=np.uint64)
+    arrays["relin64"] = np.array([c for c in cases[3:]], dtype=np.uint64)
+    # negacyclic poly_mult at N=256 on the 45-bit config prime and on the toy q=113
+    qc = 35184371884033
+    rng = random.Random(7)
+    a = [rng.randrange(qc) for _ in range(256)]
+    b = [rng.randrange(qc) for _ in range(256)]
+    arrays["pmneg256"] = np.array([a, b, vk.poly_mult(a, b, qc)], dtype=np.uint64)
+    a = [rng.randrange(113) for _ in range(16)]
+    b = [rng.randrange(113) for _ in range(16)]
+    arrays["pmneg16_q113"] = np.array([a, b, vk.poly_mult(a, b, 113)], dtype=np.uint64)
+    meta["keyswitch"] = {"q": q0, "config_prime": qc,
+                         "source": "scripts/verify_keyswitch.py:48 poly_mult, :62 relin"}
+
+    # ---------------------------------------------------------------- 5 verify_rescale
+    vr = load("scripts/verify_rescale.py", "ref_vr")
+    primes = [p["q"] for p in vr.load_chain()]
+    rs = {}
+    for i in range(len(primes) - 1):
+        qi, qo = primes[i], primes[i + 1]
+        pts = [0, 1, 2, qi - 3, qi - 2, qi - 1, qo - 1, qo, qo + 1]
+        pts = sorted({p for p in pts if 0 <= p < qi})
+        rng = random.Random(1000 + i)
+        pts += [rng.randrange(qi) for _ in range(2000)]
+        arrays[f"rescale_{i}_in"] = np.array(pts, dtype=np.uint64)
+        arrays[f"rescale_{i}_out"] = np.array([vr.rescale_coeff(c, qi, qo) for c in pts], dtype=np.uint64)
+    rng = random.Random(12345)
+    poly = [rng.randrange(primes[0]) for _ in range(vr.N)]
+    outp = vr.rescale_poly(poly, primes[0], primes[1])
+    arrays["rescale_poly_out"] = np.array(outp, dtype=np.uint64)
+    meta["rescale"] = {"primes": primes, "poly_seed": 12345, "N": vr.N,
+                       "source": "scripts/verify_rescale.py:38,56,101"}
+
+    # ---------------------------------------------------------------- 6 verify_e2e_mult
+    ve = load("scripts/verify_e2e_mult.py", "ref_ve")
+    ch = ve.load_chain()
+    qi, qo = ch[0]["q"], ch[1]["q"]
+    rng = random.Random(42)
+    e2e = []
+    for t in range(4):
+        c = [[rng.randrange(qi) for _ in range(16)] for _ in range(6)]
+        f0, f1 = ve.e2e_mult(c[0], c[1], c[2], c[3], c[4], c[5], qi, qo, ve.SCALE_BITS)
+        e2e.append(c + [f0, f1])
+    arrays["e2e16"] = np.array(e2e, dtype=np.uint64)
+    rng = random.Random(5)
+    xs = [rng.randrange(qi) for _ in range(4000)] + [0, 1, qi - 1]
+    arrays["e2e_rescale_in"] = np.array(xs, dtype=np.uint64)
+    arrays["e2e_rescale_out"] = np.array([ve.rescale(x, qi, qo, ve.SCALE_BITS) for x in xs], dtype=np.uint64)
+    meta["e2e"] = {"q_in": qi, "q_out": qo, "scale_bits": ve.SCALE_BITS,
+                   "source": "scripts/verify_e2e_mult.py:70 rescale, :78 e2e_mult"}
+
+    # ---------------------------------------------------------------- 7 _verify_fastred (b * omega mod q3)
+    fr = load("scripts/_verify_fastred.py", "ref_fr")
+    rng = random.Random(20261003)
+    bw = [(rng.randrange(fr.Q), rng.randrange(fr.Q)) for _ in range(4096)]
+    arrays["fastred_b"] = np.array([b for b, _ in bw], dtype=np.uint64)
+    arrays["fastred_w"] = np.array([w for _, w in bw], dtype=np.uint64)
+    arrays["fastred_out"] = np.array([fr.fast_red(b * w) for b, w in bw], dtype=np.uint64)
+    meta["fastred"] = {"q": fr.Q, "source": "scripts/_verify_fastred.py:55 fast_red (seed 20261003)"}
+
+    np.savez_compressed(OUT / "golden_core.npz", **arrays)
+    with open(OUT / "golden_core.json", "w") as f:
+        json.dump(meta, f, indent=1, sort_keys=True)
+    print("wrote", OUT / "golden_core.npz", sum(a.nbytes for a in arrays.values()), "bytes raw")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())
