@@ -41,6 +41,7 @@ SIGNATURES: dict[str, tuple] = {
     "ckks_ct_mul_scratch_bytes": (_sz, [_vp, _i32, _i32]),
     "ckks_ct_mul_relin_rescale": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _i32, _i32, _vp, _sz,
                                          _vp]),
+    "ckks_ct_mul_relin_rescale_noalloc": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _i32, _i32, _vp]),
     "ckks_profile_enable": (_i32, [_i32]),
     "ckks_profile_reset": (_i32, []),
     "ckks_profile_read": (_i32, [_i32, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),

@@ -178,6 +178,37 @@ int ckks_ct_mul_relin_rescale(const ckks_ctx* ctx, uint64_t* out, const uint64_t
                               const uint64_t* ct_b, const uint64_t* key, int n_ct, int level,
                               void* scratch, size_t scratch_bytes, void* stream);
 
+/* Size of the static device scratch used by ckks_ct_mul_relin_rescale_noalloc. */
+#define CKKS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+
+/*
+ * ckks_ct_mul_relin_rescale without caller scratch and without any device
+ * allocation.  No counterpart in the reference (an FPGA design has no device
+ * allocator); added for callers that are handed only their input and output
+ * buffers and cannot call cudaMalloc - a plugin inside a foreign runtime whose
+ * host owns all device memory through its own pool, or a serving loop whose
+ * pool has reserved the GPU so that a new allocation would fail or stall other
+ * streams.  Same arguments and results as ckks_ct_mul_relin_rescale minus the
+ * scratch pair; the caller still owns `out`, `ct_a`, `ct_b` and `key`.
+ *  - Scratch comes from one static device array of CKKS_NOALLOC_SCRATCH_BYTES
+ *    (32 MiB) that every GPU loading this library keeps until process exit.
+ *    A call needing more (ckks_ct_mul_scratch_bytes(ctx, n_ct, level) > 32 MiB,
+ *    i.e. more than 51 pairs at N = 2^12, L = 3) is rejected with
+ *    CKKS_EINVAL and a message naming the largest accepted batch.
+ *  - The first call on each device looks up the array's device address
+ *    (cudaGetSymbolAddress, with that device current) and caches it; make
+ *    that first call before any stream capture.
+ *  - All calls on a device share the one array: calls whose executions
+ *    overlap on the GPU (different streams, other host threads) race and
+ *    corrupt each other's results.  Serialise them on one stream.
+ *  - Nothing in the array needs clearing between calls (every word is written
+ *    before it is read); it keeps the last call's intermediates.
+ *  - Refused while the profiler below is enabled (it creates CUDA events).
+ */
+int ckks_ct_mul_relin_rescale_noalloc(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
+                                      const uint64_t* ct_b, const uint64_t* key, int n_ct,
+                                      int level, void* stream);
+
 /*
  * Per-kernel device timing (tracing).  When enabled, the multi-kernel entry
  * points record CUDA events around each kernel on the launching stream;
