@@ -37,8 +37,8 @@ UNIT = "ct-mult/s"
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=30)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=1500)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--batch", type=int, default=256)
     ap.add_argument("--log-n", type=int, default=12)
@@ -95,25 +95,36 @@ def run_reference(a) -> int:
 
 # ------------------------------------------------------------------ clocks
 class Clocks:
+    """nvidia-smi sampler (100 ms); `summary(t0, t1)` keeps the samples taken
+    inside the timed region [t0, t1] (host wall clock)."""
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
     def __init__(self, gpu_index: int):
         self.path = tempfile.mktemp(suffix=".csv")
         self.proc = None
         self.gpu = gpu_index
 
-    def __enter__(self):
+    def start(self):
         try:
             self.proc = subprocess.Popen(
-                ["nvidia-smi", "-i", str(self.gpu),
-                 "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
                  "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except Exception:
             self.proc = None
-        return self
+            return
+        t_end = time.time() + 5.0
+        while time.time() < t_end:          # wait for the first sample
+            try:
+                if os.path.getsize(self.path) > 0:
+                    break
+            except OSError:
+                pass
+            time.sleep(0.05)
 
-    def __exit__(self, *exc):
+    def stop(self):
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -121,42 +132,46 @@ class Clocks:
             except Exception:
                 self.proc.kill()
 
-    def summary(self) -> dict:
+    def summary(self, t0: float, t1: float) -> dict:
+        import datetime as _dt
         try:
             rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
         except Exception:
             rows = []
-        sm = []
-        smax = None
+        sm, smax, power = [], None, []
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             r = [x.strip() for x in r]
             try:
-                sm.append(float(r[1]))
-                smax = float(r[2])
+                ts = _dt.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                if ts < t0 - 0.05 or ts > t1 + 0.05:
+                    continue
+                sm.append(float(r[2]))
+                smax = float(r[3])
+                power.append(float(r[4]))
             except Exception:
                 continue
-            for nm, val in zip(names, r[5:9]):
+            for nm, val in zip(names, r[6:10]):
                 if val.lower().startswith("active"):
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                "reasons": sorted(reasons), "samples": len(sm),
+                "power_w_median": statistics.median(power) if power else None}
 
 
 # ------------------------------------------------------------------ ours
 def stage_bytes(stage: int, n: int, level: int) -> int:
-    """Algorithmic HBM bytes per CTA-unit of each ct-mult kernel, times units per ciphertext.
-    Returned per ciphertext pair."""
+    """Compulsory HBM bytes of each ct-mult kernel per ciphertext pair (each
+    input and output word once; the relinearisation key is shared by the whole
+    batch and L2-resident, so it is not counted per pair).  w = one limb."""
     w = 8 * n
-    if stage == 0:   # tensor: read a0,a1,b0,b1 ; write d0,d1,d2(eval),d2(coef) -- per limb
-        return level * 8 * w
-    if stage == 1:   # modup: per target prime: read `level` digits, 2 key rows of (value, shoup)
-        # per digit, write 2 accumulators
-        return (level + 1) * (level * w + level * 2 * 2 * w + 2 * w)
-    # down: per poly k: read accp, d_t, acc_t, then per limb i<t: d_i, acc_i ; write t limbs
-    t = level - 1
-    return 2 * (3 * w + t * 2 * w + t * w)
+    if stage == 0:   # tensor: read a0,a1,b0,b1 ; write d0,d1,d2 (eval), d2 (coef) per limb
+        return 8 * level * w
+    if stage == 1:   # modup: read d2 (coef + eval); write acc over q (2 polys) and over p
+        return (4 * level + 2) * w
+    # down: read acc over p (2), d0/d1 (2L), acc over q (2L); write 2 (L-1) limbs
+    return 6 * level * w
 
 
 def run_ours(a) -> int:
@@ -222,14 +237,20 @@ def run_ours(a) -> int:
     lib.ckks_profile_enable(1)
     barrier()
     torch.cuda.synchronize()
-    with Clocks(local if ws > 1 else 0) as clk:
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for i in range(a.steps):
-            step(i)
-        e1.record()
-        torch.cuda.synchronize()
+    clk = Clocks(local if ws > 1 else 0)
+    clk.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    t_host0 = time.time()
+    e0.record()
+    for i in range(a.steps):
+        step(i)
+    e1.record()
+    torch.cuda.synchronize()
+    t_host1 = time.time()
+    clk.stop()
     barrier()
     lib.ckks_profile_enable(0)
     ms = max_over_ranks(e0.elapsed_time(e1))
@@ -240,7 +261,7 @@ def run_ours(a) -> int:
         cnt = C.c_longlong()
         lib.ckks_profile_read(s, C.byref(tot), C.byref(cnt))
         stages.append((tot.value, cnt.value))
-    clocks = clk.summary()
+    clocks = clk.summary(t_host0, t_host1)
 
     # ---------------- end to end: pinned host buffers, H2D + call + D2H each step
     ha = cts[0][0].cpu().pin_memory()
@@ -257,7 +278,7 @@ def run_ours(a) -> int:
     barrier()
     e2 = torch.cuda.Event(enable_timing=True)
     e3 = torch.cuda.Event(enable_timing=True)
-    e2_steps = max(3, a.steps // 2)
+    e2_steps = max(3, a.steps // 4)
     e2.record()
     for _ in range(e2_steps):
         da.copy_(ha, non_blocking=True)

@@ -8,10 +8,9 @@
 //                          (Karatsuba), d2 -> INTT_j -> coefficient digit j.
 //   B  modup+ip  (ct, i):  for target prime i in {q_0..q_t, p}:
 //                          acc_k = sum_j NTT_i([digit_j]_{q_i}) * ksk[j][k][i]
-//                          (digit j at its own prime reuses the NTT-domain d2);
-//                          the special-prime CTA also INTTs acc_0, acc_1.
+//                          (digit j at its own prime reuses the NTT-domain d2).
 //   C  moddown+rescale (ct, k):
-//                          v = centred(acc_k mod p)            (coefficient)
+//                          v = centred(INTT_p(acc_k,p))        (coefficient)
 //                          limb t : o_t = d_k,t + (acc_k,t - NTT_t([v]_t)) p^-1
 //                                   w = centred(INTT_t(o_t))
 //                          limb i<t: out = (d_k,i + acc_k,i p^-1
@@ -19,8 +18,12 @@
 //                          (ModDown and rescale conversions merged into one
 //                          NTT per limb by linearity; bit-identical to doing
 //                          them one after the other).
-// Transforms per ct-mult at level L: L + (L-1)L + (L + 2) + 2(L + 1)
-// = 22 at L = 3 (vs 26 for the unmerged sequence).
+// Transforms per ct-mult at level L: L + (L-1)L + L + 2(L + 2) = 22 at L = 3
+// (vs 26 for the unmerged sequence).
+//
+// Launch shape: K = log2 coefficients per thread (3: N/8 threads, radix-8
+// passes; 4: N/16 threads, radix-16) and MINB = CTAs per SM the register
+// budget is cut for (__launch_bounds__).  Both are context tuning parameters.
 #include "dispatch.cuh"
 #include "profile.hpp"
 
@@ -29,7 +32,7 @@ struct CmScratch {
   u64* d2n;   // [n_ct][level][N]     tensor d2 (evaluation)
   u64* d2c;   // [n_ct][level][N]     d2 digits (coefficient)
   u64* acc;   // [n_ct][2][level][N]  key inner product over q_i (evaluation)
-  u64* accp;  // [n_ct][2][N]         key inner product over p (coefficient)
+  u64* accp;  // [n_ct][2][N]         key inner product over p (evaluation)
 };
 
 static size_t cm_words(int n, int n_ct, int level) {
@@ -52,9 +55,48 @@ static CmScratch cm_carve(void* base, int n, int n_ct, int level) {
   return s;
 }
 
+// ct-mult kernels are instantiated for log N in [6, 14] with K in {3, 4} at
+// MINB = 1, and for log N in {12, 13} also at MINB = 2.  Defaults K = 3,
+// MINB = 1 (measured fastest at N = 2^12 and 2^13: the 64-register budget of
+// MINB = 2 spills in the NTT passes).
+// f is called as f.template operator()<L, K, MINB>().
+template <typename F>
+static int dispatch_cm(int log_n, int kreq, int mreq, F&& f, const char* fn) {
+  const int k = kreq ? kreq : 3;
+  const bool big = log_n == 12 || log_n == 13;
+  const int mb = mreq ? mreq : 1;
+  if (k != 3 && k != 4) return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=%d not built", fn, k);
+  if (mb != 1 && !(mb == 2 && big))
+    return ckks_set_error(CKKS_EUNSUPPORTED, "%s: MINB=%d not built for log_n=%d", fn, mb, log_n);
+  switch (log_n) {
+#define CKKS_CM_CASE(L) \
+  case L:               \
+    return k == 3 ? f.template operator()<L, 3, 1>() : f.template operator()<L, 4, 1>();
+#define CKKS_CM_CASE2(L)                                                                     \
+  case L:                                                                                    \
+    if (mb == 2)                                                                             \
+      return k == 3 ? f.template operator()<L, 3, 2>() : f.template operator()<L, 4, 2>(); \
+    return k == 3 ? f.template operator()<L, 3, 1>() : f.template operator()<L, 4, 1>();
+    CKKS_CM_CASE(6)
+    CKKS_CM_CASE(7)
+    CKKS_CM_CASE(8)
+    CKKS_CM_CASE(9)
+    CKKS_CM_CASE(10)
+    CKKS_CM_CASE(11)
+    CKKS_CM_CASE2(12)
+    CKKS_CM_CASE2(13)
+    CKKS_CM_CASE(14)
+#undef CKKS_CM_CASE
+#undef CKKS_CM_CASE2
+    default:
+      return ckks_set_error(CKKS_EUNSUPPORTED, "%s: log_n=%d outside [6, 14]", fn, log_n);
+  }
+}
+
 // ---------------------------------------------------------------- kernel A
-template <int LOGN, int K>
-__global__ void __launch_bounds__(NttShape<LOGN, K>::T)
+// One CTA per (ct, limb j).  Registers: one coefficient array.
+template <int LOGN, int K, int MINB>
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_tensor(const u64* __restrict__ A, const u64* __restrict__ B, CmScratch S, int level,
                 const PrimeInfo* __restrict__ pi, const TwPair* __restrict__ tw) {
   extern __shared__ u64 sm[];
@@ -66,40 +108,48 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   const PrimeInfo P = pi[j];
   const size_t LN = (size_t)level * N;
   const u64* a0 = A + ct * 2 * LN + (size_t)j * N;
-  const u64* a1 = a0 + LN;
   const u64* b0 = B + ct * 2 * LN + (size_t)j * N;
-  const u64* b1 = b0 + LN;
   u64* d0 = S.d01 + ct * 2 * LN + (size_t)j * N;
-  u64* d1 = d0 + LN;
-  u64* d2n = S.d2n + ct * LN + (size_t)j * N;
-  u64* d2c = S.d2c + ct * LN + (size_t)j * N;
-  u64 x[Sh::E];
+  u64 x[Sh::E], y[Sh::E];
+  // d2 = a1 b1 ; keep in x
+  load_z<LOGN, K>(x, a0 + LN, tid);
+  load_z<LOGN, K>(y, b0 + LN, tid);
+  u64 m2[Sh::E];
+#pragma unroll
+  for (int e = 0; e < Sh::E; ++e) m2[e] = mulmod(x[e], y[e], P);
+  // d0 = a0 b0 ; d1 = (a0 + a1)(b0 + b1) - d0 - d2
+  u64 a0v[Sh::E], b0v[Sh::E];
+  load_z<LOGN, K>(a0v, a0, tid);
+  load_z<LOGN, K>(b0v, b0, tid);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) {
-    const int p = posZ<LOGN, K>(tid, e);
-    const u64 A0 = a0[p], A1 = a1[p], B0 = b0[p], B1 = b1[p];
-    const u64 m0 = mulmod(A0, B0, P);
-    const u64 m2 = mulmod(A1, B1, P);
-    u64 m1 = mulmod(addmod(A0, A1, P.q), addmod(B0, B1, P.q), P);
-    m1 = submod(submod(m1, m0, P.q), m2, P.q);
-    d0[p] = m0;
-    d1[p] = m1;
-    d2n[p] = m2;
-    x[e] = m2;
+    const u64 m0 = mulmod(a0v[e], b0v[e], P);
+    u64 m1 = mulmod(addmod(a0v[e], x[e], P.q), addmod(b0v[e], y[e], P.q), P);
+    m1 = submod(submod(m1, m0, P.q), m2[e], P.q);
+    a0v[e] = m0;
+    b0v[e] = m1;
   }
-  ntt_inv<LOGN, K>(x, sm, tid, tw + ((size_t)j * 4 + TW_INV) * N, P);
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) d2c[posC<LOGN, K>(tid, e)] = x[e];
+  store_z<LOGN, K>(a0v, d0, tid);
+  store_z<LOGN, K>(b0v, d0 + LN, tid);
+  store_z<LOGN, K>(m2, S.d2n + ct * LN + (size_t)j * N, tid);
+  ntt_inv<LOGN, K>(m2, sm, tid, tw + ((size_t)j * 4 + TW_INV) * N, P);
+  store_c<LOGN, K>(m2, S.d2c + ct * LN + (size_t)j * N, tid);
 }
 
 // ---------------------------------------------------------------- kernel B
-template <int LOGN, int K>
-__global__ void __launch_bounds__(NttShape<LOGN, K>::T)
+// One CTA per (ct, target prime).  The two accumulators live in thread-private
+// shared-memory slots (index e * T + tid), so only one coefficient array is in
+// registers.
+template <int LOGN, int K, int MINB>
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_modup(CmScratch S, const ulonglong2* __restrict__ key, int level, int nq,
                const PrimeInfo* __restrict__ pi, const TwPair* __restrict__ tw) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
+  constexpr int T = Sh::T;
+  u64* acc0s = sm + Sh::SMEM_WORDS;
+  u64* acc1s = acc0s + N;
   const long long ct = blockIdx.x / (level + 1);
   const int ti = blockIdx.x % (level + 1);
   const bool special = ti == level;
@@ -108,20 +158,15 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   const PrimeInfo P = pi[pidx];
   const size_t LN = (size_t)level * N;
   const TwPair* tf = tw + ((size_t)pidx * 4 + TW_FWD) * N;
-  u64 acc0[Sh::E], acc1[Sh::E];
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) acc0[e] = acc1[e] = 0;
 #pragma unroll 1
   for (int j = 0; j < level; ++j) {
     u64 x[Sh::E];
     if (!special && j == ti) {
-      const u64* src = S.d2n + ct * LN + (size_t)j * N;
-#pragma unroll
-      for (int e = 0; e < Sh::E; ++e) x[e] = src[posZ<LOGN, K>(tid, e)];
+      load_z<LOGN, K>(x, S.d2n + ct * LN + (size_t)j * N, tid);
     } else {
-      const u64* src = S.d2c + ct * LN + (size_t)j * N;
+      load_c<LOGN, K>(x, S.d2c + ct * LN + (size_t)j * N, tid);
 #pragma unroll
-      for (int e = 0; e < Sh::E; ++e) x[e] = csub(src[posC<LOGN, K>(tid, e)], P.q);
+      for (int e = 0; e < Sh::E; ++e) x[e] = csub(x[e], P.q);
       ntt_fwd_lazy<LOGN, K>(x, sm, tid, tf, P.q, P.q2);
     }
     const ulonglong2* k0 = key + (((size_t)j * 2 + 0) * (nq + 1) + pidx) * N;
@@ -131,46 +176,42 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
       const int p = posZ<LOGN, K>(tid, e);
       const ulonglong2 w0 = __ldg(k0 + p);
       const ulonglong2 w1 = __ldg(k1 + p);
-      acc0[e] += shoup_lazy(x[e], w0.x, w0.y, P.q);
-      acc1[e] += shoup_lazy(x[e], w1.x, w1.y, P.q);
+      const u64 t0 = shoup_lazy(x[e], w0.x, w0.y, P.q);
+      const u64 t1 = shoup_lazy(x[e], w1.x, w1.y, P.q);
+      const int s = e * T + tid;
+      acc0s[s] = (j == 0 ? 0ull : acc0s[s]) + t0;
+      acc1s[s] = (j == 0 ? 0ull : acc1s[s]) + t1;
     }
   }
+  // Special-prime accumulators stay in the evaluation domain here; kernel C
+  // (one CTA per output polynomial) brings each back with one INTT, which
+  // keeps the per-CTA work of this kernel within one transform of each other.
+  u64 x[Sh::E];
+  u64* o = special ? S.accp + ct * 2 * N : S.acc + ct * 2 * LN + (size_t)ti * N;
+  const size_t kstride = special ? (size_t)N : LN;
+#pragma unroll 1
+  for (int k = 0; k < 2; ++k) {
+    const u64* a = k ? acc1s : acc0s;
 #pragma unroll
-  for (int e = 0; e < Sh::E; ++e) {
-    acc0[e] = reduce_any(acc0[e], P);
-    acc1[e] = reduce_any(acc1[e], P);
-  }
-  if (special) {
-    const TwPair* ti_tab = tw + ((size_t)pidx * 4 + TW_INV) * N;
-    u64* o0 = S.accp + ct * 2 * N;
-    u64* o1 = o0 + N;
-    ntt_inv<LOGN, K>(acc0, sm, tid, ti_tab, P);
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e) o0[posC<LOGN, K>(tid, e)] = acc0[e];
-    ntt_inv<LOGN, K>(acc1, sm, tid, ti_tab, P);
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e) o1[posC<LOGN, K>(tid, e)] = acc1[e];
-  } else {
-    u64* o0 = S.acc + ct * 2 * LN + (size_t)ti * N;
-    u64* o1 = o0 + LN;
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e) {
-      const int p = posZ<LOGN, K>(tid, e);
-      o0[p] = acc0[e];
-      o1[p] = acc1[e];
-    }
+    for (int e = 0; e < Sh::E; ++e) x[e] = reduce_any(a[e * T + tid], P);
+    store_z<LOGN, K>(x, o + (size_t)k * kstride, tid);
   }
 }
 
 // ---------------------------------------------------------------- kernel C
-template <int LOGN, int K>
-__global__ void __launch_bounds__(NttShape<LOGN, K>::T)
+// One CTA per (ct, poly k).  The centred special-prime accumulator v and the
+// rescale limb w are kept in thread-private shared-memory slots.
+template <int LOGN, int K, int MINB>
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_down(CmScratch S, u64* __restrict__ out, int level, int nq,
               const PrimeInfo* __restrict__ pi, const TwPair* __restrict__ tw,
               const TwPair* __restrict__ pinv, const TwPair* __restrict__ qtinv) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
+  constexpr int T = Sh::T;
+  u64* vs = sm + Sh::SMEM_WORDS;
+  u64* ws = vs + N;
   const long long ct = blockIdx.x >> 1;
   const int k = blockIdx.x & 1;
   const int t = level - 1;
@@ -178,48 +219,56 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   const size_t LN = (size_t)level * N;
   const PrimeInfo PP = pi[nq];
   const PrimeInfo PT = pi[t];
-  const u64* accp = S.accp + (ct * 2 + k) * N;
   const u64* dk = S.d01 + ct * 2 * LN + (size_t)k * LN;
   const u64* ak = S.acc + ct * 2 * LN + (size_t)k * LN;
   u64* ok = out + ((size_t)ct * 2 + k) * (size_t)t * N;
 
-  u64 v[Sh::E], x[Sh::E];
+  u64 x[Sh::E];
+  load_z<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
+  ntt_inv<LOGN, K>(x, sm, tid, tw + ((size_t)nq * 4 + TW_INV) * N, PP);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) {
-    v[e] = accp[posC<LOGN, K>(tid, e)];
-    x[e] = v[e] > PP.half ? v[e] - PP.q + PT.q : v[e];
+    vs[e * T + tid] = x[e];
+    x[e] = x[e] > PP.half ? x[e] - PP.q + PT.q : x[e];
   }
   ntt_fwd_lazy<LOGN, K>(x, sm, tid, tw + ((size_t)t * 4 + TW_FWD) * N, PT.q, PT.q2);
   {
     const TwPair pt = pinv[t];
+    u64 dv[Sh::E], av[Sh::E];
+    load_z<LOGN, K>(dv, dk + (size_t)t * N, tid);
+    load_z<LOGN, K>(av, ak + (size_t)t * N, tid);
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) {
-      const int p = posZ<LOGN, K>(tid, e);
-      const u64 ks = shoup(ak[(size_t)t * N + p] + PT.q4 - x[e], pt.w, pt.ws, PT.q);
-      x[e] = addmod(dk[(size_t)t * N + p], ks, PT.q);
+      const u64 ks = shoup(av[e] + PT.q4 - x[e], pt.w, pt.ws, PT.q);
+      x[e] = addmod(dv[e], ks, PT.q);
     }
   }
   ntt_inv<LOGN, K>(x, sm, tid, tw + ((size_t)t * 4 + TW_INV) * N, PT);
+#pragma unroll
+  for (int e = 0; e < Sh::E; ++e) ws[e * T + tid] = x[e];
 #pragma unroll 1
   for (int i = 0; i < t; ++i) {
     const PrimeInfo P = pi[i];
     const TwPair pv = pinv[i];
     const TwPair ci = qtinv[(size_t)t * nq + i];
-    u64 z[Sh::E];
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) {
-      const u64 vi = v[e] > PP.half ? v[e] - PP.q + P.q : v[e];
-      const u64 wi = x[e] > PT.half ? x[e] - PT.q + P.q : x[e];
-      z[e] = shoup_lazy(vi, pv.w, pv.ws, P.q) + wi;  // [0, 3q)
+      const u64 v = vs[e * T + tid];
+      const u64 w = ws[e * T + tid];
+      const u64 vi = v > PP.half ? v - PP.q + P.q : v;
+      const u64 wi = w > PT.half ? w - PT.q + P.q : w;
+      x[e] = shoup_lazy(vi, pv.w, pv.ws, P.q) + wi;  // [0, 3q)
     }
-    ntt_fwd_lazy<LOGN, K>(z, sm, tid, tw + ((size_t)i * 4 + TW_FWD) * N, P.q, P.q2);
+    ntt_fwd_lazy<LOGN, K>(x, sm, tid, tw + ((size_t)i * 4 + TW_FWD) * N, P.q, P.q2);
+    u64 dv[Sh::E], av[Sh::E];
+    load_z<LOGN, K>(dv, dk + (size_t)i * N, tid);
+    load_z<LOGN, K>(av, ak + (size_t)i * N, tid);
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) {
-      const int p = posZ<LOGN, K>(tid, e);
-      const u64 s = dk[(size_t)i * N + p] + shoup_lazy(ak[(size_t)i * N + p], pv.w, pv.ws, P.q) +
-                    P.q4 - z[e];  // (0, 7q)
-      ok[(size_t)i * N + p] = shoup(s, ci.w, ci.ws, P.q);
+      const u64 s = dv[e] + shoup_lazy(av[e], pv.w, pv.ws, P.q) + P.q4 - x[e];  // (0, 7q)
+      x[e] = shoup(s, ci.w, ci.ws, P.q);
     }
+    store_z<LOGN, K>(x, ok + (size_t)i * N, tid);
   }
 }
 
@@ -264,7 +313,7 @@ int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
   CKKS_REQUIRE(ctx->n_special == 1, "%s: context needs exactly one special prime", fn);
   CKKS_REQUIRE(level >= 2 && level <= ctx->n_q, "%s: level=%d outside [2, %d]", fn, level,
                ctx->n_q);
-  CKKS_REQUIRE(ctx->log_n >= 5, "%s: log_n=%d below the supported minimum 5", fn, ctx->log_n);
+  CKKS_REQUIRE(ctx->log_n >= 6, "%s: log_n=%d below the supported minimum 6", fn, ctx->log_n);
   CKKS_REQUIRE(n_ct >= 0, "%s: n_ct < 0", fn);
   u64 pmin = ~0ull, pmax = 0;
   for (int i = 0; i < ctx->n_primes; ++i) {
@@ -281,40 +330,37 @@ int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
                need);
   CmScratch S = cm_carve(scratch, ctx->n, n_ct, level);
   cudaStream_t st = as_stream(stream);
-  return dispatch_logn(ctx->log_n, [&]<int L, int K>() -> int {
-    if constexpr (L < 5) {
-      return ckks_set_error(CKKS_EUNSUPPORTED, "%s: log_n too small", fn);
-    } else {
-      using Sh = NttShape<L, K>;
-      const int smem = Sh::SMEM_WORDS * 8;
-      auto ka = k_cm_tensor<L, K>;
-      auto kb = k_cm_modup<L, K>;
-      auto kc = k_cm_down<L, K>;
-      ensure_smem(ka, smem);
-      ensure_smem(kb, smem);
-      ensure_smem(kc, smem);
-      {
-        ProfSpan span(CKKS_STAGE_CM_TENSOR, st);
-        ka<<<grid1d((long long)n_ct * level), Sh::T, smem, st>>>(
-            reinterpret_cast<const u64*>(ct_a), reinterpret_cast<const u64*>(ct_b), S, level,
-            ctx->d_pi, ctx->d_tw);
-      }
-      if (int rc = ckks_check_launch(fn)) return rc;
-      {
-        ProfSpan span(CKKS_STAGE_CM_MODUP, st);
-        kb<<<grid1d((long long)n_ct * (level + 1)), Sh::T, smem, st>>>(
-            S, reinterpret_cast<const ulonglong2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw);
-      }
-      if (int rc = ckks_check_launch(fn)) return rc;
-      {
-        ProfSpan span(CKKS_STAGE_CM_DOWN, st);
-        kc<<<grid1d((long long)n_ct * 2), Sh::T, smem, st>>>(
-            S, reinterpret_cast<u64*>(out), level, ctx->n_q, ctx->d_pi, ctx->d_tw, ctx->d_pinv,
-            ctx->d_qtinv);
-      }
-      return ckks_check_launch(fn);
+  return dispatch_cm(ctx->log_n, ctx->tune_cm_k, ctx->tune_cm_minb, [&]<int L, int K, int MINB>() -> int {
+    using Sh = NttShape<L, K>;
+    const int smem_a = Sh::SMEM_WORDS * 8;
+    const int smem_bc = (Sh::SMEM_WORDS + 2 * Sh::N) * 8;
+    auto ka = k_cm_tensor<L, K, MINB>;
+    auto kb = k_cm_modup<L, K, MINB>;
+    auto kc = k_cm_down<L, K, MINB>;
+    ensure_smem(ka, smem_a);
+    ensure_smem(kb, smem_bc);
+    ensure_smem(kc, smem_bc);
+    {
+      ProfSpan span(CKKS_STAGE_CM_TENSOR, st);
+      ka<<<grid1d((long long)n_ct * level), Sh::T, smem_a, st>>>(
+          reinterpret_cast<const u64*>(ct_a), reinterpret_cast<const u64*>(ct_b), S, level,
+          ctx->d_pi, ctx->d_tw);
     }
-  });
+    if (int rc = ckks_check_launch(fn)) return rc;
+    {
+      ProfSpan span(CKKS_STAGE_CM_MODUP, st);
+      kb<<<grid1d((long long)n_ct * (level + 1)), Sh::T, smem_bc, st>>>(
+          S, reinterpret_cast<const ulonglong2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw);
+    }
+    if (int rc = ckks_check_launch(fn)) return rc;
+    {
+      ProfSpan span(CKKS_STAGE_CM_DOWN, st);
+      kc<<<grid1d((long long)n_ct * 2), Sh::T, smem_bc, st>>>(
+          S, reinterpret_cast<u64*>(out), level, ctx->n_q, ctx->d_pi, ctx->d_tw, ctx->d_pinv,
+          ctx->d_qtinv);
+    }
+    return ckks_check_launch(fn);
+  }, fn);
 }
 
 extern "C" int ckks_ct_mul_relin_rescale(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,

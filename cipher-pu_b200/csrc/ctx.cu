@@ -213,3 +213,21 @@ extern "C" int ckks_ctx_destroy(ckks_ctx* ctx) {
   free_ctx(ctx);
   return CKKS_OK;
 }
+
+extern "C" int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value) {
+  CKKS_REQUIRE(ctx != nullptr, "ckks_ctx_set_tuning: ctx is NULL");
+  switch (param) {
+    case CKKS_TUNE_CM_LOG_ELEMS:
+      CKKS_REQUIRE(value == 0 || value == 3 || value == 4,
+                   "ckks_ctx_set_tuning: ct-mult log2 elements per thread must be 0, 3 or 4");
+      ctx->tune_cm_k = value;
+      return CKKS_OK;
+    case CKKS_TUNE_CM_MIN_BLOCKS:
+      CKKS_REQUIRE(value == 0 || value == 1 || value == 2,
+                   "ckks_ctx_set_tuning: ct-mult CTAs per SM must be 0, 1 or 2");
+      ctx->tune_cm_minb = value;
+      return CKKS_OK;
+    default:
+      return ckks_set_error(CKKS_EINVAL, "ckks_ctx_set_tuning: unknown parameter %d", param);
+  }
+}

@@ -16,6 +16,8 @@ struct ckks_ctx {
   int n_special = 0;  // trailing special primes (0 or 1)
   int n_q = 0;        // n_primes - n_special
   int device = 0;
+  int tune_cm_k = 0;     // ct-mult: log2 coefficients per thread (0 = default)
+  int tune_cm_minb = 0;  // ct-mult: CTAs per SM targeted by the register budget (0 = default)
   std::vector<u64> primes, psi, omega;
   std::vector<int> has_nega;
   std::vector<PrimeInfo> h_pi;

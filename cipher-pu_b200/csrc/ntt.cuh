@@ -230,6 +230,34 @@ __device__ __forceinline__ void ntt_inv(u64 (&x)[1 << K], u64* sm, int tid,
   for (int e = 0; e < (1 << K); ++e) x[e] = csub(shoup_lazy(x[e], P.ninv, P.ninv_s, P.q), P.q);
 }
 
+// Layout-Z global access: the last pass has unit stride inside each run, so
+// registers (e, e+1) with e even are adjacent words; move them as 16-byte vectors.
+template <int LOGN, int K>
+__device__ __forceinline__ void load_z(u64 (&x)[1 << K], const u64* __restrict__ src, int tid) {
+#pragma unroll
+  for (int e = 0; e < (1 << K); e += 2) {
+    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(src + posZ<LOGN, K>(tid, e)));
+    x[e] = v.x;
+    x[e + 1] = v.y;
+  }
+}
+template <int LOGN, int K>
+__device__ __forceinline__ void store_z(const u64 (&x)[1 << K], u64* __restrict__ dst, int tid) {
+#pragma unroll
+  for (int e = 0; e < (1 << K); e += 2)
+    *reinterpret_cast<ulonglong2*>(dst + posZ<LOGN, K>(tid, e)) = make_ulonglong2(x[e], x[e + 1]);
+}
+template <int LOGN, int K>
+__device__ __forceinline__ void load_c(u64 (&x)[1 << K], const u64* __restrict__ src, int tid) {
+#pragma unroll
+  for (int e = 0; e < (1 << K); ++e) x[e] = __ldg(src + posC<LOGN, K>(tid, e));
+}
+template <int LOGN, int K>
+__device__ __forceinline__ void store_c(const u64 (&x)[1 << K], u64* __restrict__ dst, int tid) {
+#pragma unroll
+  for (int e = 0; e < (1 << K); ++e) dst[posC<LOGN, K>(tid, e)] = x[e];
+}
+
 // Dynamic shared memory bytes needed by one transform.
 template <int LOGN, int K>
 constexpr int ntt_smem_bytes() {

@@ -62,6 +62,19 @@ int ckks_ctx_create(int log_n, int n_primes, int n_special, const uint64_t* prim
 int ckks_ctx_destroy(ckks_ctx* ctx);
 
 /*
+ * Launch-shape tuning of a context (used by the autotuner).  Parameters:
+ *   CKKS_TUNE_CM_LOG_ELEMS: coefficients per thread of the ct-mult kernels
+ *   as log2 (3 -> radix-8 passes with N/8 threads, 4 -> radix-16 with N/16;
+ *   0 = default 3).
+ *   CKKS_TUNE_CM_MIN_BLOCKS: CTAs per SM the ct-mult kernels' register
+ *   budget targets (1 or 2; 2 is built for N = 2^12, 2^13 only; 0 = default).
+ * The reference fixes its datapath shape at synthesis time
+ * (rtl/m1/ntt_unit.sv:39-52 parameters).
+ */
+enum { CKKS_TUNE_CM_LOG_ELEMS = 0, CKKS_TUNE_CM_MIN_BLOCKS = 1 };
+int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value);
+
+/*
  * In-place forward (inverse = 0) or inverse NTT of n_polys x n_limbs
  * polynomials, negacyclic (cyclic = 0, ring X^N + 1) or cyclic (X^N - 1).
  * Forward: natural coefficients -> bit-reversed evaluations; inverse: back,

@@ -35,7 +35,14 @@ OUT = Path(__file__).resolve().parent
 def load(relpath: str, name: str):
     spec = importlib.util.spec_from_file_location(name, REF / relpath)
     mod = importlib.util.module_from_spec(spec)
-    spec.loader.exec_module(mod)
+    sys.modules[name] = mod  # dataclasses look their module up here
+    import contextlib
+    import io
+    try:
+        with contextlib.redirect_stdout(io.StringIO()):
+            spec.loader.exec_module(mod)
+    except SystemExit:
+        pass  # some scripts run their checks at import and exit; their functions are defined first
     return mod
 
 
@@ -200,6 +207,120 @@ def main() -> int:
     arrays["fastred_w"] = np.array([w for _, w in bw], dtype=np.uint64)
     arrays["fastred_out"] = np.array([fr.fast_red(b * w) for b, w in bw], dtype=np.uint64)
     meta["fastred"] = {"q": fr.Q, "source": "scripts/_verify_fastred.py:55 fast_red (seed 20261003)"}
+
+    # ---------------------------------------------------------------- 8 golden_fc_layer
+    sys.path.insert(0, str(REF / "scripts"))
+    fc = load("scripts/golden_fc_layer.py", "ref_fc")
+    import contextlib
+    import io
+    with contextlib.redirect_stdout(io.StringIO()):
+        f1, f2 = fc.build_mnist_cnn_model(512, 128, 10)
+        y1, y1q = f1.test_forward(num_slots=4)
+        y2, y2q = f2.test_forward(num_slots=4)
+    arrays["fc1_w"] = f1.weights
+    arrays["fc2_w"] = f2.weights
+    arrays["fc1_test_y"] = np.asarray(y1, dtype=np.float64)
+    arrays["fc2_test_y"] = np.asarray(y2, dtype=np.float64)
+    arrays["fc1_test_yq"] = np.asarray(y1q, dtype=np.float64)
+    rng = np.random.default_rng(99)
+    xe = rng.standard_normal((4, 512))
+    arrays["fc_e2e_x"] = xe
+    arrays["fc_e2e_logits"] = np.asarray(f2.forward(np.maximum(f1.forward(xe), 0)), dtype=np.float64)
+    meta["fc"] = {"source": "scripts/golden_fc_layer.py:28,93,128"}
+
+    # ---------------------------------------------------------------- 9 slot encode / decode
+    ms = load("scripts/verify_multi_slot_simd.py", "ref_ms")
+    rng = np.random.default_rng(3)
+    vv = rng.uniform(-1, 1, size=(5, ms.SLOTS))
+    arrays["simd_v"] = vv
+    arrays["simd_m"] = np.array([ms.encode(v) for v in vv])
+    arrays["simd_dec"] = np.array([ms.decode(ms.encode(v)) for v in vv])
+    mlp = load("scripts/verify_project_b_mlp_reference.py", "ref_mlp")
+    xs = rng.standard_normal((3, 64)) + 1j * rng.standard_normal((3, 64))
+    arrays["negfft_x"] = xs
+    arrays["negfft_y"] = np.array([mlp.neg_fft(x) for x in xs])
+    arrays["negifft_y"] = np.array([mlp.neg_ifft(x) for x in xs])
+    meta["simd"] = {"N": ms.N_POLY, "scale": ms.SCALE, "slots": ms.SLOTS,
+                    "source": "scripts/verify_multi_slot_simd.py:32,42,75,88; "
+                              "scripts/verify_project_b_mlp_reference.py:60,73"}
+
+    # ---------------------------------------------------------------- 10 noise monitor
+    mh = load("scripts/verify_m4_h_multilayer.py", "ref_mh")
+    rng = random.Random(11)
+    nm = []
+    for q, n, mag in ((q3, 4096, None), (q0, 1024, 1 << 20), (113, 16, None)):
+        c = [rng.randrange(q) if mag is None else (rng.randrange(-mag, mag) % q) for _ in range(n)]
+        e, r = mh.noise_monitor_energy(c, q)
+        sw, rw = mh.layer_sigma_welford(c, q)
+        nm.append({"q": q, "coeffs": c, "E": e, "r_hat": r, "sigma_w": sw, "r_hat_w": rw})
+    meta["noise"] = {"cases": nm, "source": "scripts/verify_m4_h_multilayer.py:162,193"}
+
+    # ---------------------------------------------------------------- 11 gear controllers
+    ad = load("scripts/verify_m4_h_adaptive.py", "ref_ad")
+    ga = load("scripts/verify_m4_a_gear_ctrl.py", "ref_ga")
+    rs = [10 ** (-k / 4) for k in range(0, 40)]
+    seq_r = [0.001, 0.001, 0.3, 0.001, 0.2, 0.05, 0.05, 0.05, 0.4, 0.01, 0.01, 0.01, 0.01]
+    hyst = []
+    g_old = 0
+    for r in seq_r:
+        g_new = ad.select_gear_safe(r)
+        g_old = ad.select_gear_with_hysteresis(g_new, g_old, r)
+        hyst.append(g_old)
+    agc = mlp.AdaptiveGearCtrl()
+    agc_seq = [agc.step(r) for r in [0.05, 0.05, 0.05, 0.3, 0.3, 0.3, 0.15, 0.15, 0.15, 0.6, 0.6, 0.6]]
+    meta["gear"] = {
+        "geo": [{k: g[k] for k in ("threshold", "trunc_bits", "skip_rate")} | {
+            "extra": ad.compute_extra(g)[2], "total_growth": ad.total_growth(g)} for g in ad.GEO],
+        "r_sweep": rs, "safe": [ad.select_gear_safe(r) for r in rs],
+        "seq_r": seq_r, "hyst": hyst,
+        "gear_config": [ga.get_gear_config(g) for g in range(6)],
+        "gear_config_ovr": ga.get_gear_config(2, 1234, True),
+        "agc_seq": agc_seq,
+        "source": "scripts/verify_m4_h_adaptive.py:37,48,101,114; scripts/verify_m4_a_gear_ctrl.py:41; "
+                  "scripts/verify_project_b_mlp_reference.py:279"}
+
+    # ---------------------------------------------------------------- 12 block sparsity
+    da = load("scripts/verify_m4_d_approx_mult.py", "ref_da")
+    rng = random.Random(5)
+    bs = []
+    for B in (1, 2, 4, 16):
+        x = [rng.randrange(113) for _ in range(16)]
+        out, skipped = da.post_process_block(x, 20, True, 113, B)
+        bs.append({"B": B, "x": x, "out": out, "skipped": skipped})
+    meta["block_post"] = bs
+    e10 = load("scripts/exp_e10_sparsity_sweep_v2.py", "ref_e10")
+    rng = np.random.default_rng(4)
+    W = rng.standard_normal((128, 784)) / np.sqrt(784)
+    for thr in (0.02, 0.05):
+        mW, skip, tot, dens = e10.apply_block_sparse_mask(W, thr, 4)
+        arrays[f"bsm_mask_{thr}"] = np.packbits(mW != 0)
+        meta[f"bsm_{thr}"] = {"skip": skip, "total": tot, "density": dens}
+    arrays["bsm_W"] = W
+    meta["block_sparse_source"] = ("scripts/verify_m4_d_approx_mult.py:50 post_process_block; "
+                                   "scripts/exp_e10_sparsity_sweep_v2.py:102 apply_block_sparse_mask")
+
+    # ---------------------------------------------------------------- 13 DARE (exp_e24)
+    e24 = load("scripts/exp_e24_rotation_bootstrap.py", "ref_e24")
+    n24, q24 = e24.N, e24.Q
+    rng = np.random.default_rng(8)
+    s = rng.integers(-1, 2, size=n24)
+    np.random.seed(1234)
+    m_int = rng.integers(-(1 << 20), 1 << 20, size=n24)
+    e0 = rng.integers(-3, 4, size=n24)
+    ct = e24.rlwe_encrypt_mint(m_int, s, e0, q24)
+    dec = e24.decrypt_exact_int(ct, s, q24)
+    ct2, m_new = e24.reencrypt(ct, s, q24, 2 ** 20, np.random.default_rng(9))
+    dec2 = e24.decrypt_exact_int(ct2, s, q24)
+    arrays["dare_s"] = s
+    arrays["dare_ct_b"] = np.asarray(ct[0], dtype=np.int64)
+    arrays["dare_ct_a"] = np.asarray(ct[1], dtype=np.int64)
+    arrays["dare_dec"] = dec
+    arrays["dare_ct2_b"] = np.asarray(ct2[0], dtype=np.int64)
+    arrays["dare_ct2_a"] = np.asarray(ct2[1], dtype=np.int64)
+    arrays["dare_dec2"] = dec2
+    arrays["dare_m_new"] = np.asarray(m_new, dtype=np.int64)
+    arrays["dare_e_new"] = np.random.default_rng(9).integers(-1, 2, size=n24).astype(np.int64)
+    meta["dare"] = {"N": n24, "q": q24, "source": "scripts/exp_e24_rotation_bootstrap.py:126,209,287"}
 
     np.savez_compressed(OUT / "golden_core.npz", **arrays)
     with open(OUT / "golden_core.json", "w") as f:

@@ -168,3 +168,99 @@ def test_rns_oracle_matches_bigint(n, l):
     b = rnd((1, 2, l, n), qs)
     ksk = rnd((l, 2, l + 1, n), qs + [p])
     assert np.array_equal(R.ct_mul_relin_rescale(a, b, ksk, qs, p)[0], R.bigint_ct_mul(a, b, ksk, qs, p))
+
+
+# ---------------------------------------------------------------- second golden set
+from oracle import encode as OE  # noqa: E402
+from oracle import noise_gear as NG  # noqa: E402
+
+
+def test_fc_golden_model_dropin_matches_reference():
+    sys_path = str(Path(__file__).resolve().parents[1] / "cipher-pu_b200" / "scripts")
+    import sys
+    if sys_path not in sys.path:
+        sys.path.insert(0, sys_path)
+    import golden_fc_layer as fc
+    f1, f2 = fc.build_mnist_cnn_model(512, 128, 10)
+    assert np.array_equal(f1.weights, ARR["fc1_w"]) and np.array_equal(f2.weights, ARR["fc2_w"])
+    y1, y1q = f1.test_forward(num_slots=4)
+    assert np.array_equal(np.asarray(y1, dtype=np.float64), ARR["fc1_test_y"])
+    assert np.array_equal(np.asarray(y1q, dtype=np.float64), ARR["fc1_test_yq"])
+    y2, _ = f2.test_forward(num_slots=4)
+    assert np.array_equal(np.asarray(y2, dtype=np.float64), ARR["fc2_test_y"])
+    logits = f2.forward(np.maximum(f1.forward(ARR["fc_e2e_x"]), 0))
+    assert np.array_equal(np.asarray(logits, dtype=np.float64), ARR["fc_e2e_logits"])
+
+
+def test_slot_encode_decode_golden():
+    m = META["simd"]
+    for v, mm, dd in zip(ARR["simd_v"], ARR["simd_m"], ARR["simd_dec"]):
+        assert np.allclose(OE.encode(v, m["scale"], m["N"]), mm, atol=1e-12)
+        assert np.allclose(OE.decode(OE.encode(v, m["scale"], m["N"]), m["scale"], m["slots"]), dd, atol=1e-12)
+    for x, y, z in zip(ARR["negfft_x"], ARR["negfft_y"], ARR["negifft_y"]):
+        assert np.allclose(OE.pb_neg_fft(x), y, atol=1e-9)
+        assert np.allclose(OE.pb_neg_ifft(x), z, atol=1e-12)
+    # the scaled integer codec round-trips uniform [-1, 1] slots to ~1e-12 at Delta = 2^40
+    rng = np.random.default_rng(0)
+    s = rng.uniform(-1, 1, 2048)
+    back = OE.ckks_decode(OE.ckks_encode(s, 2.0 ** 40, 4096), 2.0 ** 40, 2048)
+    assert np.abs(back.real - s).max() < 1e-9
+
+
+def test_noise_monitor_golden():
+    for c in META["noise"]["cases"]:
+        e, r = NG.noise_energy(c["coeffs"], c["q"])
+        assert e == c["E"] and r == c["r_hat"]
+        sw, rw = NG.welford(c["coeffs"], c["q"])
+        assert abs(sw - c["sigma_w"]) <= 1e-9 * max(1.0, c["sigma_w"]) and abs(rw - c["r_hat_w"]) < 1e-15
+
+
+def test_gear_controllers_golden():
+    g = META["gear"]
+    for rec, geo in zip(g["geo"], NG.GEO):
+        assert NG.compute_extra(geo)[2] == rec["extra"] and NG.total_growth(geo) == rec["total_growth"]
+    assert [NG.select_gear_safe(r) for r in g["r_sweep"]] == g["safe"]
+    old, seq = 0, []
+    for r in g["seq_r"]:
+        old = NG.select_gear_with_hysteresis(NG.select_gear_safe(r), old, r)
+        seq.append(old)
+    assert seq == g["hyst"]
+    assert [NG.gear_config(i) for i in range(6)] == g["gear_config"]
+    assert NG.gear_config(2, 1234, True) == g["gear_config_ovr"]
+    agc = NG.AgcRhat()
+    assert [agc.step(r) for r in [0.05, 0.05, 0.05, 0.3, 0.3, 0.3, 0.15, 0.15, 0.15, 0.6, 0.6, 0.6]] == g["agc_seq"]
+
+
+def test_rtl_gear_controller_semantics():
+    # rtl/m4/adaptive_gear_ctrl.sv: reset gear 3; downgrade at once; upgrade after HYST_CNT
+    c = NG.GearCtrlRTL(500, 200, 50, 3)
+    assert c.flush(600) == 0            # downgrade immediately
+    seq = [c.flush(10) for _ in range(5)]  # candidate 3 must be seen HYST_CNT+1 times
+    assert seq == [0, 0, 0, 3, 3]
+    assert c.flush(300) == 1
+    assert c.flush(10, manual_en=True, manual_gear=2) == 2
+    assert c.flush(10, hysteresis=False) == 3
+
+
+def test_block_sparsity_golden():
+    for rec in META["block_post"]:
+        out, sk = NG.post_process_block(rec["x"], 20, True, 113, rec["B"])
+        assert out == rec["out"] and sk == rec["skipped"]
+    W = ARR["bsm_W"]
+    for thr in (0.02, 0.05):
+        mW, skip, tot, dens = NG.block_sparse_mask(W, thr, 4)
+        assert np.array_equal(np.packbits(mW != 0), ARR[f"bsm_mask_{thr}"])
+        rec = META[f"bsm_{thr}"]
+        assert (skip, tot) == (rec["skip"], rec["total"]) and abs(dens - rec["density"]) < 1e-15
+
+
+def test_dare_golden_semantics():
+    q = META["dare"]["q"]
+    s = ARR["dare_s"]
+    b, a = ARR["dare_ct_b"], ARR["dare_ct_a"]
+    # reference convention (b, a) -> (c0, c1) = (b, -a)
+    c0, c1 = [int(x) % q for x in b], [(-int(x)) % q for x in a]
+    a2 = ARR["dare_ct2_a"]
+    new_c0, new_c1, dec = OE.dare_refresh(c0, c1, s, [(-int(x)) % q for x in a2], ARR["dare_e_new"], q)
+    assert dec == [int(x) for x in ARR["dare_dec"]]
+    assert new_c0 == [int(x) % q for x in ARR["dare_ct2_b"]]
