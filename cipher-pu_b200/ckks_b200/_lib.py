@@ -43,6 +43,26 @@ SIGNATURES: dict[str, tuple] = {
     "ckks_ct_mul_relin_rescale": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _i32, _i32, _vp, _sz,
                                          _vp]),
     "ckks_ct_mul_relin_rescale_noalloc": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _i32, _i32, _vp]),
+    "ckks_encode": (_i32, [_vp, _u64p, _vp, _i32, _i32, _i32, C.c_double, _vp]),
+    "ckks_decode": (_i32, [_vp, _vp, _u64p, _i32, _i32, _i32, C.c_double, _vp]),
+    "ckks_decrypt": (_i32, [_vp, _u64p, _u64p, _u64p, _i32, _i32, _vp]),
+    "ckks_encrypt": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _vp, _i32, _i32, _vp]),
+    "ckks_dare_scratch_bytes": (_sz, [_vp, _i32, _i32]),
+    "ckks_dare_refresh": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _vp, _i32, _i32, _i32, _i32, _vp,
+                                 _sz, _vp]),
+    "ckks_noise_energy": (_i32, [_u64p, _u64p, _i32, _i32, _u64, _vp]),
+    "ckks_snr_sums": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _vp]),
+    "ckks_block_sparse_mask": (_i32, [_vp, _vp, _vp, _i64, _i32, C.c_double, _vp]),
+    "ckks_block_post_process": (_i32, [_u64p, _vp, _u64p, _i32, _i32, _i32, _u64, _u64, _i32, _vp]),
+    "ckks_rns_split": (_i32, [C.POINTER(_u64), _i32, _u64p, _u64p, _i64, _i32, _i32, _vp]),
+    "ckks_rns_merge": (_i32, [C.POINTER(_u64), _i32, _u64p, _u64p, _i64, _i32, _i32, _vp]),
+    "ckks_linear_plain_weights": (_i32, [_vp, _u64p, _u64p, _vp, _vp, _vp, _i32, _i32, _i32, _vp]),
+    "ckks_sample_uniform": (_i32, [_vp, _u64p, _i32, _i32, _i32, _u64, _u64, _vp]),
+    "ckks_sample_ternary": (_i32, [_vp, _i64, _u64, _u64, _vp]),
+    "ckks_sample_dgauss": (_i32, [_vp, _i64, C.c_double, _u64, _u64, _vp]),
+    "ckks_gear_ctrl_init": (_i32, [_vp, C.POINTER(_u64), C.POINTER(_u64), _i32]),
+    "ckks_gear_ctrl_raw": (_i32, [_vp, _u64, _u64]),
+    "ckks_gear_ctrl_flush": (_i32, [_vp, _u64, _u64, _i32, _i32, _i32]),
     "ckks_profile_enable": (_i32, [_i32]),
     "ckks_profile_reset": (_i32, []),
     "ckks_profile_read": (_i32, [_i32, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),

@@ -1,0 +1,160 @@
+"""High-level CKKS evaluator: keys, encryption, homomorphic multiply, DARE.
+
+Conventions: decryption m ~ c0 + c1 s; ciphertexts [C, 2, level, N] in the
+evaluation domain over q_0..q_{level-1}; the relinearisation key is hybrid
+(dnum = L digits, one special prime P); the scale of every ciphertext is
+tracked on the host in float64 (rescaling divides by a 45-bit prime, so the
+scale drifts away from Delta; decoding uses the tracked scale).
+
+Randomness comes from the library's Philox sampler: (seed, stream id) pairs
+are drawn from a per-evaluator counter, so a run is reproducible per seed.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import ops
+from .context import Context
+from .params import CkksParams
+
+U64 = torch.uint64
+
+
+@dataclass
+class Ciphertext:
+    data: torch.Tensor          # [C, 2, level, N] evaluation domain
+    scale: float
+
+    @property
+    def level(self) -> int:
+        return int(self.data.shape[2])
+
+    @property
+    def count(self) -> int:
+        return int(self.data.shape[0])
+
+
+@dataclass
+class SecretKey:
+    s_coef: torch.Tensor        # [N] int64 ternary
+    s_eval: torch.Tensor        # [n_primes, N] evaluation domain over q_0..q_{L-1}, P
+
+
+class Evaluator:
+    def __init__(self, params: CkksParams, device=None):
+        self.params = params
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        self.ctx = Context.get(params.log_n, params.primes, n_special=1)
+        self.n = params.n
+        self._stream_id = 1
+        self.seed = params.seed
+        self.sk: SecretKey | None = None
+        self.rlk: torch.Tensor | None = None      # prepared relinearisation key
+        self.ksk: torch.Tensor | None = None      # raw [L, 2, L+1, N]
+        self._scratch: torch.Tensor | None = None
+
+    # ---------------------------------------------------------------- sampling
+    def _sid(self) -> int:
+        self._stream_id += 1
+        return self._stream_id
+
+    def uniform(self, n_polys: int, n_limbs: int, prime_begin: int = 0) -> torch.Tensor:
+        return ops.sample_uniform(self.ctx, n_polys, n_limbs, self.seed, self._sid(), prime_begin,
+                                  device=self.device)
+
+    def dgauss(self, shape) -> torch.Tensor:
+        return ops.sample_dgauss(shape, self.params.sigma, self.seed, self._sid(), device=self.device)
+
+    # ---------------------------------------------------------------- keys
+    def keygen(self, s_coef: torch.Tensor | None = None) -> SecretKey:
+        n, k = self.n, len(self.params.primes)
+        if s_coef is None:
+            s_coef = ops.sample_ternary((n,), self.seed, self._sid(), device=self.device)
+        s_coef = s_coef.to(self.device, torch.int64).contiguous()
+        s_eval = self._int_poly_to_eval(s_coef, k)
+        self.sk = SecretKey(s_coef, s_eval)
+        self._make_relin_key()
+        return self.sk
+
+    def _int_poly_to_eval(self, x: torch.Tensor, n_limbs: int) -> torch.Tensor:
+        """Small signed integer polynomial [N] -> evaluation domain [n_limbs, N]."""
+        rows = []
+        for i in range(n_limbs):
+            q = self.params.primes[i]
+            rows.append(torch.remainder(x, q))
+        t = torch.stack(rows).contiguous().view(U64)
+        ops.ntt(self.ctx, t, prime_begin=0, n_limbs=n_limbs)
+        return t
+
+    def _make_relin_key(self, a: torch.Tensor | None = None, e: torch.Tensor | None = None):
+        """ksk[j] = Enc_s over all L+1 primes of m_j with m_j[i] = delta_ij (P mod q_j) s^2."""
+        L = self.params.levels
+        n = self.n
+        s = self.sk.s_eval
+        s2 = ops.pointwise_mul(self.ctx, s, s, n_limbs=L + 1)
+        P = self.params.special
+        if a is None:
+            a = self.uniform(L, L + 1)
+        if e is None:
+            e = self.dgauss((L, n))
+        m = torch.zeros((L, L + 1, n), dtype=U64, device=self.device)
+        for j in range(L):
+            qj = self.params.q[j]
+            c = torch.full((1, n), P % qj, dtype=torch.int64, device=self.device).view(U64)
+            m[j, j] = ops.pointwise_mul(self.ctx, s2[j:j + 1].contiguous(), c, prime_begin=j, n_limbs=1)[0]
+        self.ksk = ops.encrypt(self.ctx, m, s, a.contiguous(), e.contiguous())
+        self.rlk = ops.relin_key_prepare(self.ctx, self.ksk)
+        self._key_samples = (a, e)
+
+    # ---------------------------------------------------------------- encode / encrypt
+    def encode(self, values, level: int | None = None, scale: float | None = None) -> torch.Tensor:
+        """values: [C, n_slots] real or complex (numpy or tensor) -> plaintext [C, level, N]."""
+        level = level or self.params.levels
+        scale = scale or self.params.scale
+        v = torch.as_tensor(np.asarray(values) if not torch.is_tensor(values) else values)
+        v = v.to(self.device).to(torch.complex128)
+        if v.dim() == 1:
+            v = v[None]
+        return ops.encode(self.ctx, v.contiguous(), level, scale)
+
+    def encrypt_values(self, values, level: int | None = None, scale: float | None = None) -> Ciphertext:
+        level = level or self.params.levels
+        scale = scale or self.params.scale
+        m = self.encode(values, level, scale)
+        C = m.shape[0]
+        a = self.uniform(C, level)
+        e = self.dgauss((C, self.n))
+        return Ciphertext(ops.encrypt(self.ctx, m, self.sk.s_eval, a, e), scale)
+
+    def decrypt_coef(self, ct: Ciphertext) -> torch.Tensor:
+        return ops.decrypt(self.ctx, ct.data, self.sk.s_eval)
+
+    def decrypt_values(self, ct: Ciphertext, n_slots: int | None = None) -> torch.Tensor:
+        n_slots = n_slots or self.n // 2
+        return ops.decode(self.ctx, self.decrypt_coef(ct), n_slots, ct.scale)
+
+    # ---------------------------------------------------------------- evaluation
+    def mul_relin_rescale(self, a: Ciphertext, b: Ciphertext, out: torch.Tensor | None = None) -> Ciphertext:
+        level = a.level
+        need = ops.ct_mul_scratch_bytes(self.ctx, a.count, level)
+        if self._scratch is None or self._scratch.numel() * 8 < need:
+            self._scratch = torch.empty((need + 7) // 8, dtype=U64, device=self.device)
+        r = ops.ct_mul_relin_rescale(self.ctx, a.data, b.data, self.rlk, scratch=self._scratch, out=out)
+        return Ciphertext(r, a.scale * b.scale / self.params.q[level - 1])
+
+    def rescale(self, ct: Ciphertext) -> Ciphertext:
+        C, two, level, n = ct.data.shape
+        r = ops.rescale_rns(self.ctx, ct.data.reshape(C * 2, level, n)).reshape(C, 2, level - 1, n)
+        return Ciphertext(r, ct.scale / self.params.q[level - 1])
+
+    def dare_refresh(self, ct: Ciphertext, level_out: int | None = None, shift_bits: int = 0) -> Ciphertext:
+        """Decrypt-reencrypt: fresh noise, modulus restored to level_out, scale / 2^shift."""
+        level_out = level_out or self.params.levels
+        C = ct.count
+        a = self.uniform(C, level_out)
+        e = self.dgauss((C, self.n))
+        r = ops.dare_refresh(self.ctx, ct.data, self.sk.s_eval, a, e, level_out, shift_bits)
+        return Ciphertext(r, ct.scale / float(2 ** shift_bits))

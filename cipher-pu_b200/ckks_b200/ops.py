@@ -151,3 +151,143 @@ def ct_mul_relin_rescale(ctx: Context, ct_a: torch.Tensor, ct_b: torch.Tensor,
     _lib.call("ckks_ct_mul_relin_rescale", ctx.handle, _p(out), _p(ct_a), _p(ct_b), _p(key_prepared),
               n_ct, level, _p(scratch), scratch.numel() * scratch.element_size(), _stream())
     return out
+
+
+# ------------------------------------------------------------------ encode / decode
+def _f64(t: torch.Tensor) -> int:
+    if not t.is_cuda or t.dtype not in (torch.float64, torch.complex128) or not t.is_contiguous():
+        raise ValueError("expected a contiguous CUDA float64 / complex128 tensor")
+    return t.data_ptr()
+
+
+def encode(ctx: Context, slots: torch.Tensor, level: int, scale: float) -> torch.Tensor:
+    """slots: complex128 [P, n_slots] (CUDA) -> plaintext [P, level, N] (evaluation domain)."""
+    slots = slots.to(torch.complex128).contiguous()
+    P, ns = slots.shape
+    out = torch.empty((P, level, ctx.n), dtype=U64, device=slots.device)
+    _lib.call("ckks_encode", ctx.handle, _p(out), _f64(slots), P, ns, level, float(scale), _stream())
+    return out
+
+
+def decode(ctx: Context, coef: torch.Tensor, n_slots: int, scale: float) -> torch.Tensor:
+    """coef: [P, level, N] coefficient-domain residues -> complex128 [P, n_slots]."""
+    P, level, n = coef.shape
+    out = torch.empty((P, n_slots), dtype=torch.complex128, device=coef.device)
+    _lib.call("ckks_decode", ctx.handle, _f64(out), _p(coef), P, n_slots, level, float(scale), _stream())
+    return out
+
+
+def decrypt(ctx: Context, ct: torch.Tensor, s_eval: torch.Tensor) -> torch.Tensor:
+    """ct [C, 2, level, N] -> coefficient residues [C, level, N] of c0 + c1 s."""
+    C_, two, level, n = ct.shape
+    out = torch.empty((C_, level, n), dtype=U64, device=ct.device)
+    _lib.call("ckks_decrypt", ctx.handle, _p(out), _p(ct), _p(s_eval), C_, level, _stream())
+    return out
+
+
+def encrypt(ctx: Context, m_eval: torch.Tensor | None, s_eval: torch.Tensor, a: torch.Tensor,
+            e: torch.Tensor) -> torch.Tensor:
+    """a [C, level, N] uniform; e [C, N] int64; m_eval [C, level, N] or None -> ct [C, 2, level, N]."""
+    C_, level, n = a.shape
+    out = torch.empty((C_, 2, level, n), dtype=U64, device=a.device)
+    if e.dtype != torch.int64 or not e.is_contiguous():
+        raise ValueError("e must be a contiguous int64 tensor")
+    _lib.call("ckks_encrypt", ctx.handle, _p(out), _p(m_eval) if m_eval is not None else None,
+              _p(s_eval), _p(a), e.data_ptr(), C_, level, _stream())
+    return out
+
+
+def dare_refresh(ctx: Context, ct: torch.Tensor, s_eval: torch.Tensor, a: torch.Tensor,
+                 e: torch.Tensor, level_out: int, shift_bits: int = 0,
+                 scratch: torch.Tensor | None = None) -> torch.Tensor:
+    C_, two, level_in, n = ct.shape
+    need = int(_lib.raw("ckks_dare_scratch_bytes")(ctx.handle, C_, level_in))
+    if scratch is None or scratch.numel() * 8 < need:
+        scratch = torch.empty((need + 7) // 8, dtype=U64, device=ct.device)
+    out = torch.empty((C_, 2, level_out, n), dtype=U64, device=ct.device)
+    _lib.call("ckks_dare_refresh", ctx.handle, _p(out), _p(ct), _p(s_eval), _p(a), e.data_ptr(), C_,
+              level_in, level_out, int(shift_bits), _p(scratch), scratch.numel() * 8, _stream())
+    return out
+
+
+def noise_energy(x: torch.Tensor, q: int) -> list[int]:
+    """Exact sum of min(c, q-c)^2 per row of x [R, L] -> Python ints."""
+    R, L = x.shape
+    out = torch.empty((R, 2), dtype=U64, device=x.device)
+    _lib.call("ckks_noise_energy", _p(out), _p(x), R, L, int(q), _stream())
+    h = to_host(out)
+    return [int(lo) + (int(hi) << 64) for lo, hi in h]
+
+
+def snr_sums(dec: torch.Tensor, ref: torch.Tensor) -> torch.Tensor:
+    """Per row (signal energy, error energy) of complex or real float64 tensors [R, L]."""
+    cplx = dec.is_complex()
+    R, L = dec.shape
+    out = torch.empty((R, 2), dtype=torch.float64, device=dec.device)
+    _lib.call("ckks_snr_sums", out.data_ptr(), dec.contiguous().data_ptr(), ref.contiguous().data_ptr(),
+              R, L, int(cplx), _stream())
+    return out
+
+
+def block_sparse_mask(w: torch.Tensor, block: int, threshold: float):
+    w = w.to(torch.float64).contiguous()
+    out = torch.empty_like(w)
+    keep = torch.empty(w.numel() // block, dtype=torch.uint8, device=w.device)
+    _lib.call("ckks_block_sparse_mask", out.data_ptr(), keep.data_ptr(), w.data_ptr(), w.numel(), block,
+              float(threshold), _stream())
+    return out, keep
+
+
+def block_post_process(x: torch.Tensor, q: int, block: int, threshold: int, use_approx: bool = True):
+    R, L = x.shape
+    out = torch.empty_like(x)
+    skipped = torch.empty(R, dtype=torch.int32, device=x.device)
+    _lib.call("ckks_block_post_process", _p(out), skipped.data_ptr(), _p(x), R, L, block, int(q),
+              int(threshold), int(use_approx), _stream())
+    return out, skipped
+
+
+def _primes_arr(primes):
+    import ctypes as C
+    arr = (C.c_uint64 * len(primes))(*[int(p) for p in primes])
+    return arr
+
+
+def rns_split(primes, x_words: torch.Tensor, centered: bool = False) -> torch.Tensor:
+    """x_words [n, W] little-endian integers -> residues [k, n]."""
+    n, W = x_words.shape
+    out = torch.empty((len(primes), n), dtype=U64, device=x_words.device)
+    _lib.call("ckks_rns_split", _primes_arr(primes), len(primes), _p(out), _p(x_words), n, W,
+              int(centered), _stream())
+    return out
+
+
+def rns_merge(primes, residues: torch.Tensor, words: int, centered: bool = False) -> torch.Tensor:
+    k, n = residues.shape
+    out = torch.empty((n, words), dtype=U64, device=residues.device)
+    _lib.call("ckks_rns_merge", _primes_arr(primes), len(primes), _p(out), _p(residues), n, words,
+              int(centered), _stream())
+    return out
+
+
+# ------------------------------------------------------------------ sampling
+def sample_uniform(ctx: Context, n_polys: int, n_limbs: int, seed: int, stream_id: int,
+                   prime_begin: int = 0, device=None) -> torch.Tensor:
+    out = torch.empty((n_polys, n_limbs, ctx.n), dtype=U64, device=device or "cuda")
+    _lib.call("ckks_sample_uniform", ctx.handle, _p(out), n_polys, prime_begin, n_limbs,
+              int(seed) & (2 ** 64 - 1), int(stream_id) & (2 ** 64 - 1), _stream())
+    return out
+
+
+def sample_ternary(shape, seed: int, stream_id: int, device=None) -> torch.Tensor:
+    out = torch.empty(shape, dtype=torch.int64, device=device or "cuda")
+    _lib.call("ckks_sample_ternary", out.data_ptr(), out.numel(), int(seed) & (2 ** 64 - 1),
+              int(stream_id) & (2 ** 64 - 1), _stream())
+    return out
+
+
+def sample_dgauss(shape, sigma: float, seed: int, stream_id: int, device=None) -> torch.Tensor:
+    out = torch.empty(shape, dtype=torch.int64, device=device or "cuda")
+    _lib.call("ckks_sample_dgauss", out.data_ptr(), out.numel(), float(sigma), int(seed) & (2 ** 64 - 1),
+              int(stream_id) & (2 ** 64 - 1), _stream())
+    return out

@@ -10,8 +10,10 @@
  *  - Plain C: no torch or CUDA types in signatures.  `stream` is a
  *    cudaStream_t passed as void* (NULL = legacy default stream).
  *  - All data pointers are DEVICE pointers owned by the caller; calls are
- *    stream-ordered and never synchronise the host.  The only allocating
- *    calls are ckks_ctx_create / ckks_ctx_destroy.
+ *    stream-ordered and never synchronise the host.  Device memory is
+ *    allocated only by ckks_ctx_create (tables) and, once per thread and
+ *    device, by ckks_sample_dgauss (its CDF table); every other entry uses
+ *    caller buffers.
  *  - Polynomials are uint64 coefficient arrays, limb-major:
  *    [batch][poly][limb][N]; limb l of a call with prime_begin b uses the
  *    context prime b + l.  Values are canonical residues in [0, q).
@@ -190,6 +192,168 @@ size_t ckks_ct_mul_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level);
 int ckks_ct_mul_relin_rescale(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
                               const uint64_t* ct_b, const uint64_t* key, int n_ct, int level,
                               void* scratch, size_t scratch_bytes, void* stream);
+
+/*
+ * CKKS slot encoding (FP64 canonical embedding, scale Delta):
+ * slots [n_polys][n_slots] complex doubles (re, im interleaved), n_slots <=
+ * N/2; slot k is the evaluation at Phi^(2k+1), Phi = exp(i pi / N), with its
+ * conjugate at N-1-k; coefficients round(Delta * m) -> out [n_polys][level][N]
+ * in the evaluation domain.  Replaces scripts/verify_multi_slot_simd.py:75
+ * encode (and :42 neg_ifft) at production N (log_n <= 13).
+ */
+int ckks_encode(const ckks_ctx* ctx, uint64_t* out, const double* slots, int n_polys, int n_slots,
+                int level, double scale, void* stream);
+
+/*
+ * Decoding: in [n_polys][level][N] COEFFICIENT-domain residues (e.g. the
+ * output of ckks_decrypt) -> balanced CRT to the centred integer -> / scale ->
+ * slots [n_polys][n_slots] complex.  Replaces scripts/verify_multi_slot_simd.py:88
+ * decode (and :32 neg_fft).
+ */
+int ckks_decode(const ckks_ctx* ctx, double* slots, const uint64_t* in_coef, int n_polys,
+                int n_slots, int level, double scale, void* stream);
+
+/*
+ * Decryption: ct [n_ct][2][level][N] (evaluation domain) -> out
+ * [n_ct][level][N] coefficient-domain residues of c0 + c1 s.  s_eval: the
+ * secret in the evaluation domain, [n_primes][N] over all context primes.
+ * Replaces scripts/exp_e11_ckks_e2e_real.py:90 rlwe_decrypt and
+ * scripts/exp_e24_rotation_bootstrap.py:126 decrypt_exact_int (their
+ * (b, a) with b = a s + e + m equals (c0, c1) = (b, -a) here).
+ */
+int ckks_decrypt(const ckks_ctx* ctx, uint64_t* out_coef, const uint64_t* ct,
+                 const uint64_t* s_eval, int n_ct, int level, void* stream);
+
+/*
+ * Encryption under the secret: c1 = a, c0 = -a s + NTT(e) + m over
+ * q_0..q_{level-1}.  m_eval [n_ct][level][N] plaintext (evaluation domain, or
+ * NULL for zero), a [n_ct][level][N] uniform residues, e [n_ct][N] small
+ * signed errors.  Host samplers provide a and e (seeded).  Replaces
+ * scripts/exp_e11_ckks_e2e_real.py:72 rlwe_encrypt and
+ * scripts/exp_e24_rotation_bootstrap.py:209 rlwe_encrypt_mint.
+ */
+int ckks_encrypt(const ckks_ctx* ctx, uint64_t* out, const uint64_t* m_eval,
+                 const uint64_t* s_eval, const uint64_t* a, const int64_t* e, int n_ct, int level,
+                 void* stream);
+
+/*
+ * DARE refresh (decrypt -> re-encrypt): the centred integer m_int + e_old of
+ * each ciphertext at level_in (balanced CRT over its limbs) is divided by
+ * 2^shift_bits with rounding (0 keeps the scale) and encrypted afresh with a,
+ * e at level_out (which may exceed level_in: the modulus is restored).
+ * ct [n_ct][2][level_in][N] -> out [n_ct][2][level_out][N];
+ * a [n_ct][level_out][N]; e [n_ct][N]; scratch >= ckks_dare_scratch_bytes.
+ * With shift_bits > 0 the integer must satisfy |x| < 2^127.
+ * Replaces scripts/exp_e24_rotation_bootstrap.py:287 reencrypt.
+ */
+size_t ckks_dare_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level_in);
+int ckks_dare_refresh(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct, const uint64_t* s_eval,
+                      const uint64_t* a_fresh, const int64_t* e_fresh, int n_ct, int level_in,
+                      int level_out, int shift_bits, void* scratch, size_t scratch_bytes,
+                      void* stream);
+
+/*
+ * Noise monitor: per row of row_len residues mod q, the exact sum of
+ * min(c, q - c)^2 as a 128-bit integer out_sum[2*row] (low) / [2*row+1]
+ * (high); E = sum / row_len.  Replaces rtl/m4/noise_monitor.sv:42-129 and
+ * scripts/verify_m4_h_multilayer.py:162 noise_monitor_energy.
+ */
+int ckks_noise_energy(uint64_t* out_sum, const uint64_t* in, int n_rows, int row_len, uint64_t q,
+                      void* stream);
+
+/*
+ * Slot SNR sums: per row, out[2*row] = sum |ref|^2, out[2*row+1] =
+ * sum |dec - ref|^2 over row_len values (complex when complex_vals != 0).
+ * SNR_dB = 10 log10(out0 / out1).  The decrypt-based SNR probe of the gear
+ * loop (the reference estimates r_hat from decrypted vs plaintext values,
+ * scripts/exp_e11_ckks_e2e_real.py:169 estimate_r_hat).
+ */
+int ckks_snr_sums(double* out, const double* dec, const double* ref, int n_rows, int row_len,
+                  int complex_vals, void* stream);
+
+/*
+ * Block sparsity of a weight array: flat blocks of `block` weights whose
+ * max |w| < threshold are zeroed; keep[b] (may be NULL) = 1 for kept blocks.
+ * Replaces scripts/exp_e10_sparsity_sweep_v2.py:102 apply_block_sparse_mask
+ * and rtl/m4/block_sparse_mask.sv.
+ */
+int ckks_block_sparse_mask(double* out, uint8_t* keep, const double* w, int64_t n, int block,
+                           double threshold, void* stream);
+
+/*
+ * Output block skip of the approximate multiplier: per row, blocks of
+ * `block` residues with max min(x, q - x) < threshold are zeroed when
+ * use_approx and threshold != 0; skipped[row] = number of zeroed blocks.
+ * Replaces scripts/verify_m4_d_approx_mult.py:50 post_process_block and
+ * rtl/m4/approx_poly_mult.sv:1-44 (block mode).
+ */
+int ckks_block_post_process(uint64_t* out, int32_t* skipped, const uint64_t* in, int n_rows,
+                            int row_len, int block, uint64_t q, uint64_t threshold, int use_approx,
+                            void* stream);
+
+/*
+ * RNS split / merge over up to 8 primes (< 2^62, given in host memory).
+ * split: in [n][words] little-endian integers (two's complement when
+ *        centered) -> out [n_primes][n] residues.
+ * merge: in [n_primes][n] residues -> out [n][words] integers via Garner CRT,
+ *        in [0, M) or, when centered, the representative in (-M/2, M/2]
+ *        (two's complement).
+ * Replace rtl/m5/rns_split.sv:58-62 and rtl/m5/rns_merge.sv:84-135
+ * (p1/p2/p3 = 77309411329, 206158430209, 2061584302081; M 115 bits).
+ */
+int ckks_rns_split(const uint64_t* primes, int n_primes, uint64_t* out, const uint64_t* in,
+                   int64_t n, int words, int centered, void* stream);
+int ckks_rns_merge(const uint64_t* primes, int n_primes, uint64_t* out, const uint64_t* in,
+                   int64_t n, int words, int centered, void* stream);
+
+/*
+ * Energy-threshold gear controller (host state machine, no device work):
+ * energy >= thresh[0] -> gear 0, >= thresh[1] -> 1, >= thresh[2] -> 2, else 3;
+ * with hysteresis an upgrade (higher gear) takes effect after hyst_cnt
+ * agreeing candidates while a downgrade is immediate; manual override.
+ * Reset state: gear 3.  Replaces rtl/m4/adaptive_gear_ctrl.sv:43-99.
+ */
+typedef struct ckks_gear_ctrl {
+  uint64_t thresh_lo[3], thresh_hi[3];
+  int hyst_cnt, gear, counter, candidate;
+} ckks_gear_ctrl;
+int ckks_gear_ctrl_init(ckks_gear_ctrl* g, const uint64_t thresh_lo[3], const uint64_t thresh_hi[3],
+                        int hyst_cnt);
+int ckks_gear_ctrl_raw(const ckks_gear_ctrl* g, uint64_t energy_lo, uint64_t energy_hi);
+int ckks_gear_ctrl_flush(ckks_gear_ctrl* g, uint64_t energy_lo, uint64_t energy_hi,
+                         int hysteresis_en, int manual_en, int manual_gear);
+
+/*
+ * Seeded counter-based sampling (Philox4x32-10): element i of stream
+ * `stream_id` depends only on (seed, stream_id, i).
+ *  uniform: out [n_polys][n_limbs][N] residues uniform mod the limb primes;
+ *  ternary: out[n] in {-1, 0, 1} uniform (the secret distribution);
+ *  dgauss:  out[n] discrete Gaussian of width sigma (<= 16), tail cut at
+ *           12 sigma (allocates a small CDF table once per thread and device).
+ * The reference samples with numpy / random (scripts/exp_e33_real_ciphertext.py:75
+ * dgauss, :153 ternary; scripts/exp_e11_ckks_e2e_real.py:72 uniform a).
+ */
+int ckks_sample_uniform(const ckks_ctx* ctx, uint64_t* out, int n_polys, int prime_begin,
+                        int n_limbs, uint64_t seed, uint64_t stream_id, void* stream);
+int ckks_sample_ternary(int64_t* out, int64_t n, uint64_t seed, uint64_t stream_id, void* stream);
+int ckks_sample_dgauss(int64_t* out, int64_t n, double sigma, uint64_t seed, uint64_t stream_id,
+                       void* stream);
+
+/*
+ * Encrypted linear layer with plaintext integer weights and 4x4 block
+ * sparsity: out[o] = sum_f w[o][f] * in[f] (+ bias[o] on component 0), exact
+ * mod every limb prime (< 2^47).  in [n_in][2][level][N], out
+ * [n_out][2][level][N] (evaluation domain); w int32 [n_out][n_in] with
+ * |w| < 2^24; bias int64 [n_out] or NULL; block_keep uint8
+ * [ceil(n_out/4)][ceil(n_in/4)] (1 = compute the 4x4 block) or NULL = dense;
+ * n_in <= 1024.  Zero blocks are skipped, so the work scales with the kept
+ * fraction.  Replaces the encrypted FC layer of
+ * scripts/exp_e11_ckks_e2e_real.py:142 encrypted_linear_layer and
+ * rtl/m4/fc_layer_e2e.sv with slot-packed (SIMD over samples) ciphertexts.
+ */
+int ckks_linear_plain_weights(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in,
+                              const int32_t* w, const int64_t* bias, const uint8_t* block_keep,
+                              int n_out, int n_in, int level, void* stream);
 
 /* Size of the static device scratch used by ckks_ct_mul_relin_rescale_noalloc. */
 #define CKKS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
