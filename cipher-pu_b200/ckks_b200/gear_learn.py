@@ -1,0 +1,293 @@
+"""Learned gear controller: features, trace generation, training (on the GPU
+with the library's own forward / backward / Adam kernels), checkpointing and
+the two controllers compared by the encrypted-inference benchmark.
+
+Trace: one neuron of one encrypted layer evaluation.  Features (16, gear
+independent except the per-gear sparsity terms) describe the neuron's
+weights, the layer input statistics and the ciphertext level / scale;
+targets are the neuron's measured output SNR (dB, FP64 gear-0 layer as the
+reference) at each of the four gears.  The network predicts all four at
+once; the controller picks the sparsest gear predicted to meet the target and
+runs the decrypt-based SNR probe only when the prediction is within the
+uncertainty band of the target.
+
+The plain controller is the reference's rule (rtl/m4/adaptive_gear_ctrl.sv:
+62-99): downgrade at once when the measured SNR misses the target, upgrade
+one gear after HYST_CNT consecutive qualifying measurements, reset to gear 3,
+and a probe after every layer of every batch.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib
+from .gear import GEAR_SPARSITY
+from .mlp import EncryptedMLP, Layer, apply_keep, block_norms, gear_keep, make_block_sparse
+
+N_FEAT = 16
+N_GEAR = 4
+SCHEMA = 1
+SNR_CLIP = (-10.0, 120.0)
+
+
+# ------------------------------------------------------------------ features
+def neuron_features(W: np.ndarray, b: np.ndarray, keeps: list, x_mean: float, x_std: float,
+                    x_ms: float, act: str, level: int, scale: float) -> np.ndarray:
+    O, F = W.shape
+    row_e = (W ** 2).sum(1) + 1e-30
+    rb = np.arange(O) // 4
+    nz_blocks = (block_norms(W) > 0).sum(1).astype(np.float64) + 1e-9
+    feats = np.zeros((O, N_FEAT), dtype=np.float64)
+    feats[:, 0] = math.log2(F) / 10.0
+    feats[:, 1] = x_mean
+    feats[:, 2] = x_std
+    feats[:, 3] = math.log10(x_ms + 1e-12) / 4.0
+    mu = W @ np.full(F, x_mean) + b
+    feats[:, 4] = np.abs(mu) / (np.sqrt(row_e * x_ms) + 1e-12)
+    for g, k in enumerate(keeps):
+        Wg = apply_keep(W, k)
+        dropped = np.clip(1.0 - (Wg ** 2).sum(1) / row_e, 0.0, 1.0)
+        feats[:, 5 + g] = np.log10(dropped + 1e-12) / 12.0 + 1.0
+        feats[:, 9 + g] = k.sum(1)[rb] / nz_blocks[rb]
+    feats[:, 13] = 1.0 if act == "square" else 0.0
+    feats[:, 14] = level / 8.0
+    feats[:, 15] = math.log2(scale) / 64.0
+    return feats
+
+
+def layer_features(m: EncryptedMLP, li: int, x_in: np.ndarray | None, stats: dict | None, level: int,
+                   scale: float) -> np.ndarray:
+    L = m.layers[li]
+    if stats is None:
+        stats = {"mean": float(x_in.mean()), "std": float(x_in.std()), "ms": float((x_in ** 2).mean())}
+    return neuron_features(L.W, L.b, L.keeps_np, stats["mean"], stats["std"], stats["ms"], L.act, level,
+                           scale)
+
+
+# ------------------------------------------------------------------ network
+class GearNet:
+    """The 16 -> 64 -> 64 -> 4 predictor on the GPU (library kernels)."""
+
+    def __init__(self, params: np.ndarray | None = None, seed: int = 0, device=None):
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        self.n_params = int(_lib.raw("ckks_gear_mlp_param_count")())
+        if params is None:
+            from_init = _default_init(seed)
+            params = from_init
+        self.p = torch.as_tensor(np.asarray(params, dtype=np.float32)).to(self.device).contiguous()
+        self.mu = np.zeros(N_FEAT)
+        self.sd = np.ones(N_FEAT)
+
+    def _norm(self, X: np.ndarray) -> torch.Tensor:
+        Z = (np.asarray(X, dtype=np.float64) - self.mu) / self.sd
+        return torch.from_numpy(Z.astype(np.float32)).to(self.device).contiguous()
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        """features [B, 16] -> predicted SNR dB [B, 4]."""
+        x = self._norm(X)
+        y = torch.empty((x.shape[0], N_GEAR), dtype=torch.float32, device=self.device)
+        _lib.call("ckks_gear_mlp_forward", self.p.data_ptr(), x.data_ptr(), y.data_ptr(), None, x.shape[0],
+                  torch.cuda.current_stream().cuda_stream)
+        return y.cpu().numpy().astype(np.float64) * 100.0
+
+    def fit(self, X: np.ndarray, T: np.ndarray, epochs: int = 30, batch: int = 1024, lr: float = 2e-3,
+            seed: int = 0, val_frac: float = 0.1) -> dict:
+        X = np.asarray(X, dtype=np.float64)
+        T = np.clip(np.asarray(T, dtype=np.float64), *SNR_CLIP) / 100.0
+        self.mu = X.mean(0)
+        self.sd = X.std(0) + 1e-6
+        rng = np.random.default_rng(seed)
+        idx = rng.permutation(len(X))
+        nv = int(len(X) * val_frac)
+        va, tr = idx[:nv], idx[nv:]
+        Xd = self._norm(X)
+        Td = torch.from_numpy(T.astype(np.float32)).to(self.device)
+        m = torch.zeros_like(self.p)
+        v = torch.zeros_like(self.p)
+        grad = torch.empty_like(self.p)
+        y = torch.empty((batch, N_GEAR), dtype=torch.float32, device=self.device)
+        cache = torch.empty((batch, 128), dtype=torch.float32, device=self.device)
+        dcache = torch.empty((batch, 132), dtype=torch.float32, device=self.device)
+        st = torch.cuda.current_stream().cuda_stream
+        step = 0
+        hist = []
+        for ep in range(epochs):
+            perm = torch.from_numpy(rng.permutation(tr)).to(self.device)
+            for s in range(0, len(tr) - batch + 1, batch):
+                bi = perm[s:s + batch]
+                xb = Xd[bi].contiguous()
+                tb = Td[bi].contiguous()
+                _lib.call("ckks_gear_mlp_forward", self.p.data_ptr(), xb.data_ptr(), y.data_ptr(),
+                          cache.data_ptr(), batch, st)
+                _lib.call("ckks_gear_mlp_backward", self.p.data_ptr(), xb.data_ptr(), cache.data_ptr(),
+                          y.data_ptr(), tb.data_ptr(), None, grad.data_ptr(), dcache.data_ptr(), batch, st)
+                step += 1
+                lr_t = lr * 0.5 * (1 + math.cos(math.pi * ep / max(1, epochs)))
+                _lib.call("ckks_gear_mlp_adam", self.p.data_ptr(), grad.data_ptr(), m.data_ptr(),
+                          v.data_ptr(), step, float(lr_t), 0.9, 0.999, 1e-8, st)
+            pv = self.predict(X[va])
+            hist.append(float(np.sqrt(((pv - T[va] * 100.0) ** 2).mean())))
+        return {"val_rmse_db": hist, "train": len(tr), "val": nv, "steps": step}
+
+    def save(self, path):
+        np.savez(path, schema=SCHEMA, params=self.p.cpu().numpy(), mu=self.mu, sd=self.sd)
+
+    @staticmethod
+    def load(path, device=None) -> "GearNet":
+        z = np.load(path)
+        if int(z["schema"]) != SCHEMA:
+            raise ValueError("gear network checkpoint schema mismatch")
+        g = GearNet(z["params"], device=device)
+        g.mu, g.sd = z["mu"], z["sd"]
+        return g
+
+
+def _default_init(seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    parts = [rng.standard_normal((64, 16)) * math.sqrt(2 / 16), np.zeros(64),
+             rng.standard_normal((64, 64)) * math.sqrt(2 / 64), np.zeros(64),
+             rng.standard_normal((4, 64)) * math.sqrt(1 / 64), np.zeros(4)]
+    return np.concatenate([p.reshape(-1) for p in parts]).astype(np.float32)
+
+
+# ------------------------------------------------------------------ traces
+def random_layer(rng, F: int, O: int, act: str, base_sparsity: float) -> Layer:
+    W = rng.standard_normal((O, F)) / math.sqrt(F)
+    W = make_block_sparse(W, base_sparsity, int(rng.integers(1 << 30)))
+    b = rng.standard_normal(O) * 0.1
+    return Layer(W, b, act)
+
+
+def gen_traces(ev, n_traces: int, seed: int = 0, batch: int = 256, progress=None) -> tuple:
+    """Run random encrypted layers at all four gears; one trace per neuron."""
+    rng = np.random.default_rng(seed)
+    Xs, Ts = [], []
+    total = 0
+    while total < n_traces:
+        F = int(rng.choice([128, 256, 512, 784]))
+        O = int(rng.choice([16, 32, 64, 128]))
+        act = "square" if rng.random() < 0.7 else "none"
+        L = random_layer(rng, F, O, act, float(rng.choice([0.25, 0.5, 0.75])))
+        m = EncryptedMLP(ev, [L])
+        lo, hi = sorted(rng.uniform(0.0, 1.5, 2))
+        x = rng.uniform(lo, hi + 0.05, (batch, F))
+        X = m.encrypt_inputs(x)
+        ref = x @ L.W.T + L.b
+        if act == "square":
+            ref = ref * ref
+        T = np.zeros((O, N_GEAR))
+        for g in range(N_GEAR):
+            Y = m.linear(X, 0, g)
+            if act == "square":
+                Y = m.square(Y)
+            d = m.decrypt(Y, batch)                       # [O, B]
+            err = ((d - ref.T) ** 2).sum(1)
+            sig = (ref.T ** 2).sum(1) + 1e-300
+            T[:, g] = 10 * np.log10(sig / np.maximum(err, 1e-300))
+        Xs.append(layer_features(m, 0, x, None, X.level, X.scale))
+        Ts.append(T)
+        total += O
+        if progress:
+            progress(total)
+    return np.concatenate(Xs)[:n_traces], np.concatenate(Ts)[:n_traces]
+
+
+# ------------------------------------------------------------------ controllers
+def layer_snr_from_neurons(snr_db: np.ndarray, sig_weight: np.ndarray | None = None) -> np.ndarray:
+    """[O, G] per-neuron SNR -> [G] layer SNR (signal-weighted NSR average)."""
+    nsr = 10.0 ** (-np.clip(np.asarray(snr_db), *SNR_CLIP) / 10.0)
+    w = np.ones(nsr.shape[0]) if sig_weight is None else sig_weight
+    return -10 * np.log10((w[:, None] * nsr).sum(0) / w.sum())
+
+
+class PlainController:
+    """Probe after every layer; downgrade at once when the SNR misses the
+    target, upgrade one gear after `hyst` consecutive measurements at least
+    `margin` dB above target; reset gear 3."""
+
+    def __init__(self, n_layers: int, target_db: float, margin_db: float = 10.0, hyst: int = 3,
+                 reset_gear: int = 3):
+        self.target, self.margin, self.hyst = target_db, margin_db, hyst
+        self.gear = [reset_gear] * n_layers
+        self.count = [0] * n_layers
+        self.probes = 0
+
+    def choose(self, li, info):
+        return self.gear[li]
+
+    def probe_policy(self, li, g, info):
+        self.probes += 1
+        return True
+
+    def on_probe(self, pr):
+        li = pr.layer
+        if pr.snr_db < self.target:
+            self.gear[li] = max(0, self.gear[li] - 1)
+            self.count[li] = 0
+        elif pr.snr_db >= self.target + self.margin and self.gear[li] < N_GEAR - 1:
+            self.count[li] += 1
+            if self.count[li] > self.hyst:
+                self.gear[li] += 1
+                self.count[li] = 0
+        else:
+            self.count[li] = 0
+
+
+class LearnedController:
+    """Predict each gear's layer SNR from features; take the sparsest gear
+    predicted >= target + margin.  The decrypt-based probe (the plain monitor)
+    stays as judge and fallback: it runs on the first use of a (layer, gear),
+    every `audit_every`-th batch, and whenever the prediction lies within
+    `band_db` of the target; a measurement below the target caps the layer's
+    gear and triggers the recompute."""
+
+    def __init__(self, m: EncryptedMLP, net: GearNet, target_db: float, margin_db: float = 3.0,
+                 band_db: float = 6.0, audit_every: int = 8):
+        self.m, self.net = m, net
+        self.target, self.margin, self.band, self.audit = target_db, margin_db, band_db, audit_every
+        self.cap = [N_GEAR - 1] * len(m.layers)
+        self.pred = {}
+        self.verified = set()
+        self.probes = 0
+        self.stats = {}
+        self.calls = [0] * len(m.layers)
+
+    def set_input_stats(self, li: int, stats: dict):
+        self.stats[li] = stats
+        self.pred.pop(li, None)
+
+    def predicted(self, li: int, info) -> np.ndarray:
+        key = (info["level"], round(math.log2(info["scale"]), 3))
+        hit = self.pred.get(li)
+        if hit is None or hit[0] != key:
+            st = self.stats.get(li) or self.stats.get(0)
+            feats = layer_features(self.m, li, None, st, info["level"], info["scale"])
+            hit = (key, layer_snr_from_neurons(self.net.predict(feats)))
+            self.pred[li] = hit
+        return hit[1]
+
+    def choose(self, li, info):
+        p = self.predicted(li, info)
+        ok = [g for g in range(N_GEAR) if p[g] >= self.target + self.margin and g <= self.cap[li]]
+        return max(ok) if ok else 0
+
+    def probe_policy(self, li, g, info):
+        self.calls[li] += 1
+        p = self.predicted(li, info)
+        need = ((li, g) not in self.verified or abs(p[g] - self.target) < self.band
+                or (self.audit and self.calls[li] % self.audit == 0))
+        if need:
+            self.probes += 1
+        return need
+
+    def on_probe(self, pr):
+        if pr.snr_db < self.target:
+            self.cap[pr.layer] = max(0, pr.gear - 1)
+            self.verified.discard((pr.layer, pr.gear))
+        else:
+            self.verified.add((pr.layer, pr.gear))

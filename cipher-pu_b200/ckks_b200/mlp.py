@@ -151,29 +151,50 @@ class EncryptedMLP:
         return self.ev.decrypt_values(ct, n_slots).real.cpu().numpy()
 
     # ---------------------------------------------------------------- probe
-    def probe(self, li: int, gear: int, out_ct: Ciphertext, x_in: np.ndarray, B: int) -> tuple:
-        """Decrypt the layer output and compare with the FP64 gear-0 layer on x_in."""
+    def _dev_layer(self, L: Layer):
+        if getattr(L, "_Wt", None) is None:
+            L._Wt = torch.from_numpy(np.ascontiguousarray(L.W.T)).to(self.ev.device)
+            L._b = torch.from_numpy(np.asarray(L.b, dtype=np.float64)).to(self.ev.device)
+        return L._Wt, L._b
+
+    def layer_ref(self, li: int, x_in: torch.Tensor) -> torch.Tensor:
+        """FP64 gear-0 layer on the device: x_in [B, F] -> [O, B]."""
         L = self.layers[li]
-        dec = self.ev.decrypt_values(out_ct, B).real              # [O, B] on device
-        ref = torch.from_numpy(x_in).to(self.ev.device) @ torch.from_numpy(L.W.T).to(self.ev.device)
-        ref = (ref + torch.from_numpy(L.b).to(self.ev.device)).T.contiguous()
+        Wt, b = self._dev_layer(L)
+        r = x_in @ Wt + b
         if L.act == "square":
-            ref = ref * ref
-        sums = ops.snr_sums(dec.contiguous(), ref).sum(0).cpu().numpy()
+            r = r * r
+        return r.T.contiguous()
+
+    def probe(self, li: int, gear: int, out_ct: Ciphertext, x_in: torch.Tensor, B: int) -> tuple:
+        """Decrypt the layer output and compare it with the FP64 gear-0 layer
+        evaluated on this layer's (decrypted) input; everything stays on the
+        device except the two energy sums."""
+        dec = self.ev.decrypt_values(out_ct, B).real.contiguous()      # [O, B]
+        ref = self.layer_ref(li, x_in)
+        sums = ops.snr_sums(dec, ref).sum(0).cpu().numpy()
         nsr = float(sums[1] / max(sums[0], 1e-300))
         snr = 10 * math.log10(1.0 / max(nsr, 1e-30))
-        return ProbeResult(li, gear, snr, nsr), dec.T.cpu().numpy()
+        return ProbeResult(li, gear, snr, nsr), dec.T.contiguous()
 
     # ---------------------------------------------------------------- forward
-    def forward(self, x: np.ndarray, choose_gear, on_probe=None, probe_policy=None) -> dict:
+    def forward(self, x: np.ndarray, choose_gear, on_probe=None, probe_policy=None,
+                X: Ciphertext | None = None, fallback_db: float | None = None) -> dict:
         """Run one batch.  choose_gear(layer, info) -> gear; probe_policy(layer,
         gear, info) -> bool decides whether the SNR probe runs (default: always).
-        Returns logits [B, O_last] and the probe records."""
+        X: the batch already encrypted (else it is encrypted here).
+        fallback_db: when a probe measures less than this at a gear > 0, the
+        layer is recomputed at gear 0 before its result is used (the probe is
+        both the judge and the fallback trigger).
+        Returns logits [B, O_last] (numpy), the probe records and the number of
+        recomputed layers."""
         B = x.shape[0]
         t0 = time.perf_counter()
-        X = self.encrypt_inputs(x)
-        x_in = np.asarray(x, dtype=np.float64)   # plaintext input of the current layer, if known
+        if X is None:
+            X = self.encrypt_inputs(x)
+        x_in = torch.from_numpy(np.asarray(x, dtype=np.float64)).to(self.ev.device)
         probes, gears = [], []
+        recomputed = 0
         out = None
         for li, L in enumerate(self.layers):
             info = {"layer": li, "level": X.level, "scale": X.scale, "batch": B}
@@ -182,33 +203,33 @@ class EncryptedMLP:
             last = li == len(self.layers) - 1
             do_probe = True if probe_policy is None else bool(probe_policy(li, g, info))
             if do_probe and x_in is None:            # the probe needs this layer's input
-                x_in = self.decrypt(X, B).T
+                x_in = self.ev.decrypt_values(X, B).real.T.contiguous()
             Y = self.linear(X, li, g)
             if L.act == "square":
                 Y = self.square(Y)
-            if last:
-                vals = self.decrypt(Y, B).T                   # [B, O]
-                if do_probe:
-                    ref = x_in @ L.W.T + L.b
+            vals = None
+            if do_probe:
+                pr, vals = self.probe(li, g, Y, x_in, B)
+                probes.append(pr)
+                if on_probe:
+                    on_probe(pr)
+                if fallback_db is not None and g > 0 and pr.snr_db < fallback_db:
+                    recomputed += 1
+                    gears[-1] = 0
+                    Y = self.linear(X, li, 0)
                     if L.act == "square":
-                        ref = ref * ref
-                    nsr = float(((vals - ref) ** 2).sum() / max((ref ** 2).sum(), 1e-300))
-                    pr = ProbeResult(li, g, 10 * math.log10(1.0 / max(nsr, 1e-30)), nsr)
-                    probes.append(pr)
-                    if on_probe:
-                        on_probe(pr)
-                out = vals
+                        Y = self.square(Y)
+                    vals = None
+            if last:
+                if vals is None:
+                    vals = self.ev.decrypt_values(Y, B).real.T
+                out = vals.cpu().numpy()
             else:
-                x_next = None
-                if do_probe:
-                    pr, x_next = self.probe(li, g, Y, x_in, B)
-                    probes.append(pr)
-                    if on_probe:
-                        on_probe(pr)
                 X = self.refresh(Y)
-                x_in = x_next
+                x_in = vals
         torch.cuda.synchronize()
-        return {"logits": out, "probes": probes, "gears": gears, "seconds": time.perf_counter() - t0}
+        return {"logits": out, "probes": probes, "gears": gears, "recomputed": recomputed,
+                "seconds": time.perf_counter() - t0}
 
 
 def encrypted_linear_demo(x: np.ndarray, W: np.ndarray, b: np.ndarray, log_n: int = 13, levels: int = 3,

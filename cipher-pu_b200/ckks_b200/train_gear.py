@@ -1,0 +1,107 @@
+"""Train the learned gear controller and compare it with the plain one.
+
+    python -m ckks_b200.train_gear train   [--traces 200000] [--epochs 40] [--out PATH]
+    python -m ckks_b200.train_gear compare [--net PATH] [--model mlp|cnn] [--batches 8]
+
+train: generates noise-monitor traces by running random encrypted layers of
+the encrypted-MLP family (N = 2^13, L = 4) at every gear, trains the
+16 -> 64 -> 64 -> 4 network on the GPU with the library's kernels and writes
+the checkpoint (weights, feature normalisation, schema version).
+compare: encrypted inference of a batch stream under the plain controller
+(probe every layer) and the learned one (probe when uncertain), same model,
+same inputs; prints samples/s, logit SNR vs FP64, top-1 agreement, probes.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+DEFAULT_NET = Path(__file__).resolve().parent / "data" / "gear_net.npz"
+
+
+def train(n_traces: int = 200_000, epochs: int = 40, out: Path = DEFAULT_NET, seed: int = 0,
+          log_n: int = 13, levels: int = 4) -> dict:
+    from .evaluator import Evaluator
+    from .gear_learn import GearNet, gen_traces
+    from .params import CkksParams
+    ev = Evaluator(CkksParams.standard(log_n, levels, seed=seed + 100))
+    ev.keygen()
+    t0 = time.perf_counter()
+    X, T = gen_traces(ev, n_traces, seed=seed)
+    t_gen = time.perf_counter() - t0
+    net = GearNet(seed=seed)
+    t1 = time.perf_counter()
+    hist = net.fit(X, T, epochs=epochs, seed=seed)
+    t_fit = time.perf_counter() - t1
+    out = Path(out)
+    out.parent.mkdir(parents=True, exist_ok=True)
+    net.save(out)
+    return {"traces": len(X), "gen_s": t_gen, "fit_s": t_fit, "val_rmse_db": hist["val_rmse_db"][-1],
+            "val_rmse_curve": hist["val_rmse_db"], "checkpoint": str(out)}
+
+
+def compare(net_path: Path = DEFAULT_NET, model: str = "mlp", batches: int = 8, batch: int = 1024,
+            target_db: float = 40.0, seed: int = 0) -> dict:
+    from .evaluator import Evaluator
+    from .gear_learn import GearNet, LearnedController, PlainController
+    from .mlp import EncryptedMLP
+    from .models import cnn_28x28, mlp_784_128_10, run_stream
+    from .params import CkksParams
+    levels = 4 if model == "mlp" else 5
+    ev = Evaluator(CkksParams.standard(13, levels, seed=seed + 7))
+    ev.keygen()
+    layers = mlp_784_128_10(seed) if model == "mlp" else cnn_28x28(seed)
+    m = EncryptedMLP(ev, layers)
+    rng = np.random.default_rng(seed + 1)
+    data = [rng.uniform(0, 1, (batch, 784)) for _ in range(batches)]
+    # warm-up (kernels, contexts)
+    m.forward(data[0][:64], lambda li, info: 0)
+    plain = PlainController(len(layers), target_db)
+    rp = run_stream(m, plain, data, fallback_db=target_db)
+    net = GearNet.load(net_path)
+    learned = LearnedController(m, net, target_db)
+    # input statistics per layer from one calibration pass (probed, counted)
+    cal = m.forward(data[0][:256], lambda li, info: 0)
+    x_in = data[0][:256]
+    for li, L in enumerate(layers):
+        learned.set_input_stats(li, {"mean": float(x_in.mean()), "std": float(x_in.std()),
+                                     "ms": float((x_in ** 2).mean())})
+        h = x_in @ L.W.T + L.b
+        x_in = h * h if L.act == "square" else h
+    learned.probes += len(layers)
+    rl = run_stream(m, learned, data, fallback_db=target_db)
+    return {"model": model, "target_db": target_db, "batch": batch, "batches": batches,
+            "plain": {k: v for k, v in rp.items() if k != "gears"}, "plain_gears": rp["gears"],
+            "learned": {k: v for k, v in rl.items() if k != "gears"}, "learned_gears": rl["gears"],
+            "speedup": rl["samples_per_s"] / rp["samples_per_s"],
+            "snr_gap_db": rl["snr_db"] - rp["snr_db"]}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser()
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    t = sub.add_parser("train")
+    t.add_argument("--traces", type=int, default=200_000)
+    t.add_argument("--epochs", type=int, default=40)
+    t.add_argument("--out", default=str(DEFAULT_NET))
+    c = sub.add_parser("compare")
+    c.add_argument("--net", default=str(DEFAULT_NET))
+    c.add_argument("--model", default="mlp", choices=["mlp", "cnn"])
+    c.add_argument("--batches", type=int, default=8)
+    c.add_argument("--target-db", type=float, default=40.0)
+    a = ap.parse_args(argv)
+    if a.cmd == "train":
+        r = train(a.traces, a.epochs, Path(a.out))
+    else:
+        r = compare(Path(a.net), a.model, a.batches, target_db=a.target_db)
+    print(json.dumps(r, default=float))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -8,7 +8,7 @@
 // so the layer is a modular GEMM over the 2 * level * N coefficient positions.
 // Exactness: each residue x < 2^47 is split x = xh 2^23 + xl, products with
 // |w| < 2^24 are accumulated in signed 64-bit (|sum| < 2^57 for <= 1024
-// inputs), and reduced once per output element.
+// inputs; |sum| < 2^59 for 2048), reduced once per output element.
 //
 // Tiling: one CTA = 16 outputs (four 4-row blocks) x 256 positions, one
 // position per thread; the weight tile and the block-keep mask live in
@@ -19,7 +19,7 @@
 
 constexpr int LIN_OT = 16;     // outputs per CTA
 constexpr int LIN_THREADS = 256;
-constexpr int LIN_MAX_IN = 1024;
+constexpr int LIN_MAX_IN = 2048;
 
 __global__ void __launch_bounds__(LIN_THREADS)
     k_linear(u64* __restrict__ out, const u64* __restrict__ in, const int* __restrict__ w,

@@ -346,7 +346,7 @@ int ckks_sample_dgauss(int64_t* out, int64_t n, double sigma, uint64_t seed, uin
  * [n_out][2][level][N] (evaluation domain); w int32 [n_out][n_in] with
  * |w| < 2^24; bias int64 [n_out] or NULL; block_keep uint8
  * [ceil(n_out/4)][ceil(n_in/4)] (1 = compute the 4x4 block) or NULL = dense;
- * n_in <= 1024.  Zero blocks are skipped, so the work scales with the kept
+ * n_in <= 2048.  Zero blocks are skipped, so the work scales with the kept
  * fraction.  Replaces the encrypted FC layer of
  * scripts/exp_e11_ckks_e2e_real.py:142 encrypted_linear_layer and
  * rtl/m4/fc_layer_e2e.sv with slot-packed (SIMD over samples) ciphertexts.
@@ -354,6 +354,27 @@ int ckks_sample_dgauss(int64_t* out, int64_t n, double sigma, uint64_t seed, uin
 int ckks_linear_plain_weights(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in,
                               const int32_t* w, const int64_t* bias, const uint8_t* block_keep,
                               int n_out, int n_in, int level, void* stream);
+
+/*
+ * Learned gear controller network (no counterpart in the reference, whose
+ * gear logic is thresholds + hysteresis, rtl/m4/adaptive_gear_ctrl.sv): a
+ * 16 -> 64 -> 64 -> 4 FP32 MLP with ReLU hidden layers predicting the
+ * post-layer SNR of each gear.  params: ckks_gear_mlp_param_count() floats
+ * laid out W1[64][16], b1[64], W2[64][64], b2[64], W3[4][64], b3[4].
+ *  forward:  x [batch][16] -> y [batch][4]; cache [batch][128] (hidden
+ *            activations, needed by backward) may be NULL.
+ *  backward: loss = (1/batch) sum mask * (y - target)^2 (mask may be NULL);
+ *            grad [param_count]; dcache scratch [batch][132]; deterministic.
+ *  adam:     in-place Adam step (bias-corrected, step counts from 1).
+ */
+int ckks_gear_mlp_param_count(void);
+int ckks_gear_mlp_forward(const float* params, const float* x, float* y, float* cache, int batch,
+                          void* stream);
+int ckks_gear_mlp_backward(const float* params, const float* x, const float* cache, const float* y,
+                           const float* target, const float* mask, float* grad, float* dcache,
+                           int batch, void* stream);
+int ckks_gear_mlp_adam(float* params, const float* grad, float* m, float* v, int step, float lr,
+                       float beta1, float beta2, float eps, void* stream);
 
 /* Size of the static device scratch used by ckks_ct_mul_relin_rescale_noalloc. */
 #define CKKS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
