@@ -1,0 +1,189 @@
+"""Batched uneven workload: thousands of ciphertext operations of mixed ring
+dimension (N = 2^12, 2^13), level (2..8 limbs) and kind (ct x ct + relin +
+rescale, ct x pt + rescale) in one CUDA-graph replay per step.
+
+Items are grouped into same-shape buckets (kind, log N, level); each bucket
+is one batched launch sequence of the library's kernels (one CTA per
+polynomial limb, so the buckets of different shapes need no padding).  The
+buckets are spread over a pool of streams and the whole plan is captured
+once into a CUDA graph, so a step costs one graph launch.  The autotuner
+times every bucket alone under each launch shape (per-thread radix 2^K,
+register budget for 1 or 2 CTAs per SM, chunking of the bucket into
+launches) and keeps the fastest; the choice is baked into the graph at
+capture time.
+
+The reference's batching is time multiplexing of four poly-mult instances on
+one FPGA (rtl/m4/e2e_ckks_mult_ctrl_m4.sv:368-482, TIME_MULT = 4 in
+scripts/exp_e17_energy_efficiency.py:32).
+"""
+from __future__ import annotations
+
+import itertools
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib, ops
+from .evaluator import Evaluator
+from .params import CkksParams
+
+U64 = torch.uint64
+
+
+@dataclass(frozen=True)
+class Shape:
+    op: str          # "ctct" or "ctpt"
+    log_n: int
+    level: int
+
+
+def synthetic_workload(n_items: int = 4096, seed: int = 0, frac_ctct: float = 0.6,
+                       log_ns=(12, 13), levels=tuple(range(2, 9))) -> list:
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n_items):
+        op = "ctct" if rng.random() < frac_ctct else "ctpt"
+        out.append(Shape(op, int(rng.choice(log_ns)), int(rng.choice(levels))))
+    return out
+
+
+@dataclass
+class Bucket:
+    shape: Shape
+    count: int
+    a: torch.Tensor = None
+    b: torch.Tensor = None          # second ciphertext (ctct) or plaintext (ctpt)
+    out: torch.Tensor = None
+    scratch: torch.Tensor = None
+    tune: dict = field(default_factory=lambda: {"k": 3, "minb": 1, "chunk": 0})
+
+
+class BatchExecutor:
+    def __init__(self, items: list, max_level: int = 8, seed: int = 0, n_streams: int = 4, device=None):
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        counts = {}
+        for it in items:
+            counts[it] = counts.get(it, 0) + 1
+        self.n_items = len(items)
+        self.evs = {}
+        for log_n in sorted({s.log_n for s in counts}):
+            ev = Evaluator(CkksParams.standard(log_n, max_level, seed=seed + log_n), device=self.device)
+            ev.keygen()
+            self.evs[log_n] = ev
+        self.buckets = []
+        for sh, cnt in sorted(counts.items(), key=lambda kv: (kv[0].op, kv[0].log_n, kv[0].level)):
+            ev = self.evs[sh.log_n]
+            bk = Bucket(sh, cnt)
+            bk.a = ev.uniform(cnt * 2, sh.level).reshape(cnt, 2, sh.level, ev.n)
+            if sh.op == "ctct":
+                bk.b = ev.uniform(cnt * 2, sh.level).reshape(cnt, 2, sh.level, ev.n)
+                need = ops.ct_mul_scratch_bytes(ev.ctx, cnt, sh.level)
+                bk.scratch = torch.empty((need + 7) // 8, dtype=U64, device=self.device)
+            else:
+                bk.b = ev.uniform(cnt, sh.level)
+            bk.out = torch.empty((cnt, 2, sh.level - 1, ev.n), dtype=U64, device=self.device)
+            self.buckets.append(bk)
+        self.streams = [torch.cuda.Stream(device=self.device) for _ in range(n_streams)]
+        self.graph = None
+
+    # ---------------------------------------------------------------- launches
+    def launch(self, bk: Bucket):
+        ev = self.evs[bk.shape.log_n]
+        ctx = ev.ctx
+        st = torch.cuda.current_stream().cuda_stream
+        chunk = bk.tune["chunk"] or bk.count
+        lvl = bk.shape.level
+        if bk.shape.op == "ctct":
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 0, bk.tune["k"])
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 1, bk.tune["minb"])
+            for s in range(0, bk.count, chunk):
+                e = min(bk.count, s + chunk)
+                n = e - s
+                _lib.call("ckks_ct_mul_relin_rescale", ctx.handle, bk.out[s:e].data_ptr(), bk.a[s:e].data_ptr(),
+                          bk.b[s:e].data_ptr(), ev.rlk.data_ptr(), n, lvl, bk.scratch.data_ptr(),
+                          bk.scratch.numel() * 8, st)
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 0, 0)
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 1, 0)
+        else:
+            for s in range(0, bk.count, chunk):
+                e = min(bk.count, s + chunk)
+                _lib.call("ckks_ct_mul_plain_rescale", ctx.handle, bk.out[s:e].data_ptr(), bk.a[s:e].data_ptr(),
+                          bk.b[s:e].data_ptr(), 1, e - s, lvl, st)
+
+    def run_eager(self):
+        cur = torch.cuda.current_stream()
+        fork = torch.cuda.Event()
+        fork.record(cur)
+        for s in self.streams:
+            s.wait_event(fork)
+        order = sorted(self.buckets, key=lambda b: -b.count * (1 << b.shape.log_n) * b.shape.level)
+        for i, bk in enumerate(order):
+            with torch.cuda.stream(self.streams[i % len(self.streams)]):
+                self.launch(bk)
+        for s in self.streams:
+            j = torch.cuda.Event()
+            j.record(s)
+            cur.wait_event(j)
+
+    def capture(self):
+        self.run_eager()                      # kernel attributes, lazy module loading
+        torch.cuda.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.run_eager()
+        self.graph = g
+        return g
+
+    def step(self):
+        if self.graph is None:
+            self.capture()
+        self.graph.replay()
+
+    def time_steps(self, steps: int = 10, warmup: int = 3, use_graph: bool = True) -> dict:
+        fn = self.step if use_graph else self.run_eager
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(steps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        return {"ms_per_step": ms, "items_per_s": self.n_items / (ms / 1000.0), "graph": use_graph}
+
+    # ---------------------------------------------------------------- autotuner
+    def autotune(self, reps: int = 3) -> dict:
+        """Time each bucket alone under every launch shape; keep the fastest."""
+        choices = {}
+        for bk in self.buckets:
+            cands = [{"k": 3, "minb": 1, "chunk": 0}]
+            if bk.shape.op == "ctct":
+                cands = [{"k": k, "minb": mb, "chunk": ch}
+                         for k, mb, ch in itertools.product((3, 4), (1, 2), (0, 128))
+                         if not (mb == 2 and bk.shape.log_n not in (12, 13))
+                         and not (ch and ch >= bk.count)]
+            best = None
+            for c in cands:
+                bk.tune = c
+                self.launch(bk)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(reps):
+                    self.launch(bk)
+                e1.record()
+                torch.cuda.synchronize()
+                t = e0.elapsed_time(e1) / reps
+                if best is None or t < best[0]:
+                    best = (t, c)
+            bk.tune = best[1]
+            choices[f"{bk.shape.op}/N=2^{bk.shape.log_n}/L={bk.shape.level}"] = {"ms": best[0], **best[1],
+                                                                              "count": bk.count}
+        self.graph = None
+        return choices

@@ -20,7 +20,8 @@ struct TwPair {
 
 // Per-prime constants, one record per prime of a context.
 struct PrimeInfo {
-  u64 q, q2, q4;
+  u64 q, q2;
+  u64 qlazy;      // 32 q: above any lazy forward-NTT output (see ntt.cuh)
   u64 mont_qinv;  // -q^{-1} mod 2^64
   u64 r_mod;      // 2^64 mod q
   u64 r_mod_s;    // Shoup companion of r_mod

@@ -164,9 +164,8 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     if (!special && j == ti) {
       load_z<LOGN, K>(x, S.d2n + ct * LN + (size_t)j * N, tid);
     } else {
+      // digit j residues (< q_j < 2 q_i) go into the lazy transform unreduced
       load_c<LOGN, K>(x, S.d2c + ct * LN + (size_t)j * N, tid);
-#pragma unroll
-      for (int e = 0; e < Sh::E; ++e) x[e] = csub(x[e], P.q);
       ntt_fwd_lazy<LOGN, K>(x, sm, tid, tf, P.q, P.q2);
     }
     const ulonglong2* k0 = key + (((size_t)j * 2 + 0) * (nq + 1) + pidx) * N;
@@ -239,7 +238,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     load_z<LOGN, K>(av, ak + (size_t)t * N, tid);
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) {
-      const u64 ks = shoup(av[e] + PT.q4 - x[e], pt.w, pt.ws, PT.q);
+      const u64 ks = shoup(av[e] + PT.qlazy - x[e], pt.w, pt.ws, PT.q);
       x[e] = addmod(dv[e], ks, PT.q);
     }
   }
@@ -265,7 +264,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     load_z<LOGN, K>(av, ak + (size_t)i * N, tid);
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) {
-      const u64 s = dv[e] + shoup_lazy(av[e], pv.w, pv.ws, P.q) + P.q4 - x[e];  // (0, 7q)
+      const u64 s = dv[e] + shoup_lazy(av[e], pv.w, pv.ws, P.q) + P.qlazy - x[e];  // (0, 35q)
       x[e] = shoup(s, ci.w, ci.ws, P.q);
     }
     store_z<LOGN, K>(x, ok + (size_t)i * N, tid);

@@ -1,0 +1,85 @@
+// ctpt.cu - ciphertext x plaintext multiply fused with the RNS rescale.
+//
+// One CTA per (ct, poly k): x_i = a_k,i * p_i per limb (evaluation domain);
+// the last limb is brought to the coefficient domain (INTT), centred, and for
+// every remaining limb out_i = (x_i - NTT_i([w]_{q_i})) * q_t^-1.  The
+// plaintext may be shared by all ciphertexts (pt_stride = 0) or given per
+// ciphertext (pt_stride = 1).
+#include "dispatch.cuh"
+#include "profile.hpp"
+
+template <int LOGN, int K>
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T)
+    k_ctpt_rescale(u64* __restrict__ out, const u64* __restrict__ ct, const u64* __restrict__ pt,
+                   int pt_stride, int level, const PrimeInfo* __restrict__ pi,
+                   const TwPair* __restrict__ tw, const TwPair* __restrict__ qtinv, int nq) {
+  extern __shared__ u64 sm[];
+  using Sh = NttShape<LOGN, K>;
+  constexpr int N = Sh::N;
+  constexpr int T = Sh::T;
+  u64* ws = sm + Sh::SMEM_WORDS;
+  const long long c = blockIdx.x >> 1;
+  const int k = blockIdx.x & 1;
+  const int t = level - 1;
+  const int tid = threadIdx.x;
+  const size_t LN = (size_t)level * N;
+  const u64* a = ct + (c * 2 + k) * LN;
+  const u64* p = pt + (size_t)c * pt_stride * LN;
+  u64* o = out + (c * 2 + k) * (size_t)t * N;
+  const PrimeInfo PT = pi[t];
+  u64 x[Sh::E], y[Sh::E];
+  load_z<LOGN, K>(x, a + (size_t)t * N, tid);
+  load_z<LOGN, K>(y, p + (size_t)t * N, tid);
+#pragma unroll
+  for (int e = 0; e < Sh::E; ++e) x[e] = mulmod(x[e], y[e], PT);
+  ntt_inv<LOGN, K>(x, sm, tid, tw + ((size_t)t * 4 + TW_INV) * N, PT);
+#pragma unroll
+  for (int e = 0; e < Sh::E; ++e) ws[e * T + tid] = x[e];
+#pragma unroll 1
+  for (int i = 0; i < t; ++i) {
+    const PrimeInfo P = pi[i];
+    const TwPair ci = qtinv[(size_t)t * nq + i];
+#pragma unroll
+    for (int e = 0; e < Sh::E; ++e) {
+      const u64 w = ws[e * T + tid];
+      x[e] = w > PT.half ? w - PT.q + P.q : w;
+    }
+    ntt_fwd_lazy<LOGN, K>(x, sm, tid, tw + ((size_t)i * 4 + TW_FWD) * N, P.q, P.q2);
+    load_z<LOGN, K>(y, a + (size_t)i * N, tid);
+    u64 pv[Sh::E];
+    load_z<LOGN, K>(pv, p + (size_t)i * N, tid);
+#pragma unroll
+    for (int e = 0; e < Sh::E; ++e) {
+      const u64 xi = mulmod(y[e], pv[e], P);
+      x[e] = shoup(xi + P.qlazy - x[e], ci.w, ci.ws, P.q);
+    }
+    store_z<LOGN, K>(x, o + (size_t)i * N, tid);
+  }
+}
+
+extern "C" int ckks_ct_mul_plain_rescale(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct,
+                                         const uint64_t* pt, int pt_per_ct, int n_ct, int level,
+                                         void* stream) {
+  const char* fn = "ckks_ct_mul_plain_rescale";
+  CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
+  CKKS_REQUIRE(level >= 2 && level <= ctx->n_q, "%s: level=%d outside [2, %d]", fn, level, ctx->n_q);
+  CKKS_REQUIRE(n_ct >= 0, "%s: n_ct < 0", fn);
+  for (int i = 0; i < level; ++i)
+    CKKS_REQUIRE(ctx->has_nega[i], "%s: prime %d has no 2N-th root", fn, i);
+  for (int i = 0; i < level - 1; ++i)
+    CKKS_REQUIRE(ctx->primes[level - 1] < 2 * ctx->primes[i],
+                 "%s: q_%d must be < 2 q_%d for the centred conversion", fn, level - 1, i);
+  if (n_ct == 0) return CKKS_OK;
+  CKKS_REQUIRE(out && ct && pt, "%s: NULL pointer argument", fn);
+  cudaStream_t st = as_stream(stream);
+  return dispatch_logn(ctx->log_n, [&]<int L, int K>() -> int {
+    using Sh = NttShape<L, K>;
+    const int smem = (Sh::SMEM_WORDS + Sh::N) * 8;
+    ensure_smem(k_ctpt_rescale<L, K>, smem);
+    ProfSpan span(CKKS_STAGE_OTHER, st);
+    k_ctpt_rescale<L, K><<<grid1d(2ll * n_ct), Sh::T, smem, st>>>(
+        reinterpret_cast<u64*>(out), reinterpret_cast<const u64*>(ct), reinterpret_cast<const u64*>(pt),
+        pt_per_ct ? 1 : 0, level, ctx->d_pi, ctx->d_tw, ctx->d_qtinv, ctx->n_q);
+    return ckks_check_launch(fn);
+  });
+}

@@ -124,7 +124,7 @@ extern "C" int ckks_ctx_create(int log_n, int n_primes, int n_special, const uin
     std::memset(&P, 0, sizeof(P));
     P.q = q;
     P.q2 = 2 * q;
-    P.q4 = 4 * q;
+    P.qlazy = q << 5;
     u64 inv = 1;  // q^{-1} mod 2^64 by Newton
     for (int k = 0; k < 7; ++k) inv *= 2 - q * inv;
     P.mont_qinv = (u64)0 - inv;

@@ -74,16 +74,25 @@ __device__ __forceinline__ int posZ(int tid, int e) {
 }
 
 // ---------------------------------------------------------------- butterflies
+// No per-butterfly reduction: with q < 2^47 the 64-bit words have room for
+// the growth.  Forward (Cooley-Tukey): t = w y mod q lands in [0, 2q), so
+// both outputs grow by at most 2q per stage (x + t, x + 2q - t); after the
+// LOGN <= 14 stages a value below B_in is below B_in + 28q.  Inverse
+// (Gentleman-Sande): the difference branch is re-reduced by the Shoup
+// multiply to [0, 2q) while the sum branch at most doubles, so the input of
+// the stage run d-th is below 2q * 2^d; the difference is offset by that
+// bound (bs) to stay non-negative.  After LOGN stages values are below
+// 2q * 2^14 < 2^62, and the closing N^-1 Shoup multiply accepts any word.
 __device__ __forceinline__ void ct_bfly(u64& x, u64& y, const TwPair& w, u64 q, u64 q2) {
-  const u64 xr = csub(x, q2);
   const u64 t = shoup_lazy(y, w.w, w.ws, q);
+  const u64 xr = x;
   x = xr + t;
-  y = xr - t + q2;
+  y = xr + q2 - t;
 }
 
-__device__ __forceinline__ void gs_bfly(u64& x, u64& y, const TwPair& w, u64 q, u64 q2) {
-  const u64 u = csub(x + y, q2);
-  const u64 v = x - y + q2;
+__device__ __forceinline__ void gs_bfly(u64& x, u64& y, const TwPair& w, u64 q, u64 bs) {
+  const u64 u = x + y;
+  const u64 v = x + bs - y;
   x = u;
   y = shoup_lazy(v, w.w, w.ws, q);
 }
@@ -133,13 +142,14 @@ __device__ __forceinline__ void inv_pass(u64 (&x)[1 << K], int tid, const TwPair
 #pragma unroll
     for (int u = KP - 1; u >= 0; --u) {
       const int half = RR >> (u + 1);
+      const u64 bs = q2 << (LOGN - 1 - (S0 + u));  // input bound of this stage
 #pragma unroll
       for (int grp = 0; grp < (1 << u); ++grp) {
         const TwPair w = ldtw(itw + (1 << (S0 + u)) + block * (1 << u) + grp);
 #pragma unroll
         for (int j = 0; j < half; ++j) {
           const int r = grp * 2 * half + j;
-          gs_bfly(x[c * RR + r], x[c * RR + r + half], w, q, q2);
+          gs_bfly(x[c * RR + r], x[c * RR + r + half], w, q, bs);
         }
       }
     }
@@ -202,7 +212,11 @@ struct InvRest {
   }
 };
 
-// Forward NTT: x in layout C with values in [0, 4q) -> layout Z, values in [0, 4q).
+// Forward NTT: x in layout C with values below 4q -> layout Z, values below
+// 4q + 2q LOGN <= 32q (see the butterfly notes); callers that subtract a
+// transformed value add LAZY_FWD_BOUND(q) first.
+__device__ __forceinline__ u64 lazy_fwd_bound(u64 q) { return q << 5; }
+
 template <int LOGN, int K>
 __device__ __forceinline__ void ntt_fwd_lazy(u64 (&x)[1 << K], u64* sm, int tid,
                                              const TwPair* __restrict__ tw, u64 q, u64 q2) {
@@ -216,7 +230,7 @@ __device__ __forceinline__ void ntt_fwd(u64 (&x)[1 << K], u64* sm, int tid,
                                         const TwPair* __restrict__ tw, const PrimeInfo& P) {
   ntt_fwd_lazy<LOGN, K>(x, sm, tid, tw, P.q, P.q2);
 #pragma unroll
-  for (int e = 0; e < (1 << K); ++e) x[e] = reduce4(x[e], P.q, P.q2);
+  for (int e = 0; e < (1 << K); ++e) x[e] = reduce_any(x[e], P);
 }
 
 // Inverse NTT: x in layout Z with values in [0, 2q) -> layout C, values in [0, q),
@@ -228,6 +242,34 @@ __device__ __forceinline__ void ntt_inv(u64 (&x)[1 << K], u64* sm, int tid,
   inv_pass<LOGN, K, 0, K>(x, tid, itw, P.q, P.q2);
 #pragma unroll
   for (int e = 0; e < (1 << K); ++e) x[e] = csub(shoup_lazy(x[e], P.ninv, P.ninv_s, P.q), P.q);
+}
+
+// Layout-Z global access: the last pass has unit stride inside each run, so
+// registers (e, e+1) with e even are adjacent words; move them as 16-byte vectors.
+template <int LOGN, int K>
+__device__ __forceinline__ void load_z(u64 (&x)[1 << K], const u64* __restrict__ src, int tid) {
+#pragma unroll
+  for (int e = 0; e < (1 << K); e += 2) {
+    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(src + posZ<LOGN, K>(tid, e)));
+    x[e] = v.x;
+    x[e + 1] = v.y;
+  }
+}
+template <int LOGN, int K>
+__device__ __forceinline__ void store_z(const u64 (&x)[1 << K], u64* __restrict__ dst, int tid) {
+#pragma unroll
+  for (int e = 0; e < (1 << K); e += 2)
+    *reinterpret_cast<ulonglong2*>(dst + posZ<LOGN, K>(tid, e)) = make_ulonglong2(x[e], x[e + 1]);
+}
+template <int LOGN, int K>
+__device__ __forceinline__ void load_c(u64 (&x)[1 << K], const u64* __restrict__ src, int tid) {
+#pragma unroll
+  for (int e = 0; e < (1 << K); ++e) x[e] = __ldg(src + posC<LOGN, K>(tid, e));
+}
+template <int LOGN, int K>
+__device__ __forceinline__ void store_c(const u64 (&x)[1 << K], u64* __restrict__ dst, int tid) {
+#pragma unroll
+  for (int e = 0; e < (1 << K); ++e) dst[posC<LOGN, K>(tid, e)] = x[e];
 }
 
 // Layout-Z global access: the last pass has unit stride inside each run, so

@@ -157,7 +157,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   ntt_fwd_lazy<LOGN, K>(y, sm, tid, tf, P.q, P.q2);
 #pragma unroll
   for (int e = 0; e < S::E; ++e)
-    x[e] = mulmod(reduce4(x[e], P.q, P.q2), reduce4(y[e], P.q, P.q2), P);
+    x[e] = mulmod(x[e], y[e], P);  // lazy inputs < 32q: a b < q 2^64 holds
   __syncthreads();
   ntt_inv<LOGN, K>(x, sm, tid, ti, P);
 #pragma unroll
@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     ntt_fwd_lazy<LOGN, K>(y, sm, tid, tf, P.q, P.q2);
 #pragma unroll
     for (int e = 0; e < S::E; ++e)
-      x[e] = mulmod(reduce4(x[e], P.q, P.q2), reduce4(y[e], P.q, P.q2), P);
+      x[e] = mulmod(x[e], y[e], P);  // lazy inputs < 32q: a b < q 2^64 holds
     __syncthreads();
     ntt_inv<LOGN, K>(x, sm, tid, ti, P);
     __syncthreads();

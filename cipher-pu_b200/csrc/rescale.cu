@@ -104,7 +104,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     for (int e = 0; e < S::E; ++e) {
       const int p = posZ<LOGN, K>(tid, e);
       const u64 xi = src[(size_t)i * S::N + p];
-      const u64 d = xi + P.q4 - x[e];  // (0, 5q)
+      const u64 d = xi + P.qlazy - x[e];  // (0, 33q)
       dst[(size_t)i * S::N + p] = shoup(d, ci.w, ci.ws, P.q);
     }
   }

@@ -376,6 +376,28 @@ int ckks_gear_mlp_backward(const float* params, const float* x, const float* cac
 int ckks_gear_mlp_adam(float* params, const float* grad, float* m, float* v, int step, float lr,
                        float beta1, float beta2, float eps, void* stream);
 
+/*
+ * Ciphertext x plaintext multiply fused with the RNS rescale:
+ * ct [n_ct][2][level][N], pt [level][N] shared (pt_per_ct = 0) or
+ * [n_ct][level][N] (pt_per_ct = 1), all evaluation domain ->
+ * out [n_ct][2][level-1][N].  Replaces scripts/exp_e11_ckks_e2e_real.py:102
+ * rlwe_mul_plain (and scripts/exp_e24_rotation_bootstrap.py mul_plain_exact)
+ * followed by the rescale of rtl/m5/rescale_rns.sv.
+ */
+int ckks_ct_mul_plain_rescale(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct,
+                              const uint64_t* pt, int pt_per_ct, int n_ct, int level, void* stream);
+
+/*
+ * Modular-multiply throughput microbenchmark (compute roofline of the
+ * NTT-bound kernels): n_blocks x threads threads each run 8 independent
+ * chains of `iters` lazy modular multiplies by w mod q (q < 2^47) - kind 0:
+ * integer Shoup, 1: FP64 double-word, 2: both interleaved.  out receives one
+ * word per thread (to keep the work alive).  Time it with events on `stream`:
+ * modmul/s = n_blocks * threads * iters * 8 / seconds.
+ */
+int ckks_modmul_peak(uint64_t* out, int n_blocks, int threads, int iters, int kind, uint64_t q,
+                     uint64_t w, void* stream);
+
 /* Size of the static device scratch used by ckks_ct_mul_relin_rescale_noalloc. */
 #define CKKS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 

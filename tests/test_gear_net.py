@@ -79,7 +79,7 @@ def test_learned_controller_gains_over_plain(cuda):
     if not NET.exists():
         pytest.fail(f"trained gear network missing: {NET}")
     from ckks_b200.train_gear import compare
-    r = compare(NET, "mlp", batches=4, batch=1024)
+    r = compare(NET, "mlp", batches=8, batch=1024)
     assert r["learned"]["probes"] < r["plain"]["probes"]
     assert r["learned"]["snr_db"] >= r["plain"]["snr_db"] - 0.5
     assert r["learned"]["top1_agreement"] >= r["plain"]["top1_agreement"]
