@@ -58,7 +58,7 @@ def _list(t) -> list[int]:
 
 
 def nega_friendly(q: int, n: int) -> bool:
-    return q < (1 << 50) and (q - 1) % (2 * n) == 0
+    return q < (1 << 47) and (q - 1) % (2 * n) == 0
 
 
 # ------------------------------------------------------------------ transforms
@@ -96,7 +96,7 @@ def poly_mult_many(As, Bs, q: int, cyclic: bool = False) -> list[list[int]]:
     a = _dev([v % q for row in As for v in row]).reshape(len(As), 1, n)
     b = _dev([v % q for row in Bs for v in row]).reshape(len(Bs), 1, n)
     friendly = (q - 1) % n == 0 if cyclic else nega_friendly(q, n)
-    if friendly and q < (1 << 50):
+    if friendly and q < (1 << 47):
         ctx = _ctx(log_n, [q])
         out = ops.poly_mul(ctx, a, b, cyclic=cyclic)
     else:

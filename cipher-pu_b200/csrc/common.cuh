@@ -1,11 +1,12 @@
 // common.cuh - shared types and exact 64-bit modular arithmetic for the
 // CKKS evaluation core (sm_100a).
 //
-// Moduli are NTT-friendly primes below 2^50 (the production chain is 45-bit).
-// Twiddle multiplications use Shoup's precomputed quotient
-// (w' = floor(w * 2^64 / q)), variable x variable products use Montgomery
-// multiplication with R = 2^64 followed by a Shoup multiply by (R mod q).
-// All lazy ranges stay below 4q < 2^52, far inside 64 bits.
+// Moduli are NTT-friendly primes below 2^47 (the production chain is 45-bit).
+// The NTT butterflies run in exact FP64 (see ntt.cuh) with twiddles stored as
+// (w, w / q) pairs; integer twiddle multiplications elsewhere use Shoup's
+// precomputed quotient (w' = floor(w * 2^64 / q)), variable x variable
+// products use Montgomery multiplication with R = 2^64 followed by a Shoup
+// multiply by (R mod q).  All lazy integer ranges stay far inside 64 bits.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -18,10 +19,27 @@ struct TwPair {
   u64 ws;  // floor(w * 2^64 / q)
 };
 
+// FP64 NTT twiddle: value and value / q (correctly rounded).
+struct TwD {
+  double w;
+  double wq;
+};
+
+// Per-prime FP64 table slots ([n_primes][TWF_SLOTS][N] entries of TwD).
+enum {
+  TWF_FWD = 0,       // merged negacyclic forward: psi^brv(k), k in [1, N)
+  TWF_INV = 1,       // negacyclic inverse DIT twiddles: omega^-i, i in [0, N/2), omega = psi^2
+  TWF_FWD_CYC = 2,   // merged cyclic forward
+  TWF_INV_CYC = 3,   // cyclic inverse DIT twiddles: omega_cyc^-i, i in [0, N/2)
+  TWF_POST = 4,      // N^-1 psi^-j, j in [0, N)
+  TWF_POST_CYC = 5,  // N^-1 (every j)
+  TWF_SLOTS = 6
+};
+
 // Per-prime constants, one record per prime of a context.
 struct PrimeInfo {
   u64 q, q2;
-  u64 qlazy;      // 32 q: above any lazy forward-NTT output (see ntt.cuh)
+  u64 qlazy;      // 32 q: added before subtracting an NTT output (any value < 32 q)
   u64 mont_qinv;  // -q^{-1} mod 2^64
   u64 r_mod;      // 2^64 mod q
   u64 r_mod_s;    // Shoup companion of r_mod

@@ -98,7 +98,7 @@ static int dispatch_cm(int log_n, int kreq, int mreq, F&& f, const char* fn) {
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_tensor(const u64* __restrict__ A, const u64* __restrict__ B, CmScratch S, int level,
-                const PrimeInfo* __restrict__ pi, const TwPair* __restrict__ tw) {
+                const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   store_z<LOGN, K>(a0v, d0, tid);
   store_z<LOGN, K>(b0v, d0 + LN, tid);
   store_z<LOGN, K>(m2, S.d2n + ct * LN + (size_t)j * N, tid);
-  ntt_inv<LOGN, K>(m2, sm, tid, tw + ((size_t)j * 4 + TW_INV) * N, P);
+  ntt_inv<LOGN, K>(m2, sm, tid, twbase<LOGN>(tw, j), P);
   store_c<LOGN, K>(m2, S.d2c + ct * LN + (size_t)j * N, tid);
 }
 
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_modup(CmScratch S, const ulonglong2* __restrict__ key, int level, int nq,
-               const PrimeInfo* __restrict__ pi, const TwPair* __restrict__ tw) {
+               const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
@@ -157,16 +157,16 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   const int tid = threadIdx.x;
   const PrimeInfo P = pi[pidx];
   const size_t LN = (size_t)level * N;
-  const TwPair* tf = tw + ((size_t)pidx * 4 + TW_FWD) * N;
+  const TwD* tb = twbase<LOGN>(tw, pidx);
 #pragma unroll 1
   for (int j = 0; j < level; ++j) {
     u64 x[Sh::E];
     if (!special && j == ti) {
       load_z<LOGN, K>(x, S.d2n + ct * LN + (size_t)j * N, tid);
     } else {
-      // digit j residues (< q_j < 2 q_i) go into the lazy transform unreduced
+      // digit j residues (< q_j < 2 q_i) go into the transform unreduced
       load_c<LOGN, K>(x, S.d2c + ct * LN + (size_t)j * N, tid);
-      ntt_fwd_lazy<LOGN, K>(x, sm, tid, tf, P.q, P.q2);
+      ntt_fwd<LOGN, K>(x, sm, tid, tb, P);
     }
     const ulonglong2* k0 = key + (((size_t)j * 2 + 0) * (nq + 1) + pidx) * N;
     const ulonglong2* k1 = key + (((size_t)j * 2 + 1) * (nq + 1) + pidx) * N;
@@ -203,7 +203,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_down(CmScratch S, u64* __restrict__ out, int level, int nq,
-              const PrimeInfo* __restrict__ pi, const TwPair* __restrict__ tw,
+              const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw,
               const TwPair* __restrict__ pinv, const TwPair* __restrict__ qtinv) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
@@ -224,13 +224,13 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 
   u64 x[Sh::E];
   load_z<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
-  ntt_inv<LOGN, K>(x, sm, tid, tw + ((size_t)nq * 4 + TW_INV) * N, PP);
+  ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, nq), PP);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) {
     vs[e * T + tid] = x[e];
     x[e] = x[e] > PP.half ? x[e] - PP.q + PT.q : x[e];
   }
-  ntt_fwd_lazy<LOGN, K>(x, sm, tid, tw + ((size_t)t * 4 + TW_FWD) * N, PT.q, PT.q2);
+  ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, t), PT);
   {
     const TwPair pt = pinv[t];
     u64 dv[Sh::E], av[Sh::E];
@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
       x[e] = addmod(dv[e], ks, PT.q);
     }
   }
-  ntt_inv<LOGN, K>(x, sm, tid, tw + ((size_t)t * 4 + TW_INV) * N, PT);
+  ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, t), PT);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) ws[e * T + tid] = x[e];
 #pragma unroll 1
@@ -258,7 +258,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
       const u64 wi = w > PT.half ? w - PT.q + P.q : w;
       x[e] = shoup_lazy(vi, pv.w, pv.ws, P.q) + wi;  // [0, 3q)
     }
-    ntt_fwd_lazy<LOGN, K>(x, sm, tid, tw + ((size_t)i * 4 + TW_FWD) * N, P.q, P.q2);
+    ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
     u64 dv[Sh::E], av[Sh::E];
     load_z<LOGN, K>(dv, dk + (size_t)i * N, tid);
     load_z<LOGN, K>(av, ak + (size_t)i * N, tid);

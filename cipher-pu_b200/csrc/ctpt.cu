@@ -12,7 +12,7 @@ template <int LOGN, int K>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     k_ctpt_rescale(u64* __restrict__ out, const u64* __restrict__ ct, const u64* __restrict__ pt,
                    int pt_stride, int level, const PrimeInfo* __restrict__ pi,
-                   const TwPair* __restrict__ tw, const TwPair* __restrict__ qtinv, int nq) {
+                   const TwD* __restrict__ tw, const TwPair* __restrict__ qtinv, int nq) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
@@ -32,7 +32,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   load_z<LOGN, K>(y, p + (size_t)t * N, tid);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) x[e] = mulmod(x[e], y[e], PT);
-  ntt_inv<LOGN, K>(x, sm, tid, tw + ((size_t)t * 4 + TW_INV) * N, PT);
+  ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, t), PT);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) ws[e * T + tid] = x[e];
 #pragma unroll 1
@@ -44,7 +44,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
       const u64 w = ws[e * T + tid];
       x[e] = w > PT.half ? w - PT.q + P.q : w;
     }
-    ntt_fwd_lazy<LOGN, K>(x, sm, tid, tw + ((size_t)i * 4 + TW_FWD) * N, P.q, P.q2);
+    ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
     load_z<LOGN, K>(y, a + (size_t)i * N, tid);
     u64 pv[Sh::E];
     load_z<LOGN, K>(pv, p + (size_t)i * N, tid);

@@ -91,12 +91,12 @@ extern "C" int ckks_ctx_create(int log_n, int n_primes, int n_special, const uin
   c->n_special = n_special;
   c->n_q = n_primes - n_special;
   cudaGetDevice(&c->device);
-  std::vector<TwPair> tw((size_t)n_primes * 4 * n);
+  std::vector<TwD> tw((size_t)n_primes * TWF_SLOTS * n);
   for (int i = 0; i < n_primes; ++i) {
     const u64 q = primes[i];
-    if (q < 3 || q >= (1ull << 50) || !is_prime_u64(q)) {
+    if (q < 3 || q >= (1ull << 47) || !is_prime_u64(q)) {
       free_ctx(c);
-      return ckks_set_error(CKKS_EINVAL, "ckks_ctx_create: primes[%d]=%llu is not a prime in [3, 2^50)",
+      return ckks_set_error(CKKS_EINVAL, "ckks_ctx_create: primes[%d]=%llu is not a prime in [3, 2^47)",
                             i, (unsigned long long)q);
     }
     if ((q - 1) % (u64)n != 0) {
@@ -137,26 +137,38 @@ extern "C" int ckks_ctx_create(int log_n, int n_primes, int n_special, const uin
     P.qd = (double)q;
     P.qinv_d = 1.0 / (double)q;
     c->h_pi.push_back(P);
-    TwPair* t = tw.data() + (size_t)i * 4 * n;
-    TwPair zero;
-    zero.w = 0;
-    zero.ws = 0;
-    for (int k = 0; k < 4 * n; ++k) t[k] = zero;
+    TwD* t = tw.data() + (size_t)i * TWF_SLOTS * n;
+    for (int k = 0; k < TWF_SLOTS * n; ++k) t[k] = TwD{0.0, 0.0};
+    const u64 ninv_q = h_invmod((u64)n % q, q);
     if (nega) {
+      // forward: merged psi^brv(k); inverse: DIT twiddles omega^-i (omega = psi^2)
+      // and the closing untwist N^-1 psi^-j
       const u64 pinv = h_invmod(ps, q);
-      for (int k = 1; k < n; ++k) {
-        const int e = bitrev(k, log_n);
-        t[TW_FWD * n + k] = h_twp(h_powmod(ps, e, q), q);
-        t[TW_INV * n + k] = h_twp(h_powmod(pinv, e, q), q);
+      for (int k = 1; k < n; ++k) t[TWF_FWD * n + k] = h_twd(h_powmod(ps, bitrev(k, log_n), q), q);
+      const u64 winv = h_mulmod(pinv, pinv, q);
+      u64 cur = 1;
+      for (int k = 0; k < n / 2; ++k) {
+        t[TWF_INV * n + k] = h_twd(cur, q);
+        cur = h_mulmod(cur, winv, q);
+      }
+      cur = ninv_q;
+      for (int j = 0; j < n; ++j) {
+        t[TWF_POST * n + j] = h_twd(cur, q);
+        cur = h_mulmod(cur, pinv, q);
       }
     }
     const u64 oinv = h_invmod(om, q);
     for (int m = 1; m < n; m <<= 1)
       for (int ii = 0; ii < m; ++ii) {
         const int e = (bitrev(m + ii, log_n) - n / (2 * m)) / 2;
-        t[TW_FWD_CYC * n + m + ii] = h_twp(h_powmod(om, e, q), q);
-        t[TW_INV_CYC * n + m + ii] = h_twp(h_powmod(oinv, e, q), q);
+        t[TWF_FWD_CYC * n + m + ii] = h_twd(h_powmod(om, e, q), q);
       }
+    u64 cur = 1;
+    for (int k = 0; k < n / 2; ++k) {
+      t[TWF_INV_CYC * n + k] = h_twd(cur, q);
+      cur = h_mulmod(cur, oinv, q);
+    }
+    for (int j = 0; j < n; ++j) t[TWF_POST_CYC * n + j] = h_twd(ninv_q, q);
   }
   // keyswitch / rescale constants
   const int nq = c->n_q;
@@ -189,13 +201,13 @@ extern "C" int ckks_ctx_create(int log_n, int n_primes, int n_special, const uin
     }
   cudaError_t e = cudaSuccess;
   e = cudaMalloc(&c->d_pi, sizeof(PrimeInfo) * n_primes);
-  if (e == cudaSuccess) e = cudaMalloc(&c->d_tw, sizeof(TwPair) * tw.size());
+  if (e == cudaSuccess) e = cudaMalloc(&c->d_tw, sizeof(TwD) * tw.size());
   if (e == cudaSuccess) e = cudaMalloc(&c->d_pinv, sizeof(TwPair) * nq);
   if (e == cudaSuccess) e = cudaMalloc(&c->d_qtinv, sizeof(TwPair) * (size_t)nq * nq);
   if (e == cudaSuccess)
     e = cudaMemcpy(c->d_pi, c->h_pi.data(), sizeof(PrimeInfo) * n_primes, cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
-    e = cudaMemcpy(c->d_tw, tw.data(), sizeof(TwPair) * tw.size(), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(c->d_tw, tw.data(), sizeof(TwD) * tw.size(), cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(c->d_pinv, pinv.data(), sizeof(TwPair) * nq, cudaMemcpyHostToDevice);
   if (e == cudaSuccess)

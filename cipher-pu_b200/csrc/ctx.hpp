@@ -22,19 +22,13 @@ struct ckks_ctx {
   std::vector<int> has_nega;
   std::vector<PrimeInfo> h_pi;
   PrimeInfo* d_pi = nullptr;  // [n_primes]
-  TwPair* d_tw = nullptr;     // [n_primes][4][n]: fwd, inv, fwd cyclic, inv cyclic
+  TwD* d_tw = nullptr;        // [n_primes][TWF_SLOTS][n]: FP64 NTT tables (common.cuh)
   TwPair* d_pinv = nullptr;   // [n_q]: special^-1 mod q_i (zeros when n_special == 0)
   TwPair* d_qtinv = nullptr;  // [n_q][n_q]: q_t^-1 mod q_i at [t][i], i < t
   TwPair* d_misc = nullptr;   // [n_primes][4]: (1, one_s) helpers; slot 1: R mod q
   std::vector<std::vector<u64>> h_qtinv;  // host copies
   std::vector<u64> h_pinv;
-
-  const TwPair* tw(int prime, int which) const {
-    return d_tw + ((size_t)prime * 4 + which) * (size_t)n;
-  }
 };
-
-enum { TW_FWD = 0, TW_INV = 1, TW_FWD_CYC = 2, TW_INV_CYC = 3 };
 
 // ---------------------------------------------------------------- errors
 int ckks_set_error(int code, const char* fmt, ...);
@@ -61,6 +55,12 @@ static inline u64 h_powmod(u64 b, u64 e, u64 q) {
 }
 static inline u64 h_invmod(u64 a, u64 q) { return h_powmod(a % q, q - 2, q); }  // q prime
 static inline u64 h_shoup(u64 w, u64 q) { return (u64)(((unsigned __int128)w << 64) / q); }
+static inline TwD h_twd(u64 w, u64 q) {
+  TwD t;
+  t.w = (double)(w % q);
+  t.wq = t.w / (double)q;
+  return t;
+}
 static inline TwPair h_twp(u64 w, u64 q) {
   TwPair t;
   t.w = w % q;

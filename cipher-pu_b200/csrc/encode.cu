@@ -238,7 +238,7 @@ extern "C" int ckks_decode(const ckks_ctx* ctx, double* slots, const uint64_t* i
 template <int LOGN, int K>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     k_decrypt(u64* __restrict__ out, const u64* __restrict__ ct, const u64* __restrict__ s_eval,
-              int level, const PrimeInfo* __restrict__ pi, const TwPair* __restrict__ tw) {
+              int level, const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
@@ -254,7 +254,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   load_z<LOGN, K>(s, s_eval + (size_t)i * N, tid);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) x[e] = addmod(x[e], mulmod(y[e], s[e], P), P.q);
-  ntt_inv<LOGN, K>(x, sm, tid, tw + ((size_t)i * 4 + TW_INV) * N, P);
+  ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
   store_c<LOGN, K>(x, out + c * LN + (size_t)i * N, tid);
 }
 
@@ -286,7 +286,7 @@ template <int LOGN, int K>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     k_encrypt(u64* __restrict__ out, const u64* __restrict__ m_eval, const u64* __restrict__ s_eval,
               const u64* __restrict__ a, const long long* __restrict__ err, int level,
-              const PrimeInfo* __restrict__ pi, const TwPair* __restrict__ tw) {
+              const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
@@ -302,7 +302,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     long long v = ep[posC<LOGN, K>(tid, e)] % (long long)P.q;
     x[e] = (u64)(v < 0 ? v + (long long)P.q : v);
   }
-  ntt_fwd<LOGN, K>(x, sm, tid, tw + ((size_t)i * 4 + TW_FWD) * N, P);
+  ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
   u64 av[Sh::E], sv[Sh::E];
   load_z<LOGN, K>(av, a + c * LN + (size_t)i * N, tid);
   load_z<LOGN, K>(sv, s_eval + (size_t)i * N, tid);
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     k_dare_out(u64* __restrict__ out, const u64* __restrict__ dec, const u64* __restrict__ s_eval,
                const u64* __restrict__ a, const long long* __restrict__ err, int level_in,
                int level_out, DareConsts D, const PrimeInfo* __restrict__ pi,
-               const TwPair* __restrict__ tw) {
+               const TwD* __restrict__ tw) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
@@ -419,7 +419,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     }
     x[e] = res;
   }
-  ntt_fwd<LOGN, K>(x, sm, tid, tw + ((size_t)j * 4 + TW_FWD) * N, P);
+  ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, j), P);
   const size_t LN = (size_t)level_out * N;
   u64 av[Sh::E], sv[Sh::E];
   load_z<LOGN, K>(av, a + c * LN + (size_t)j * N, tid);

@@ -1,5 +1,13 @@
 // ntt.cuh - one-CTA negacyclic / cyclic NTT over Z_q[X]/(X^N +- 1) for
-// sm_100a, 64-bit coefficients, N = 2^LOGN.
+// sm_100a, N = 2^LOGN, primes q < 2^47.
+//
+// Arithmetic: exact FP64.  Residues below 2^52 are exact doubles; a twiddle
+// product y * w mod q is formed as hi = y w (rounded) plus lo = fma(y, w, -hi)
+// (the exact rounding error), the quotient qt = round(y * (w / q)) comes from
+// one FMA against 1.5 * 2^52, and r = fma(-qt, q, hi) + lo is exact with
+// |r| <= q.  On B200 this double-word product runs at twice the rate of the
+// integer Shoup product (measured by ckks_modmul_peak), and the butterflies
+// need no integer compare / select at all: values are kept signed and lazy.
 //
 // Each thread owns E = 2^K coefficients in registers.  The LOGN butterfly
 // stages are grouped into passes of at most K stages; inside a pass all
@@ -9,9 +17,12 @@
 //
 // Forward: Cooley-Tukey, natural-order coefficients in, evaluations in
 // bit-reversed order out; twiddle tw[m + i] for group i of stage m (merged
-// psi form; Harvey lazy butterflies with values in [0, 4q)).
-// Inverse: Gentleman-Sande with the inverse table, bit-reversed in, natural
-// out, then * N^-1 (values in [0, 2q) throughout).
+// psi form).  |x| grows by at most q per stage.
+// Inverse: the input is the bit-reversed evaluation vector, so the cyclic
+// inverse DFT is a decimation-in-time Cooley-Tukey (distance 1, 2, ... N/2,
+// pair (p, p + h) with twiddle omega^-(p mod h) * N/(2h)); the negacyclic
+// untwist psi^-j and N^-1 are one closing multiply by post[j] = N^-1 psi^-j.
+// Growth is again at most q per stage, so nothing is reduced until the end.
 //
 // Register layouts:
 //   layout "C" (pass 0): thread t holds positions t + T*r        (coalesced)
@@ -20,7 +31,8 @@
 // The forward transform takes layout C and returns layout Z; the inverse
 // takes Z and returns C.  Positions are element indices of the polynomial,
 // so a caller may load / store in either layout without changing the data
-// order in memory.
+// order in memory.  Both transforms take canonical residues in [0, q) (the
+// forward also accepts any value below 4q) and return canonical residues.
 #pragma once
 #include "common.cuh"
 
@@ -41,7 +53,6 @@ struct NttShape {
     for (int i = 0; i < p; ++i) s += kp(i);
     return s;
   }
-  __host__ __device__ static constexpr int last() { return NP; }
 };
 
 __device__ __forceinline__ int padix(int p, int sh) { return p + (p >> sh); }
@@ -59,7 +70,6 @@ __device__ __forceinline__ int pass_pos(int tid, int c, int r) {
   return block * BSZ + off + DMIN * r;
 }
 
-// Position of register index e (0..E-1) in layout C / layout Z.
 template <int LOGN, int K>
 __device__ __forceinline__ int posC(int tid, int e) {
   return tid + (NttShape<LOGN, K>::T) * e;
@@ -73,33 +83,52 @@ __device__ __forceinline__ int posZ(int tid, int e) {
   return pass_pos<LOGN, K, S0, KP>(tid, e >> KP, e & ((1 << KP) - 1));
 }
 
-// ---------------------------------------------------------------- butterflies
-// No per-butterfly reduction: with q < 2^47 the 64-bit words have room for
-// the growth.  Forward (Cooley-Tukey): t = w y mod q lands in [0, 2q), so
-// both outputs grow by at most 2q per stage (x + t, x + 2q - t); after the
-// LOGN <= 14 stages a value below B_in is below B_in + 28q.  Inverse
-// (Gentleman-Sande): the difference branch is re-reduced by the Shoup
-// multiply to [0, 2q) while the sum branch at most doubles, so the input of
-// the stage run d-th is below 2q * 2^d; the difference is offset by that
-// bound (bs) to stay non-negative.  After LOGN stages values are below
-// 2q * 2^14 < 2^62, and the closing N^-1 Shoup multiply accepts any word.
-__device__ __forceinline__ void ct_bfly(u64& x, u64& y, const TwPair& w, u64 q, u64 q2) {
-  const u64 t = shoup_lazy(y, w.w, w.ws, q);
-  const u64 xr = x;
-  x = xr + t;
-  y = xr + q2 - t;
+// ---------------------------------------------------------------- FP64 modular arithmetic
+#define CKKS_FP_MAGIC 6755399441055744.0  // 1.5 * 2^52: fma(a, b, M) - M = round(a b)
+#define CKKS_FP_TWO52 4503599627370496.0
+
+__device__ __forceinline__ TwD ldtwd(const TwD* p) {
+  const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  TwD t;
+  t.w = v.x;
+  t.wq = v.y;
+  return t;
 }
 
-__device__ __forceinline__ void gs_bfly(u64& x, u64& y, const TwPair& w, u64 q, u64 bs) {
-  const u64 u = x + y;
-  const u64 v = x + bs - y;
-  x = u;
-  y = shoup_lazy(v, w.w, w.ws, q);
+// y * w mod q up to a multiple of q: exact, |result| <= q, for |y| < 2^51.
+__device__ __forceinline__ double fmulmod(double y, double w, double wq, double qd) {
+  const double hi = __dmul_rn(y, w);
+  const double lo = __fma_rn(y, w, -hi);
+  const double qt = __dadd_rn(__fma_rn(y, wq, CKKS_FP_MAGIC), -CKKS_FP_MAGIC);
+  return __dadd_rn(__fma_rn(-qt, qd, hi), lo);
 }
 
+// u64 residue (< 2^52) -> exact double
+__device__ __forceinline__ double u2d(u64 x) {
+  return __dadd_rn(__longlong_as_double((long long)(x | 0x4330000000000000ull)), -CKKS_FP_TWO52);
+}
+
+// exact integer double with |x| < 2^51 -> canonical residue in [0, q)
+__device__ __forceinline__ u64 d2canon(double x, double qd, double qinv) {
+  const double qt = __dadd_rn(__fma_rn(x, qinv, CKKS_FP_MAGIC), -CKKS_FP_MAGIC);
+  double r = __fma_rn(-qt, qd, x);  // |r| <= q/2 + 1
+  r = r < 0.0 ? __dadd_rn(r, qd) : r;
+  r = r >= qd ? __dadd_rn(r, -qd) : r;
+  return (u64)__double_as_longlong(__dadd_rn(r, CKKS_FP_TWO52)) & 0x000FFFFFFFFFFFFFull;
+}
+
+// ---------------------------------------------------------------- passes
+__device__ __forceinline__ void ct_bfly_fp(double& x, double& y, const TwD& w, double qd) {
+  const double t = fmulmod(y, w.w, w.wq, qd);
+  const double xr = x;
+  x = __dadd_rn(xr, t);
+  y = __dadd_rn(xr, -t);
+}
+
+// forward pass: stages S0 .. S0+KP-1, group-uniform twiddles tw[m + i]
 template <int LOGN, int K, int S0, int KP>
-__device__ __forceinline__ void fwd_pass(u64 (&x)[1 << K], int tid, const TwPair* __restrict__ tw,
-                                         u64 q, u64 q2) {
+__device__ __forceinline__ void fwd_pass(double (&x)[1 << K], int tid, const TwD* __restrict__ tw,
+                                         double qd) {
   constexpr int N = 1 << LOGN;
   constexpr int T = N >> K;
   constexpr int BSZ = N >> S0;
@@ -115,20 +144,22 @@ __device__ __forceinline__ void fwd_pass(u64 (&x)[1 << K], int tid, const TwPair
       const int half = RR >> (u + 1);
 #pragma unroll
       for (int grp = 0; grp < (1 << u); ++grp) {
-        const TwPair w = ldtw(tw + (1 << (S0 + u)) + block * (1 << u) + grp);
+        const TwD w = ldtwd(tw + (1 << (S0 + u)) + block * (1 << u) + grp);
 #pragma unroll
         for (int j = 0; j < half; ++j) {
           const int r = grp * 2 * half + j;
-          ct_bfly(x[c * RR + r], x[c * RR + r + half], w, q, q2);
+          ct_bfly_fp(x[c * RR + r], x[c * RR + r + half], w, qd);
         }
       }
     }
   }
 }
 
+// inverse (DIT) pass: stages S0+KP-1 down to S0 (distances ascending);
+// the pair (p, p + h) at stage s uses itw[(p mod h) << s], h = N >> (s + 1)
 template <int LOGN, int K, int S0, int KP>
-__device__ __forceinline__ void inv_pass(u64 (&x)[1 << K], int tid, const TwPair* __restrict__ itw,
-                                         u64 q, u64 q2) {
+__device__ __forceinline__ void inv_pass(double (&x)[1 << K], int tid, const TwD* __restrict__ itw,
+                                         double qd) {
   constexpr int N = 1 << LOGN;
   constexpr int T = N >> K;
   constexpr int BSZ = N >> S0;
@@ -138,18 +169,18 @@ __device__ __forceinline__ void inv_pass(u64 (&x)[1 << K], int tid, const TwPair
 #pragma unroll
   for (int c = 0; c < SUBS; ++c) {
     const int g = tid + T * c;
-    const int block = g / DMIN;
+    const int off = g % DMIN;
 #pragma unroll
     for (int u = KP - 1; u >= 0; --u) {
       const int half = RR >> (u + 1);
-      const u64 bs = q2 << (LOGN - 1 - (S0 + u));  // input bound of this stage
+      const int s = S0 + u;
 #pragma unroll
-      for (int grp = 0; grp < (1 << u); ++grp) {
-        const TwPair w = ldtw(itw + (1 << (S0 + u)) + block * (1 << u) + grp);
+      for (int j = 0; j < half; ++j) {
+        const TwD w = ldtwd(itw + ((off + DMIN * j) << s));
 #pragma unroll
-        for (int j = 0; j < half; ++j) {
+        for (int grp = 0; grp < (1 << u); ++grp) {
           const int r = grp * 2 * half + j;
-          gs_bfly(x[c * RR + r], x[c * RR + r + half], w, q, bs);
+          ct_bfly_fp(x[c * RR + r], x[c * RR + r + half], w, qd);
         }
       }
     }
@@ -157,7 +188,7 @@ __device__ __forceinline__ void inv_pass(u64 (&x)[1 << K], int tid, const TwPair
 }
 
 template <int LOGN, int K, int S0, int KP>
-__device__ __forceinline__ void sm_store(const u64 (&x)[1 << K], u64* sm, int tid) {
+__device__ __forceinline__ void sm_store(const double (&x)[1 << K], double* sm, int tid) {
   constexpr int SUBS = 1 << (K - KP);
   constexpr int RR = 1 << KP;
   constexpr int SH = NttShape<LOGN, K>::PADSH;
@@ -168,7 +199,7 @@ __device__ __forceinline__ void sm_store(const u64 (&x)[1 << K], u64* sm, int ti
 }
 
 template <int LOGN, int K, int S0, int KP>
-__device__ __forceinline__ void sm_load(u64 (&x)[1 << K], const u64* sm, int tid) {
+__device__ __forceinline__ void sm_load(double (&x)[1 << K], const double* sm, int tid) {
   constexpr int SUBS = 1 << (K - KP);
   constexpr int RR = 1 << KP;
   constexpr int SH = NttShape<LOGN, K>::PADSH;
@@ -178,98 +209,86 @@ __device__ __forceinline__ void sm_load(u64 (&x)[1 << K], const u64* sm, int tid
     for (int r = 0; r < RR; ++r) x[c * RR + r] = sm[padix(pass_pos<LOGN, K, S0, KP>(tid, c, r), SH)];
 }
 
-// forward passes 1..NP (pass 0 done by caller-side helper below)
 template <int LOGN, int K, int P>
 struct FwdRest {
-  __device__ __forceinline__ static void run(u64 (&x)[1 << K], u64* sm, int tid,
-                                             const TwPair* __restrict__ tw, u64 q, u64 q2) {
+  __device__ __forceinline__ static void run(double (&x)[1 << K], double* sm, int tid,
+                                             const TwD* __restrict__ tw, double qd) {
     using S = NttShape<LOGN, K>;
     if constexpr (P <= S::NP) {
       sm_store<LOGN, K, S::s0(P - 1), S::kp(P - 1)>(x, sm, tid);
       __syncthreads();
       sm_load<LOGN, K, S::s0(P), S::kp(P)>(x, sm, tid);
       __syncthreads();
-      fwd_pass<LOGN, K, S::s0(P), S::kp(P)>(x, tid, tw, q, q2);
-      FwdRest<LOGN, K, P + 1>::run(x, sm, tid, tw, q, q2);
+      fwd_pass<LOGN, K, S::s0(P), S::kp(P)>(x, tid, tw, qd);
+      FwdRest<LOGN, K, P + 1>::run(x, sm, tid, tw, qd);
     }
   }
 };
 
-// inverse passes NP..1 (descending), then pass 0
 template <int LOGN, int K, int P>
 struct InvRest {
-  __device__ __forceinline__ static void run(u64 (&x)[1 << K], u64* sm, int tid,
-                                             const TwPair* __restrict__ itw, u64 q, u64 q2) {
+  __device__ __forceinline__ static void run(double (&x)[1 << K], double* sm, int tid,
+                                             const TwD* __restrict__ itw, double qd) {
     using S = NttShape<LOGN, K>;
     if constexpr (P >= 1) {
-      inv_pass<LOGN, K, S::s0(P), S::kp(P)>(x, tid, itw, q, q2);
+      inv_pass<LOGN, K, S::s0(P), S::kp(P)>(x, tid, itw, qd);
       sm_store<LOGN, K, S::s0(P), S::kp(P)>(x, sm, tid);
       __syncthreads();
       sm_load<LOGN, K, S::s0(P - 1), S::kp(P - 1)>(x, sm, tid);
       __syncthreads();
-      InvRest<LOGN, K, P - 1>::run(x, sm, tid, itw, q, q2);
+      InvRest<LOGN, K, P - 1>::run(x, sm, tid, itw, qd);
     }
   }
 };
 
-// Forward NTT: x in layout C with values below 4q -> layout Z, values below
-// 4q + 2q LOGN <= 32q (see the butterfly notes); callers that subtract a
-// transformed value add LAZY_FWD_BOUND(q) first.
-__device__ __forceinline__ u64 lazy_fwd_bound(u64 q) { return q << 5; }
+// Per-prime table base: tb = tw + prime * TWF_SLOTS * N.
+template <int LOGN>
+__device__ __forceinline__ const TwD* twbase(const TwD* tw, int prime) {
+  return tw + (size_t)prime * TWF_SLOTS * (1 << LOGN);
+}
 
+// Forward NTT: layout C in (values < 4q), layout Z out, canonical [0, q).
+template <int LOGN, int K>
+__device__ __forceinline__ void ntt_fwd(u64 (&x)[1 << K], u64* sm, int tid, const TwD* __restrict__ tb,
+                                        const PrimeInfo& P, bool cyclic = false) {
+  constexpr int N = 1 << LOGN;
+  const TwD* tw = tb + (cyclic ? TWF_FWD_CYC : TWF_FWD) * N;
+  double d[1 << K];
+#pragma unroll
+  for (int e = 0; e < (1 << K); ++e) d[e] = u2d(x[e]);
+  double* smd = reinterpret_cast<double*>(sm);
+  fwd_pass<LOGN, K, 0, K>(d, tid, tw, P.qd);
+  FwdRest<LOGN, K, 1>::run(d, smd, tid, tw, P.qd);
+#pragma unroll
+  for (int e = 0; e < (1 << K); ++e) x[e] = d2canon(d[e], P.qd, P.qinv_d);
+}
+
+// Historical name kept for the call sites: the FP64 forward already returns
+// canonical residues.
 template <int LOGN, int K>
 __device__ __forceinline__ void ntt_fwd_lazy(u64 (&x)[1 << K], u64* sm, int tid,
-                                             const TwPair* __restrict__ tw, u64 q, u64 q2) {
-  fwd_pass<LOGN, K, 0, K>(x, tid, tw, q, q2);
-  FwdRest<LOGN, K, 1>::run(x, sm, tid, tw, q, q2);
+                                             const TwD* __restrict__ tb, const PrimeInfo& P) {
+  ntt_fwd<LOGN, K>(x, sm, tid, tb, P);
 }
 
-// Forward NTT with the result reduced to [0, q).
+// Inverse NTT (with N^-1): layout Z in (canonical), layout C out, canonical.
 template <int LOGN, int K>
-__device__ __forceinline__ void ntt_fwd(u64 (&x)[1 << K], u64* sm, int tid,
-                                        const TwPair* __restrict__ tw, const PrimeInfo& P) {
-  ntt_fwd_lazy<LOGN, K>(x, sm, tid, tw, P.q, P.q2);
+__device__ __forceinline__ void ntt_inv(u64 (&x)[1 << K], u64* sm, int tid, const TwD* __restrict__ tb,
+                                        const PrimeInfo& P, bool cyclic = false) {
+  constexpr int N = 1 << LOGN;
+  const TwD* itw = tb + (cyclic ? TWF_INV_CYC : TWF_INV) * N;
+  const TwD* post = tb + (cyclic ? TWF_POST_CYC : TWF_POST) * N;
+  double d[1 << K];
 #pragma unroll
-  for (int e = 0; e < (1 << K); ++e) x[e] = reduce_any(x[e], P);
-}
-
-// Inverse NTT: x in layout Z with values in [0, 2q) -> layout C, values in [0, q),
-// multiplied by N^-1.
-template <int LOGN, int K>
-__device__ __forceinline__ void ntt_inv(u64 (&x)[1 << K], u64* sm, int tid,
-                                        const TwPair* __restrict__ itw, const PrimeInfo& P) {
-  InvRest<LOGN, K, NttShape<LOGN, K>::NP>::run(x, sm, tid, itw, P.q, P.q2);
-  inv_pass<LOGN, K, 0, K>(x, tid, itw, P.q, P.q2);
+  for (int e = 0; e < (1 << K); ++e) d[e] = u2d(x[e]);
+  double* smd = reinterpret_cast<double*>(sm);
+  InvRest<LOGN, K, NttShape<LOGN, K>::NP>::run(d, smd, tid, itw, P.qd);
+  inv_pass<LOGN, K, 0, K>(d, tid, itw, P.qd);
 #pragma unroll
-  for (int e = 0; e < (1 << K); ++e) x[e] = csub(shoup_lazy(x[e], P.ninv, P.ninv_s, P.q), P.q);
-}
-
-// Layout-Z global access: the last pass has unit stride inside each run, so
-// registers (e, e+1) with e even are adjacent words; move them as 16-byte vectors.
-template <int LOGN, int K>
-__device__ __forceinline__ void load_z(u64 (&x)[1 << K], const u64* __restrict__ src, int tid) {
-#pragma unroll
-  for (int e = 0; e < (1 << K); e += 2) {
-    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(src + posZ<LOGN, K>(tid, e)));
-    x[e] = v.x;
-    x[e + 1] = v.y;
+  for (int e = 0; e < (1 << K); ++e) {
+    const TwD pw = ldtwd(post + posC<LOGN, K>(tid, e));
+    x[e] = d2canon(fmulmod(d[e], pw.w, pw.wq, P.qd), P.qd, P.qinv_d);
   }
-}
-template <int LOGN, int K>
-__device__ __forceinline__ void store_z(const u64 (&x)[1 << K], u64* __restrict__ dst, int tid) {
-#pragma unroll
-  for (int e = 0; e < (1 << K); e += 2)
-    *reinterpret_cast<ulonglong2*>(dst + posZ<LOGN, K>(tid, e)) = make_ulonglong2(x[e], x[e + 1]);
-}
-template <int LOGN, int K>
-__device__ __forceinline__ void load_c(u64 (&x)[1 << K], const u64* __restrict__ src, int tid) {
-#pragma unroll
-  for (int e = 0; e < (1 << K); ++e) x[e] = __ldg(src + posC<LOGN, K>(tid, e));
-}
-template <int LOGN, int K>
-__device__ __forceinline__ void store_c(const u64 (&x)[1 << K], u64* __restrict__ dst, int tid) {
-#pragma unroll
-  for (int e = 0; e < (1 << K); ++e) dst[posC<LOGN, K>(tid, e)] = x[e];
 }
 
 // Layout-Z global access: the last pass has unit stride inside each run, so

@@ -7,7 +7,7 @@
 template <int LOGN, int K>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     k_ntt(u64* __restrict__ data, int n_limbs, int prime_begin, const PrimeInfo* __restrict__ pi,
-          const TwPair* __restrict__ tw, int inverse, int cyclic) {
+          const TwD* __restrict__ tw, int inverse, int cyclic) {
   extern __shared__ u64 sm[];
   using S = NttShape<LOGN, K>;
   const int limb = blockIdx.x % n_limbs;
@@ -15,20 +15,20 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   const int pidx = prime_begin + limb;
   const PrimeInfo P = pi[pidx];
   u64* d = data + ((size_t)poly * n_limbs + limb) * S::N;
-  const TwPair* t = tw + ((size_t)pidx * 4 + (cyclic ? 2 : 0) + (inverse ? 1 : 0)) * S::N;
+  const TwD* tb = twbase<LOGN>(tw, pidx);
   const int tid = threadIdx.x;
   u64 x[S::E];
   if (!inverse) {
 #pragma unroll
-    for (int e = 0; e < S::E; ++e) x[e] = d[posC<LOGN, K>(tid, e)];
-    ntt_fwd<LOGN, K>(x, sm, tid, t, P);
+    for (int e = 0; e < S::E; ++e) x[e] = reduce_any(d[posC<LOGN, K>(tid, e)], P);
+    ntt_fwd<LOGN, K>(x, sm, tid, tb, P, cyclic);
     if constexpr (S::NP == 0) __syncthreads();
 #pragma unroll
     for (int e = 0; e < S::E; ++e) d[posZ<LOGN, K>(tid, e)] = x[e];
   } else {
 #pragma unroll
-    for (int e = 0; e < S::E; ++e) x[e] = d[posZ<LOGN, K>(tid, e)];
-    ntt_inv<LOGN, K>(x, sm, tid, t, P);
+    for (int e = 0; e < S::E; ++e) x[e] = reduce_any(d[posZ<LOGN, K>(tid, e)], P);
+    ntt_inv<LOGN, K>(x, sm, tid, tb, P, cyclic);
     if constexpr (S::NP == 0) __syncthreads();
 #pragma unroll
     for (int e = 0; e < S::E; ++e) d[posC<LOGN, K>(tid, e)] = x[e];
@@ -136,7 +136,7 @@ template <int LOGN, int K>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     k_poly_mul(u64* __restrict__ out, const u64* __restrict__ a, const u64* __restrict__ b,
                int n_limbs, int prime_begin, const PrimeInfo* __restrict__ pi,
-               const TwPair* __restrict__ tw, int cyclic) {
+               const TwD* __restrict__ tw, int cyclic) {
   extern __shared__ u64 sm[];
   using S = NttShape<LOGN, K>;
   const int limb = blockIdx.x % n_limbs;
@@ -144,22 +144,20 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   const int pidx = prime_begin + limb;
   const PrimeInfo P = pi[pidx];
   const size_t off = ((size_t)poly * n_limbs + limb) * S::N;
-  const TwPair* tf = tw + ((size_t)pidx * 4 + (cyclic ? 2 : 0)) * S::N;
-  const TwPair* ti = tf + S::N;
+  const TwD* tb = twbase<LOGN>(tw, pidx);
   const int tid = threadIdx.x;
   u64 x[S::E], y[S::E];
 #pragma unroll
-  for (int e = 0; e < S::E; ++e) x[e] = a[off + posC<LOGN, K>(tid, e)];
-  ntt_fwd_lazy<LOGN, K>(x, sm, tid, tf, P.q, P.q2);
+  for (int e = 0; e < S::E; ++e) x[e] = reduce_any(a[off + posC<LOGN, K>(tid, e)], P);
+  ntt_fwd<LOGN, K>(x, sm, tid, tb, P, cyclic);
   __syncthreads();
 #pragma unroll
-  for (int e = 0; e < S::E; ++e) y[e] = b[off + posC<LOGN, K>(tid, e)];
-  ntt_fwd_lazy<LOGN, K>(y, sm, tid, tf, P.q, P.q2);
+  for (int e = 0; e < S::E; ++e) y[e] = reduce_any(b[off + posC<LOGN, K>(tid, e)], P);
+  ntt_fwd<LOGN, K>(y, sm, tid, tb, P, cyclic);
 #pragma unroll
-  for (int e = 0; e < S::E; ++e)
-    x[e] = mulmod(x[e], y[e], P);  // lazy inputs < 32q: a b < q 2^64 holds
+  for (int e = 0; e < S::E; ++e) x[e] = mulmod(x[e], y[e], P);
   __syncthreads();
-  ntt_inv<LOGN, K>(x, sm, tid, ti, P);
+  ntt_inv<LOGN, K>(x, sm, tid, tb, P, cyclic);
 #pragma unroll
   for (int e = 0; e < S::E; ++e) out[off + posC<LOGN, K>(tid, e)] = x[e];
 }
@@ -212,7 +210,7 @@ struct GarnerConsts {
 template <int LOGN, int K>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     k_poly_mul_anyq(u64* __restrict__ out, const u64* __restrict__ a, const u64* __restrict__ b,
-                    const PrimeInfo* __restrict__ pi, const TwPair* __restrict__ tw, int cyclic,
+                    const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int cyclic,
                     GarnerConsts G) {
   extern __shared__ u64 sm[];
   using S = NttShape<LOGN, K>;
@@ -223,21 +221,19 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
 #pragma unroll 1
   for (int k = 0; k < 3; ++k) {
     const PrimeInfo P = pi[k];
-    const TwPair* tf = tw + ((size_t)k * 4 + (cyclic ? 2 : 0)) * S::N;
-    const TwPair* ti = tf + S::N;
+    const TwD* tb = twbase<LOGN>(tw, k);
     u64 x[S::E], y[S::E];
 #pragma unroll
     for (int e = 0; e < S::E; ++e) x[e] = reduce_any(mod_anyq(a[off + posC<LOGN, K>(tid, e)], G.q, G.qd), P);
-    ntt_fwd_lazy<LOGN, K>(x, sm, tid, tf, P.q, P.q2);
+    ntt_fwd<LOGN, K>(x, sm, tid, tb, P, cyclic);
     __syncthreads();
 #pragma unroll
     for (int e = 0; e < S::E; ++e) y[e] = reduce_any(mod_anyq(b[off + posC<LOGN, K>(tid, e)], G.q, G.qd), P);
-    ntt_fwd_lazy<LOGN, K>(y, sm, tid, tf, P.q, P.q2);
+    ntt_fwd<LOGN, K>(y, sm, tid, tb, P, cyclic);
 #pragma unroll
-    for (int e = 0; e < S::E; ++e)
-      x[e] = mulmod(x[e], y[e], P);  // lazy inputs < 32q: a b < q 2^64 holds
+    for (int e = 0; e < S::E; ++e) x[e] = mulmod(x[e], y[e], P);
     __syncthreads();
-    ntt_inv<LOGN, K>(x, sm, tid, ti, P);
+    ntt_inv<LOGN, K>(x, sm, tid, tb, P, cyclic);
     __syncthreads();
 #pragma unroll
     for (int e = 0; e < S::E; ++e) r[k][e] = x[e];
@@ -306,29 +302,28 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     k_relin_single(u64* __restrict__ f0, u64* __restrict__ f1, const u64* __restrict__ e0,
                    const u64* __restrict__ e1, const u64* __restrict__ e2,
                    const u64* __restrict__ ka, const u64* __restrict__ kb, int prime,
-                   const PrimeInfo* __restrict__ pi, const TwPair* __restrict__ tw) {
+                   const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw) {
   extern __shared__ u64 sm[];
   using S = NttShape<LOGN, K>;
   const size_t off = (size_t)blockIdx.x * S::N;
   const PrimeInfo P = pi[prime];
-  const TwPair* tf = tw + (size_t)prime * 4 * S::N;
-  const TwPair* ti = tf + S::N;
+  const TwD* tb = twbase<LOGN>(tw, prime);
   const int tid = threadIdx.x;
   u64 x[S::E], y[S::E];
 #pragma unroll
-  for (int e = 0; e < S::E; ++e) x[e] = e2[off + posC<LOGN, K>(tid, e)];
-  ntt_fwd<LOGN, K>(x, sm, tid, tf, P);
+  for (int e = 0; e < S::E; ++e) x[e] = reduce_any(e2[off + posC<LOGN, K>(tid, e)], P);
+  ntt_fwd<LOGN, K>(x, sm, tid, tb, P);
 #pragma unroll 1
   for (int pass = 0; pass < 2; ++pass) {
     const u64* key = pass == 0 ? kb : ka;
     __syncthreads();
 #pragma unroll
-    for (int e = 0; e < S::E; ++e) y[e] = key[off + posC<LOGN, K>(tid, e)];
-    ntt_fwd<LOGN, K>(y, sm, tid, tf, P);
+    for (int e = 0; e < S::E; ++e) y[e] = reduce_any(key[off + posC<LOGN, K>(tid, e)], P);
+    ntt_fwd<LOGN, K>(y, sm, tid, tb, P);
 #pragma unroll
     for (int e = 0; e < S::E; ++e) y[e] = mulmod(x[e], y[e], P);
     __syncthreads();
-    ntt_inv<LOGN, K>(y, sm, tid, ti, P);
+    ntt_inv<LOGN, K>(y, sm, tid, tb, P);
     const u64* ein = pass == 0 ? e0 : e1;
     u64* fo = pass == 0 ? f0 : f1;
 #pragma unroll

@@ -77,7 +77,7 @@ extern "C" int ckks_rescale_scaled(uint64_t* out, const uint64_t* in, int64_t n,
 template <int LOGN, int K>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     k_rescale_rns(u64* __restrict__ out, const u64* __restrict__ in, int level,
-                  const PrimeInfo* __restrict__ pi, const TwPair* __restrict__ tw,
+                  const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw,
                   const TwPair* __restrict__ qtinv, int nq) {
   extern __shared__ u64 sm[];
   using S = NttShape<LOGN, K>;
@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   u64 w[S::E];
 #pragma unroll
   for (int e = 0; e < S::E; ++e) w[e] = src[(size_t)t * S::N + posZ<LOGN, K>(tid, e)];
-  ntt_inv<LOGN, K>(w, sm, tid, tw + ((size_t)t * 4 + TW_INV) * S::N, PT);
+  ntt_inv<LOGN, K>(w, sm, tid, twbase<LOGN>(tw, t), PT);
 #pragma unroll 1
   for (int i = 0; i < t; ++i) {
     const PrimeInfo P = pi[i];
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
 #pragma unroll
     for (int e = 0; e < S::E; ++e) x[e] = w[e] > PT.half ? w[e] - PT.q + P.q : w[e];  // [w_c]_{q_i}
     __syncthreads();
-    ntt_fwd_lazy<LOGN, K>(x, sm, tid, tw + ((size_t)i * 4 + TW_FWD) * S::N, P.q, P.q2);
+    ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
 #pragma unroll
     for (int e = 0; e < S::E; ++e) {
       const int p = posZ<LOGN, K>(tid, e);
