@@ -174,6 +174,22 @@ def stage_bytes(stage: int, n: int, level: int) -> int:
     return 6 * level * w
 
 
+def stage_modmuls(stage: int, n: int, level: int) -> int:
+    """Modular multiplies of each ct-mult kernel per ciphertext pair.  One
+    transform of N points is (N/2) log2 N butterflies, each one twiddle
+    product; an inverse adds its closing N^-1 psi^-j multiply."""
+    logn = n.bit_length() - 1
+    fwd = (n // 2) * logn
+    inv = fwd + n
+    if stage == 0:   # per limb: 3 Karatsuba products + INTT(d2)
+        return level * (3 * n + inv)
+    if stage == 1:   # L^2 NTTs (each digit to every other prime and p) + 2 key products per digit and prime
+        return level * level * fwd + (level + 1) * level * 2 * n
+    # per poly: INTT_p, NTT_t, p^-1, INTT_t, then per limb i < t: NTT_i + 3 products
+    t = level - 1
+    return 2 * (inv + fwd + n + inv + t * (fwd + 3 * n))
+
+
 def run_ours(a) -> int:
     import torch
     ws, rank, local = dist_env()
@@ -314,6 +330,11 @@ def run_ours(a) -> int:
         except Exception:
             pass
         tot_ms = sum(s[0] for s in stages)
+        # FP64 modular-multiply pipe: the butterflies' arithmetic bound, against
+        # the double-word modmul throughput measured on this GPU just now
+        from ckks_b200.peak import modmul_peak
+        mm_peak = modmul_peak(kind=1) / 1e12
+        mm_ach = stage_modmuls(dom, n, L) * B / (per_launch_ms / 1000.0) / 1e12
         cpu = None
         if ws == 1 and not a.no_cpu_baseline:
             from oracle import cpu_baseline
@@ -331,6 +352,10 @@ def run_ours(a) -> int:
                          "peak_source": f"{peak_src} hbm_gbs",
                          "algorithmic_bytes_per_launch": alg,
                          "avg_launch_ms": per_launch_ms},
+            "roofline_fp64": {"bound": "fp64 modmul", "kernel": names[dom], "achieved": mm_ach,
+                              "peak": mm_peak, "unit": "Tmodmul/s", "frac": mm_ach / mm_peak,
+                              "modmuls_per_launch": stage_modmuls(dom, n, L) * B,
+                              "peak_source": "measured live: ckks_modmul_peak kind 1 (FP64 double-word)"},
             "stage_ms_per_step": {names[s]: stages[s][0] / max(1, a.steps) for s in range(3)},
             "stage_share": {names[s]: (stages[s][0] / tot_ms if tot_ms else None) for s in range(3)},
             "cpu_baseline": cpu,

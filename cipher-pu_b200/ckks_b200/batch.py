@@ -8,7 +8,7 @@ polynomial limb, so the buckets of different shapes need no padding).  The
 buckets are spread over a pool of streams and the whole plan is captured
 once into a CUDA graph, so a step costs one graph launch.  The autotuner
 times every bucket alone under each launch shape (per-thread radix 2^K,
-register budget for 1 or 2 CTAs per SM, chunking of the bucket into
+balanced or tight register budget, chunking of the bucket into
 launches) and keeps the fastest; the choice is baked into the graph at
 capture time.
 
@@ -57,7 +57,7 @@ class Bucket:
     b: torch.Tensor = None          # second ciphertext (ctct) or plaintext (ctpt)
     out: torch.Tensor = None
     scratch: torch.Tensor = None
-    tune: dict = field(default_factory=lambda: {"k": 3, "minb": 1, "chunk": 0})
+    tune: dict = field(default_factory=lambda: {"k": 0, "minb": 0, "chunk": 0})
 
 
 class BatchExecutor:
@@ -161,11 +161,11 @@ class BatchExecutor:
         """Time each bucket alone under every launch shape; keep the fastest."""
         choices = {}
         for bk in self.buckets:
-            cands = [{"k": 3, "minb": 1, "chunk": 0}]
+            cands = [{"k": 0, "minb": 0, "chunk": 0}]
             if bk.shape.op == "ctct":
                 cands = [{"k": k, "minb": mb, "chunk": ch}
                          for k, mb, ch in itertools.product((3, 4), (1, 2), (0, 128))
-                         if not (mb == 2 and bk.shape.log_n not in (12, 13))
+                         if ((1 << bk.shape.log_n) >> k) <= 1024
                          and not (ch and ch >= bk.count)]
             best = None
             for c in cands:

@@ -26,14 +26,24 @@ struct TwD {
 };
 
 // Per-prime FP64 table slots ([n_primes][TWF_SLOTS][N] entries of TwD).
+// Forward tables: psi^brv(m + i) for stage m = 2^s, group i < m, stored at
+// m + i except in the stages of the transform's last register pass (the one
+// with one butterfly block per thread), where group i = block * 2^u + grp is
+// stored at m + grp * 2^S0 + block (S0 = first stage of that pass, u = s - S0)
+// so that the 32 lanes of a warp read 32 consecutive entries.  The last pass
+// depends on the register radix 2^K, so there is one forward table per K.
+// Inverse tables: per stage s the h = N / 2^(s+1) twiddles omega^-(k 2^s),
+// k < h, stored at h + k (one contiguous run per stage).
 enum {
-  TWF_FWD = 0,       // merged negacyclic forward: psi^brv(k), k in [1, N)
-  TWF_INV = 1,       // negacyclic inverse DIT twiddles: omega^-i, i in [0, N/2), omega = psi^2
-  TWF_FWD_CYC = 2,   // merged cyclic forward
-  TWF_INV_CYC = 3,   // cyclic inverse DIT twiddles: omega_cyc^-i, i in [0, N/2)
-  TWF_POST = 4,      // N^-1 psi^-j, j in [0, N)
-  TWF_POST_CYC = 5,  // N^-1 (every j)
-  TWF_SLOTS = 6
+  TWF_FWD3 = 0,      // merged negacyclic forward, last-pass layout of K = 3
+  TWF_FWD4 = 1,      // merged negacyclic forward, last-pass layout of K = min(4, log N)
+  TWF_FWDC3 = 2,     // merged cyclic forward, K = 3
+  TWF_FWDC4 = 3,     // merged cyclic forward, K = min(4, log N)
+  TWF_INV = 4,       // negacyclic inverse DIT twiddles (omega = psi^2), per stage
+  TWF_INV_CYC = 5,   // cyclic inverse DIT twiddles, per stage
+  TWF_POST = 6,      // N^-1 psi^-j, j in [0, N)
+  TWF_POST_CYC = 7,  // N^-1 (every j)
+  TWF_SLOTS = 8
 };
 
 // Per-prime constants, one record per prime of a context.
@@ -101,3 +111,23 @@ __device__ __forceinline__ TwPair ldtw(const TwPair* p) {
 }
 
 __device__ __forceinline__ PrimeInfo ldpi(const PrimeInfo* p) { return *p; }
+
+// ------------------------------------------------------------------ cache policy
+// Polynomial limbs and key limbs are read once per CTA: load them without
+// allocating in L1, so the L1 keeps the twiddle tables (loaded evict-last),
+// which every transform of the CTA re-reads.
+__device__ __forceinline__ u64 ld_stream(const u64* p) {
+  u64 v;
+  asm("ld.global.nc.L1::no_allocate.u64 %0, [%1];" : "=l"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ ulonglong2 ld_stream2(const void* p) {
+  ulonglong2 v;
+  asm("ld.global.nc.L1::no_allocate.v2.u64 {%0, %1}, [%2];" : "=l"(v.x), "=l"(v.y) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ double2 ld_keep2(const void* p) {
+  double2 v;
+  asm("ld.global.nc.L1::evict_last.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));
+  return v;
+}

@@ -55,46 +55,65 @@ static CmScratch cm_carve(void* base, int n, int n_ct, int level) {
   return s;
 }
 
-// ct-mult kernels are instantiated for log N in [6, 14] with K in {3, 4} at
-// MINB = 1, and for log N in {12, 13} also at MINB = 2.  Defaults K = 3,
-// MINB = 1 (measured fastest at N = 2^12 and 2^13: the 64-register budget of
-// MINB = 2 spills in the NTT passes).
+// CTAs per SM that the register budget of a launch shape targets: "balanced"
+// gives every thread 128 registers (max(1, 512 / T) CTAs of T threads),
+// "tight" 64 (twice the CTAs; not built for 1024-thread CTAs).
+template <int LOGN, int K, bool TIGHT>
+struct CmBlocks {
+  static constexpr int T = (1 << LOGN) >> K;
+  static constexpr int B = T >= 512 ? 1 : 512 / T;
+  static constexpr int value = (TIGHT && T < 1024) ? 2 * B : B;
+};
+
+// ct-mult kernels are instantiated for log N in [6, 14] with K in {3, 4}
+// (K = 3 needs N / 8 <= 1024 threads) and both register budgets.  Defaults:
+// K = 4 for log N >= 10 (3 below), balanced budget: measured fastest at
+// N = 2^12 (2 CTAs of 256 threads per SM) and 2^13 (1 CTA of 512).
 // f is called as f.template operator()<L, K, MINB>().
 template <typename F>
 static int dispatch_cm(int log_n, int kreq, int mreq, F&& f, const char* fn) {
-  const int k = kreq ? kreq : 3;
-  const bool big = log_n == 12 || log_n == 13;
-  const int mb = mreq ? mreq : 1;
+  const int k = kreq ? kreq : (log_n >= 10 ? 4 : 3);
+  const int budget = mreq ? mreq : 1;
   if (k != 3 && k != 4) return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=%d not built", fn, k);
-  if (mb != 1 && !(mb == 2 && big))
-    return ckks_set_error(CKKS_EUNSUPPORTED, "%s: MINB=%d not built for log_n=%d", fn, mb, log_n);
-  switch (log_n) {
-#define CKKS_CM_CASE(L) \
-  case L:               \
-    return k == 3 ? f.template operator()<L, 3, 1>() : f.template operator()<L, 4, 1>();
-#define CKKS_CM_CASE2(L)                                                                     \
-  case L:                                                                                    \
-    if (mb == 2)                                                                             \
-      return k == 3 ? f.template operator()<L, 3, 2>() : f.template operator()<L, 4, 2>(); \
-    return k == 3 ? f.template operator()<L, 3, 1>() : f.template operator()<L, 4, 1>();
-    CKKS_CM_CASE(6)
-    CKKS_CM_CASE(7)
-    CKKS_CM_CASE(8)
-    CKKS_CM_CASE(9)
-    CKKS_CM_CASE(10)
-    CKKS_CM_CASE(11)
-    CKKS_CM_CASE2(12)
-    CKKS_CM_CASE2(13)
-    CKKS_CM_CASE(14)
-#undef CKKS_CM_CASE
-#undef CKKS_CM_CASE2
-    default:
+  if (budget != 1 && budget != 2)
+    return ckks_set_error(CKKS_EUNSUPPORTED, "%s: register budget %d not in {1, 2}", fn, budget);
+  if (log_n < 6 || log_n > 14)
+    return ckks_set_error(CKKS_EUNSUPPORTED, "%s: log_n=%d outside [6, 14]", fn, log_n);
+  if (((1 << log_n) >> k) > 1024)
+    return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=%d gives more than 1024 threads at log_n=%d",
+                          fn, k, log_n);
+  const bool tight = budget == 2;
+  auto go = [&]<int L>() -> int {
+    if constexpr (L < 6) {
       return ckks_set_error(CKKS_EUNSUPPORTED, "%s: log_n=%d outside [6, 14]", fn, log_n);
+    } else {
+      if (k == 3) {
+        if constexpr (((1 << L) >> 3) <= 1024) {
+          return tight ? f.template operator()<L, 3, CmBlocks<L, 3, true>::value>()
+                       : f.template operator()<L, 3, CmBlocks<L, 3, false>::value>();
+        }
+        return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=3 not built at log_n=%d", fn, log_n);
+      }
+      return tight ? f.template operator()<L, 4, CmBlocks<L, 4, true>::value>()
+                   : f.template operator()<L, 4, CmBlocks<L, 4, false>::value>();
+    }
+  };
+  switch (log_n) {
+    case 6: return go.template operator()<6>();
+    case 7: return go.template operator()<7>();
+    case 8: return go.template operator()<8>();
+    case 9: return go.template operator()<9>();
+    case 10: return go.template operator()<10>();
+    case 11: return go.template operator()<11>();
+    case 12: return go.template operator()<12>();
+    case 13: return go.template operator()<13>();
+    default: return go.template operator()<14>();
   }
 }
 
 // ---------------------------------------------------------------- kernel A
-// One CTA per (ct, limb j).  Registers: one coefficient array.
+// One CTA per (ct, limb j).  All global traffic is lane-contiguous (layout C);
+// d2 is re-distributed to layout Z through shared memory for its INTT.
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_tensor(const u64* __restrict__ A, const u64* __restrict__ B, CmScratch S, int level,
@@ -111,16 +130,16 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   const u64* b0 = B + ct * 2 * LN + (size_t)j * N;
   u64* d0 = S.d01 + ct * 2 * LN + (size_t)j * N;
   u64 x[Sh::E], y[Sh::E];
-  // d2 = a1 b1 ; keep in x
-  load_z<LOGN, K>(x, a0 + LN, tid);
-  load_z<LOGN, K>(y, b0 + LN, tid);
+  // d2 = a1 b1
+  load_c<LOGN, K>(x, a0 + LN, tid);
+  load_c<LOGN, K>(y, b0 + LN, tid);
   u64 m2[Sh::E];
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) m2[e] = mulmod(x[e], y[e], P);
   // d0 = a0 b0 ; d1 = (a0 + a1)(b0 + b1) - d0 - d2
   u64 a0v[Sh::E], b0v[Sh::E];
-  load_z<LOGN, K>(a0v, a0, tid);
-  load_z<LOGN, K>(b0v, b0, tid);
+  load_c<LOGN, K>(a0v, a0, tid);
+  load_c<LOGN, K>(b0v, b0, tid);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) {
     const u64 m0 = mulmod(a0v[e], b0v[e], P);
@@ -129,17 +148,19 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     a0v[e] = m0;
     b0v[e] = m1;
   }
-  store_z<LOGN, K>(a0v, d0, tid);
-  store_z<LOGN, K>(b0v, d0 + LN, tid);
-  store_z<LOGN, K>(m2, S.d2n + ct * LN + (size_t)j * N, tid);
+  store_c<LOGN, K>(a0v, d0, tid);
+  store_c<LOGN, K>(b0v, d0 + LN, tid);
+  store_c<LOGN, K>(m2, S.d2n + ct * LN + (size_t)j * N, tid);
+  c_to_z<LOGN, K>(m2, sm, tid);
   ntt_inv<LOGN, K>(m2, sm, tid, twbase<LOGN>(tw, j), P);
   store_c<LOGN, K>(m2, S.d2c + ct * LN + (size_t)j * N, tid);
 }
 
 // ---------------------------------------------------------------- kernel B
-// One CTA per (ct, target prime).  The two accumulators live in thread-private
-// shared-memory slots (index e * T + tid), so only one coefficient array is in
-// registers.
+// One CTA per (ct, target prime).  Each digit is transformed (layout C in,
+// Z out) and re-distributed to layout C, so the key limbs, stored in natural
+// order, are read lane-contiguously.  The two accumulators live in
+// thread-private shared-memory slots (index e * T + tid).
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_modup(CmScratch S, const ulonglong2* __restrict__ key, int level, int nq,
@@ -162,24 +183,24 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   for (int j = 0; j < level; ++j) {
     u64 x[Sh::E];
     if (!special && j == ti) {
-      load_z<LOGN, K>(x, S.d2n + ct * LN + (size_t)j * N, tid);
+      load_c<LOGN, K>(x, S.d2n + ct * LN + (size_t)j * N, tid);
     } else {
       // digit j residues (< q_j < 2 q_i) go into the transform unreduced
       load_c<LOGN, K>(x, S.d2c + ct * LN + (size_t)j * N, tid);
       ntt_fwd<LOGN, K>(x, sm, tid, tb, P);
+      z_to_c<LOGN, K>(x, sm, tid);
     }
-    const ulonglong2* k0 = key + (((size_t)j * 2 + 0) * (nq + 1) + pidx) * N;
-    const ulonglong2* k1 = key + (((size_t)j * 2 + 1) * (nq + 1) + pidx) * N;
+    // one key polynomial at a time keeps at most E key words in flight
+#pragma unroll 1
+    for (int kk = 0; kk < 2; ++kk) {
+      const ulonglong2* kp = key + (((size_t)j * 2 + kk) * (nq + 1) + pidx) * N;
+      u64* acc = kk ? acc1s : acc0s;
 #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) {
-      const int p = posZ<LOGN, K>(tid, e);
-      const ulonglong2 w0 = __ldg(k0 + p);
-      const ulonglong2 w1 = __ldg(k1 + p);
-      const u64 t0 = shoup_lazy(x[e], w0.x, w0.y, P.q);
-      const u64 t1 = shoup_lazy(x[e], w1.x, w1.y, P.q);
-      const int s = e * T + tid;
-      acc0s[s] = (j == 0 ? 0ull : acc0s[s]) + t0;
-      acc1s[s] = (j == 0 ? 0ull : acc1s[s]) + t1;
+      for (int e = 0; e < Sh::E; ++e) {
+        const ulonglong2 w = ld_stream2(kp + posC<LOGN, K>(tid, e));
+        const int s = e * T + tid;
+        acc[s] = (j == 0 ? 0ull : acc[s]) + shoup_lazy(x[e], w.x, w.y, P.q);
+      }
     }
   }
   // Special-prime accumulators stay in the evaluation domain here; kernel C
@@ -193,13 +214,13 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     const u64* a = k ? acc1s : acc0s;
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) x[e] = reduce_any(a[e * T + tid], P);
-    store_z<LOGN, K>(x, o + (size_t)k * kstride, tid);
+    store_c<LOGN, K>(x, o + (size_t)k * kstride, tid);
   }
 }
 
 // ---------------------------------------------------------------- kernel C
 // One CTA per (ct, poly k).  The centred special-prime accumulator v and the
-// rescale limb w are kept in thread-private shared-memory slots.
+// rescale limb w are kept in thread-private shared-memory slots (layout C).
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_down(CmScratch S, u64* __restrict__ out, int level, int nq,
@@ -223,7 +244,8 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   u64* ok = out + ((size_t)ct * 2 + k) * (size_t)t * N;
 
   u64 x[Sh::E];
-  load_z<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
+  load_c<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
+  c_to_z<LOGN, K>(x, sm, tid);
   ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, nq), PP);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) {
@@ -259,15 +281,16 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
       x[e] = shoup_lazy(vi, pv.w, pv.ws, P.q) + wi;  // [0, 3q)
     }
     ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
+    z_to_c<LOGN, K>(x, sm, tid);
     u64 dv[Sh::E], av[Sh::E];
-    load_z<LOGN, K>(dv, dk + (size_t)i * N, tid);
-    load_z<LOGN, K>(av, ak + (size_t)i * N, tid);
+    load_c<LOGN, K>(dv, dk + (size_t)i * N, tid);
+    load_c<LOGN, K>(av, ak + (size_t)i * N, tid);
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) {
       const u64 s = dv[e] + shoup_lazy(av[e], pv.w, pv.ws, P.q) + P.qlazy - x[e];  // (0, 35q)
       x[e] = shoup(s, ci.w, ci.ws, P.q);
     }
-    store_z<LOGN, K>(x, ok + (size_t)i * N, tid);
+    store_c<LOGN, K>(x, ok + (size_t)i * N, tid);
   }
 }
 

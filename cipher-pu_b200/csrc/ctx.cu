@@ -64,6 +64,53 @@ static bool is_prime_u64(u64 n) {
   return true;
 }
 
+// root^e mod q for e in [0, n)
+static std::vector<u64> h_powers(u64 root, int n, u64 q) {
+  std::vector<u64> p(n);
+  u64 cur = 1 % q;
+  for (int e = 0; e < n; ++e) {
+    p[e] = cur;
+    cur = h_mulmod(cur, root, q);
+  }
+  return p;
+}
+
+// First stage of the last register pass of an N = 2^log_n transform with
+// 2^k coefficients per thread (the pass split of NttShape in ntt.cuh).
+static int last_pass_s0(int log_n, int k) {
+  k = k < log_n ? k : log_n;
+  const int r = log_n - k;
+  if (r == 0) return 0;
+  const int np = (r + k - 1) / k;
+  const int kp_last = r / np + ((np - 1) < (r % np) ? 1 : 0);
+  return log_n - kp_last;
+}
+
+// Forward table: group ii of stage m = 2^s at m + ii, except in the stages
+// s >= s0 of the last pass, where ii = block * 2^u + grp (u = s - s0) goes to
+// m + grp * 2^s0 + block.
+template <typename F>
+static void fill_fwd(TwD* dst, int log_n, int s0, F&& value, u64 q) {
+  for (int s = 0; s < log_n; ++s) {
+    const int m = 1 << s;
+    const int u = s - s0;
+    for (int ii = 0; ii < m; ++ii) {
+      const int at = u >= 0 ? m + (ii & ((1 << u) - 1)) * (1 << s0) + (ii >> u) : m + ii;
+      dst[at] = h_twd(value(m, ii), q);
+    }
+  }
+}
+
+// Inverse table: stage s (h = N / 2^(s+1)) holds w^(k 2^s), k < h, at h + k;
+// pw[e] = w^e.
+static void fill_inv(TwD* dst, int log_n, const std::vector<u64>& pw, u64 q) {
+  const int n = 1 << log_n;
+  for (int s = 0; s < log_n; ++s) {
+    const int h = n >> (s + 1);
+    for (int k = 0; k < h; ++k) dst[h + k] = h_twd(pw[(size_t)k << s], q);
+  }
+}
+
 static void free_ctx(ckks_ctx* c) {
   if (!c) return;
   cudaFree(c->d_pi);
@@ -140,34 +187,28 @@ extern "C" int ckks_ctx_create(int log_n, int n_primes, int n_special, const uin
     TwD* t = tw.data() + (size_t)i * TWF_SLOTS * n;
     for (int k = 0; k < TWF_SLOTS * n; ++k) t[k] = TwD{0.0, 0.0};
     const u64 ninv_q = h_invmod((u64)n % q, q);
+    const u64 oinv = h_invmod(om, q);
     if (nega) {
-      // forward: merged psi^brv(k); inverse: DIT twiddles omega^-i (omega = psi^2)
-      // and the closing untwist N^-1 psi^-j
+      const std::vector<u64> pp = h_powers(ps, n, q);
+      fill_fwd(t + TWF_FWD3 * n, log_n, last_pass_s0(log_n, 3), [&](int m, int ii) {
+        return pp[bitrev(m + ii, log_n)];
+      }, q);
+      fill_fwd(t + TWF_FWD4 * n, log_n, last_pass_s0(log_n, 4), [&](int m, int ii) {
+        return pp[bitrev(m + ii, log_n)];
+      }, q);
       const u64 pinv = h_invmod(ps, q);
-      for (int k = 1; k < n; ++k) t[TWF_FWD * n + k] = h_twd(h_powmod(ps, bitrev(k, log_n), q), q);
-      const u64 winv = h_mulmod(pinv, pinv, q);
-      u64 cur = 1;
-      for (int k = 0; k < n / 2; ++k) {
-        t[TWF_INV * n + k] = h_twd(cur, q);
-        cur = h_mulmod(cur, winv, q);
-      }
-      cur = ninv_q;
+      fill_inv(t + TWF_INV * n, log_n, h_powers(h_mulmod(pinv, pinv, q), n, q), q);
+      u64 cur = ninv_q;
       for (int j = 0; j < n; ++j) {
         t[TWF_POST * n + j] = h_twd(cur, q);
         cur = h_mulmod(cur, pinv, q);
       }
     }
-    const u64 oinv = h_invmod(om, q);
-    for (int m = 1; m < n; m <<= 1)
-      for (int ii = 0; ii < m; ++ii) {
-        const int e = (bitrev(m + ii, log_n) - n / (2 * m)) / 2;
-        t[TWF_FWD_CYC * n + m + ii] = h_twd(h_powmod(om, e, q), q);
-      }
-    u64 cur = 1;
-    for (int k = 0; k < n / 2; ++k) {
-      t[TWF_INV_CYC * n + k] = h_twd(cur, q);
-      cur = h_mulmod(cur, oinv, q);
-    }
+    const std::vector<u64> po = h_powers(om, n, q);
+    auto cyc_tw = [&](int m, int ii) { return po[(bitrev(m + ii, log_n) - n / (2 * m)) / 2]; };
+    fill_fwd(t + TWF_FWDC3 * n, log_n, last_pass_s0(log_n, 3), cyc_tw, q);
+    fill_fwd(t + TWF_FWDC4 * n, log_n, last_pass_s0(log_n, 4), cyc_tw, q);
+    fill_inv(t + TWF_INV_CYC * n, log_n, h_powers(oinv, n, q), q);
     for (int j = 0; j < n; ++j) t[TWF_POST_CYC * n + j] = h_twd(ninv_q, q);
   }
   // keyswitch / rescale constants
@@ -236,7 +277,7 @@ extern "C" int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value) {
       return CKKS_OK;
     case CKKS_TUNE_CM_MIN_BLOCKS:
       CKKS_REQUIRE(value == 0 || value == 1 || value == 2,
-                   "ckks_ctx_set_tuning: ct-mult CTAs per SM must be 0, 1 or 2");
+                   "ckks_ctx_set_tuning: ct-mult register budget must be 0, 1 (balanced) or 2 (tight)");
       ctx->tune_cm_minb = value;
       return CKKS_OK;
     default:

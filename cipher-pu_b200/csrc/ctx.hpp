@@ -17,7 +17,7 @@ struct ckks_ctx {
   int n_q = 0;        // n_primes - n_special
   int device = 0;
   int tune_cm_k = 0;     // ct-mult: log2 coefficients per thread (0 = default)
-  int tune_cm_minb = 0;  // ct-mult: CTAs per SM targeted by the register budget (0 = default)
+  int tune_cm_minb = 0;  // ct-mult: register budget, 1 balanced / 2 tight (0 = default)
   std::vector<u64> primes, psi, omega;
   std::vector<int> has_nega;
   std::vector<PrimeInfo> h_pi;

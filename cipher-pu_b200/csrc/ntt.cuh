@@ -88,7 +88,7 @@ __device__ __forceinline__ int posZ(int tid, int e) {
 #define CKKS_FP_TWO52 4503599627370496.0
 
 __device__ __forceinline__ TwD ldtwd(const TwD* p) {
-  const double2 v = __ldg(reinterpret_cast<const double2*>(p));
+  const double2 v = ld_keep2(p);
   TwD t;
   t.w = v.x;
   t.wq = v.y;
@@ -125,7 +125,9 @@ __device__ __forceinline__ void ct_bfly_fp(double& x, double& y, const TwD& w, d
   y = __dadd_rn(xr, -t);
 }
 
-// forward pass: stages S0 .. S0+KP-1, group-uniform twiddles tw[m + i]
+// forward pass: stages S0 .. S0+KP-1, group-uniform twiddles (group
+// i = block * 2^u + grp of stage m = 2^(S0+u)); in the last pass the table
+// holds that group at m + grp * 2^S0 + block (lane-contiguous, see common.cuh)
 template <int LOGN, int K, int S0, int KP>
 __device__ __forceinline__ void fwd_pass(double (&x)[1 << K], int tid, const TwD* __restrict__ tw,
                                          double qd) {
@@ -135,6 +137,7 @@ __device__ __forceinline__ void fwd_pass(double (&x)[1 << K], int tid, const TwD
   constexpr int DMIN = BSZ >> KP;
   constexpr int SUBS = 1 << (K - KP);
   constexpr int RR = 1 << KP;
+  constexpr bool LAST = S0 + KP == LOGN;
 #pragma unroll
   for (int c = 0; c < SUBS; ++c) {
     const int g = tid + T * c;
@@ -144,7 +147,9 @@ __device__ __forceinline__ void fwd_pass(double (&x)[1 << K], int tid, const TwD
       const int half = RR >> (u + 1);
 #pragma unroll
       for (int grp = 0; grp < (1 << u); ++grp) {
-        const TwD w = ldtwd(tw + (1 << (S0 + u)) + block * (1 << u) + grp);
+        const int ti = LAST ? (1 << (S0 + u)) + grp * (1 << S0) + block
+                            : (1 << (S0 + u)) + block * (1 << u) + grp;
+        const TwD w = ldtwd(tw + ti);
 #pragma unroll
         for (int j = 0; j < half; ++j) {
           const int r = grp * 2 * half + j;
@@ -156,7 +161,8 @@ __device__ __forceinline__ void fwd_pass(double (&x)[1 << K], int tid, const TwD
 }
 
 // inverse (DIT) pass: stages S0+KP-1 down to S0 (distances ascending);
-// the pair (p, p + h) at stage s uses itw[(p mod h) << s], h = N >> (s + 1)
+// the pair (p, p + h) at stage s, h = N >> (s + 1), uses omega^-((p mod h) 2^s),
+// stored at itw[h + (p mod h)]
 template <int LOGN, int K, int S0, int KP>
 __device__ __forceinline__ void inv_pass(double (&x)[1 << K], int tid, const TwD* __restrict__ itw,
                                          double qd) {
@@ -176,7 +182,7 @@ __device__ __forceinline__ void inv_pass(double (&x)[1 << K], int tid, const TwD
       const int s = S0 + u;
 #pragma unroll
       for (int j = 0; j < half; ++j) {
-        const TwD w = ldtwd(itw + ((off + DMIN * j) << s));
+        const TwD w = ldtwd(itw + (N >> (s + 1)) + off + DMIN * j);
 #pragma unroll
         for (int grp = 0; grp < (1 << u); ++grp) {
           const int r = grp * 2 * half + j;
@@ -252,7 +258,8 @@ template <int LOGN, int K>
 __device__ __forceinline__ void ntt_fwd(u64 (&x)[1 << K], u64* sm, int tid, const TwD* __restrict__ tb,
                                         const PrimeInfo& P, bool cyclic = false) {
   constexpr int N = 1 << LOGN;
-  const TwD* tw = tb + (cyclic ? TWF_FWD_CYC : TWF_FWD) * N;
+  static_assert(K <= 4, "forward twiddle layouts exist for K <= 4");
+  const TwD* tw = tb + (cyclic ? (K == 3 ? TWF_FWDC3 : TWF_FWDC4) : (K == 3 ? TWF_FWD3 : TWF_FWD4)) * N;
   double d[1 << K];
 #pragma unroll
   for (int e = 0; e < (1 << K); ++e) d[e] = u2d(x[e]);
@@ -297,7 +304,7 @@ template <int LOGN, int K>
 __device__ __forceinline__ void load_z(u64 (&x)[1 << K], const u64* __restrict__ src, int tid) {
 #pragma unroll
   for (int e = 0; e < (1 << K); e += 2) {
-    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(src + posZ<LOGN, K>(tid, e)));
+    const ulonglong2 v = ld_stream2(src + posZ<LOGN, K>(tid, e));
     x[e] = v.x;
     x[e + 1] = v.y;
   }
@@ -311,12 +318,40 @@ __device__ __forceinline__ void store_z(const u64 (&x)[1 << K], u64* __restrict_
 template <int LOGN, int K>
 __device__ __forceinline__ void load_c(u64 (&x)[1 << K], const u64* __restrict__ src, int tid) {
 #pragma unroll
-  for (int e = 0; e < (1 << K); ++e) x[e] = __ldg(src + posC<LOGN, K>(tid, e));
+  for (int e = 0; e < (1 << K); ++e) x[e] = ld_stream(src + posC<LOGN, K>(tid, e));
 }
 template <int LOGN, int K>
 __device__ __forceinline__ void store_c(const u64 (&x)[1 << K], u64* __restrict__ dst, int tid) {
 #pragma unroll
   for (int e = 0; e < (1 << K); ++e) dst[posC<LOGN, K>(tid, e)] = x[e];
+}
+
+// Register re-distribution through the transform's shared buffer: layout Z
+// (the forward output) to layout C (lane-contiguous, for coalesced global
+// access and elementwise work against naturally ordered operands), and back
+// (the inverse input).  Callers must not have threads still reading sm (every
+// transform returns with sm free); both end with a barrier.
+template <int LOGN, int K, typename V>
+__device__ __forceinline__ void z_to_c(V (&x)[1 << K], u64* sm, int tid) {
+  using S = NttShape<LOGN, K>;
+  V* sv = reinterpret_cast<V*>(sm);
+#pragma unroll
+  for (int e = 0; e < (1 << K); ++e) sv[padix(posZ<LOGN, K>(tid, e), S::PADSH)] = x[e];
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < (1 << K); ++e) x[e] = sv[padix(posC<LOGN, K>(tid, e), S::PADSH)];
+  __syncthreads();
+}
+template <int LOGN, int K, typename V>
+__device__ __forceinline__ void c_to_z(V (&x)[1 << K], u64* sm, int tid) {
+  using S = NttShape<LOGN, K>;
+  V* sv = reinterpret_cast<V*>(sm);
+#pragma unroll
+  for (int e = 0; e < (1 << K); ++e) sv[padix(posC<LOGN, K>(tid, e), S::PADSH)] = x[e];
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < (1 << K); ++e) x[e] = sv[padix(posZ<LOGN, K>(tid, e), S::PADSH)];
+  __syncthreads();
 }
 
 // Dynamic shared memory bytes needed by one transform.

@@ -67,9 +67,10 @@ int ckks_ctx_destroy(ckks_ctx* ctx);
  * Launch-shape tuning of a context (used by the autotuner).  Parameters:
  *   CKKS_TUNE_CM_LOG_ELEMS: coefficients per thread of the ct-mult kernels
  *   as log2 (3 -> radix-8 passes with N/8 threads, 4 -> radix-16 with N/16;
- *   0 = default 3).
- *   CKKS_TUNE_CM_MIN_BLOCKS: CTAs per SM the ct-mult kernels' register
- *   budget targets (1 or 2; 2 is built for N = 2^12, 2^13 only; 0 = default).
+ *   0 = default: 4 for N >= 2^10, else 3).
+ *   CKKS_TUNE_CM_MIN_BLOCKS: register budget of the ct-mult kernels:
+ *   1 = balanced (128 registers per thread, max(1, 512 / threads) CTAs per
+ *   SM), 2 = tight (64 registers, twice the CTAs); 0 = default (balanced).
  * The reference fixes its datapath shape at synthesis time
  * (rtl/m1/ntt_unit.sv:39-52 parameters).
  */
