@@ -42,6 +42,9 @@ SIGNATURES: dict[str, tuple] = {
     "ckks_ct_mul_scratch_bytes": (_sz, [_vp, _i32, _i32]),
     "ckks_ct_mul_relin_rescale": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _i32, _i32, _vp, _sz,
                                          _vp]),
+    "ckks_ct_mul_host_workspace_bytes": (_sz, [_vp, _i32, _i32]),
+    "ckks_ct_mul_relin_rescale_host": (_i32, [_vp, _vp, _vp, _vp, _u64p, _i32, _i32, _i32, _vp, _sz,
+                                              _vp]),
     "ckks_ct_mul_relin_rescale_noalloc": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _i32, _i32, _vp]),
     "ckks_encode": (_i32, [_vp, _u64p, _vp, _i32, _i32, _i32, C.c_double, _vp]),
     "ckks_decode": (_i32, [_vp, _vp, _u64p, _i32, _i32, _i32, C.c_double, _vp]),

@@ -153,6 +153,31 @@ def ct_mul_relin_rescale(ctx: Context, ct_a: torch.Tensor, ct_b: torch.Tensor,
     return out
 
 
+def ct_mul_host_workspace_bytes(ctx: Context, chunk: int, level: int) -> int:
+    return int(_lib.raw("ckks_ct_mul_host_workspace_bytes")(ctx.handle, chunk, level))
+
+
+def ct_mul_relin_rescale_host(ctx: Context, ct_a: torch.Tensor, ct_b: torch.Tensor,
+                              key_prepared: torch.Tensor, out: torch.Tensor | None = None,
+                              chunk: int = 32, workspace: torch.Tensor | None = None) -> torch.Tensor:
+    """Host (CPU, preferably pinned) ct_a, ct_b [n_ct, 2, level, N] -> host
+    [n_ct, 2, level-1, N]; copies and kernels pipelined in chunks."""
+    if ct_a.is_cuda or ct_b.is_cuda:
+        raise ValueError("ct_mul_relin_rescale_host takes host tensors")
+    if not (ct_a.is_contiguous() and ct_b.is_contiguous()) or ct_a.dtype != U64 or ct_b.dtype != U64:
+        raise ValueError("expected contiguous uint64 host tensors")
+    n_ct, two, level, n = ct_a.shape
+    if out is None:
+        out = torch.empty((n_ct, 2, level - 1, n), dtype=U64).pin_memory()
+    need = ct_mul_host_workspace_bytes(ctx, chunk, level)
+    if workspace is None or workspace.numel() * workspace.element_size() < need:
+        workspace = torch.empty((need + 7) // 8, dtype=U64, device=key_prepared.device)
+    _lib.call("ckks_ct_mul_relin_rescale_host", ctx.handle, out.data_ptr(), ct_a.data_ptr(),
+              ct_b.data_ptr(), _p(key_prepared), n_ct, level, chunk, _p(workspace),
+              workspace.numel() * workspace.element_size(), _stream())
+    return out
+
+
 # ------------------------------------------------------------------ encode / decode
 def _f64(t: torch.Tensor) -> int:
     if not t.is_cuda or t.dtype not in (torch.float64, torch.complex128) or not t.is_contiguous():

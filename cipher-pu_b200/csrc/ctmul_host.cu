@@ -1,0 +1,133 @@
+// ctmul_host.cu - the batched ct-mult + relin + rescale on HOST buffers: the
+// call a binding makes when its ciphertexts live in host memory (numpy arrays
+// behind ctypes, a JVM direct buffer, a cgo slice).
+//
+// The batch is cut into chunks; chunk i runs on pipeline stream i mod 3 as
+// H2D(a, b) -> the three ct-mult kernels -> D2H(out), so the host->device copy
+// of one chunk, the kernels of the previous one and the device->host copy of
+// the one before that overlap (B200 has separate copy engines per direction).
+// Each stream owns one slot of the caller's device workspace (inputs, output
+// and ct-mult scratch of one chunk), so a slot is reused only after its
+// previous chunk has left the stream.  The call returns when every output is
+// in host memory.  Host buffers should be page-locked (cudaHostAlloc /
+// torch pin_memory) for the copies to run asynchronously; pageable buffers
+// give the same results with serialised copies.
+#include <mutex>
+
+#include "ctx.hpp"
+
+int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
+                       const uint64_t* ct_b, const uint64_t* key, int n_ct, int level,
+                       void* scratch, size_t scratch_bytes, void* stream, const char* fn);
+
+namespace {
+
+constexpr int kPipe = 3;
+constexpr int kMaxDevices = 128;
+
+struct Pipe {
+  bool ready = false;
+  cudaStream_t s[kPipe];
+  cudaEvent_t start;
+};
+
+std::mutex g_pipe_mu;
+Pipe g_pipe[kMaxDevices];
+
+// Pipeline streams of the current device, created on first use and kept for
+// the life of the process.
+int pipe_for_device(Pipe** out, const char* fn) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
+  if (dev < 0 || dev >= kMaxDevices)
+    return ckks_set_error(CKKS_EUNSUPPORTED, "%s: device %d beyond %d", fn, dev, kMaxDevices);
+  std::lock_guard<std::mutex> lock(g_pipe_mu);
+  Pipe& p = g_pipe[dev];
+  if (!p.ready) {
+    for (int i = 0; i < kPipe && e == cudaSuccess; ++i)
+      e = cudaStreamCreateWithFlags(&p.s[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.start, cudaEventDisableTiming);
+    if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
+    p.ready = true;
+  }
+  *out = &p;
+  return CKKS_OK;
+}
+
+struct Slot {
+  size_t a_words, out_words, scratch_bytes, total_bytes;
+};
+
+Slot slot_shape(const ckks_ctx* ctx, int chunk, int level) {
+  Slot s;
+  s.a_words = (size_t)chunk * 2 * level * ctx->n;
+  s.out_words = (size_t)chunk * 2 * (level - 1) * ctx->n;
+  s.scratch_bytes = ckks_ct_mul_scratch_bytes(ctx, chunk, level);
+  s.total_bytes = (2 * s.a_words + s.out_words) * sizeof(uint64_t) + ((s.scratch_bytes + 255) & ~(size_t)255);
+  return s;
+}
+
+}  // namespace
+
+extern "C" size_t ckks_ct_mul_host_workspace_bytes(const ckks_ctx* ctx, int chunk, int level) {
+  if (!ctx || chunk < 1 || level < 2) return 0;
+  return (size_t)kPipe * slot_shape(ctx, chunk, level).total_bytes;
+}
+
+extern "C" int ckks_ct_mul_relin_rescale_host(const ckks_ctx* ctx, uint64_t* out_host,
+                                              const uint64_t* a_host, const uint64_t* b_host,
+                                              const uint64_t* key, int n_ct, int level, int chunk,
+                                              void* workspace, size_t workspace_bytes,
+                                              void* stream) {
+  const char* fn = "ckks_ct_mul_relin_rescale_host";
+  CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
+  CKKS_REQUIRE(n_ct >= 0, "%s: n_ct < 0", fn);
+  CKKS_REQUIRE(chunk >= 1, "%s: chunk=%d must be >= 1", fn, chunk);
+  CKKS_REQUIRE(level >= 2 && level <= ctx->n_q, "%s: level=%d outside [2, %d]", fn, level, ctx->n_q);
+  if (n_ct == 0) return CKKS_OK;
+  CKKS_REQUIRE(out_host && a_host && b_host && key && workspace, "%s: NULL pointer argument", fn);
+  const Slot sl = slot_shape(ctx, chunk, level);
+  CKKS_REQUIRE(workspace_bytes >= (size_t)kPipe * sl.total_bytes,
+               "%s: workspace of %zu bytes < %zu needed (ckks_ct_mul_host_workspace_bytes)", fn,
+               workspace_bytes, (size_t)kPipe * sl.total_bytes);
+  Pipe* p = nullptr;
+  if (int rc = pipe_for_device(&p, fn)) return rc;
+  // work queued earlier on the caller's stream (e.g. the key preparation)
+  // comes first
+  cudaError_t e = cudaEventRecord(p->start, as_stream(stream));
+  for (int i = 0; i < kPipe && e == cudaSuccess; ++i) e = cudaStreamWaitEvent(p->s[i], p->start, 0);
+  if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
+
+  const size_t in_ct = (size_t)2 * level * ctx->n;         // words per input ciphertext
+  const size_t out_ct = (size_t)2 * (level - 1) * ctx->n;  // words per output ciphertext
+  int rc = CKKS_OK;
+  for (int c0 = 0, i = 0; c0 < n_ct && rc == CKKS_OK; c0 += chunk, ++i) {
+    const int m = n_ct - c0 < chunk ? n_ct - c0 : chunk;
+    cudaStream_t st = p->s[i % kPipe];
+    unsigned char* base = reinterpret_cast<unsigned char*>(workspace) + (size_t)(i % kPipe) * sl.total_bytes;
+    uint64_t* da = reinterpret_cast<uint64_t*>(base);
+    uint64_t* db = da + sl.a_words;
+    uint64_t* dout = db + sl.a_words;
+    void* scratch = dout + sl.out_words;
+    const size_t in_bytes = (size_t)m * in_ct * sizeof(uint64_t);
+    e = cudaMemcpyAsync(da, a_host + (size_t)c0 * in_ct, in_bytes, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(db, b_host + (size_t)c0 * in_ct, in_bytes, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) {
+      rc = ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
+      break;
+    }
+    rc = ckks_ct_mul_launch(ctx, dout, da, db, key, m, level, scratch, sl.scratch_bytes, st, fn);
+    if (rc != CKKS_OK) break;
+    e = cudaMemcpyAsync(out_host + (size_t)c0 * out_ct, dout, (size_t)m * out_ct * sizeof(uint64_t),
+                        cudaMemcpyDeviceToHost, st);
+    if (e != cudaSuccess) rc = ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
+  }
+  for (int i = 0; i < kPipe; ++i) {
+    const cudaError_t es = cudaStreamSynchronize(p->s[i]);
+    if (es != cudaSuccess && rc == CKKS_OK)
+      rc = ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(es));
+  }
+  return rc;
+}

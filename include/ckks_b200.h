@@ -195,6 +195,25 @@ int ckks_ct_mul_relin_rescale(const ckks_ctx* ctx, uint64_t* out, const uint64_t
                               void* scratch, size_t scratch_bytes, void* stream);
 
 /*
+ * ckks_ct_mul_relin_rescale on HOST buffers: out_host, a_host, b_host are
+ * host arrays in the same layouts ([n_ct][2][level][N] in, [n_ct][2][level-1][N]
+ * out); `key` is the prepared key in device memory.  The batch is cut into
+ * chunks of `chunk` pairs pipelined over three internal streams (host->device
+ * copy, kernels and device->host copy of consecutive chunks overlap).  The
+ * device workspace (caller-owned) must hold
+ * ckks_ct_mul_host_workspace_bytes(ctx, chunk, level) bytes.  Work already
+ * queued on `stream` is ordered before the call; the call returns when all
+ * outputs are in host memory.  Host buffers should be page-locked for the
+ * copies to overlap.  Replaces the host side of scripts/verify_e2e_mult.py:78
+ * e2e_mult (list[int] in, list[int] out) for batches.
+ */
+size_t ckks_ct_mul_host_workspace_bytes(const ckks_ctx* ctx, int chunk, int level);
+int ckks_ct_mul_relin_rescale_host(const ckks_ctx* ctx, uint64_t* out_host, const uint64_t* a_host,
+                                   const uint64_t* b_host, const uint64_t* key, int n_ct, int level,
+                                   int chunk, void* workspace, size_t workspace_bytes,
+                                   void* stream);
+
+/*
  * CKKS slot encoding (FP64 canonical embedding, scale Delta):
  * slots [n_polys][n_slots] complex doubles (re, im interleaved), n_slots <=
  * N/2; slot k is the evaluation at Phi^(2k+1), Phi = exp(i pi / N), with its

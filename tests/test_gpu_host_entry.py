@@ -1,0 +1,62 @@
+"""Host-buffer ct-mult entry: chunked H2D / kernels / D2H pipeline over three
+streams must give the device-buffer entry's results bit for bit, for ragged
+batches (last chunk short), more chunks than streams (workspace slots reused)
+and the empty batch; the first pairs are also checked against the oracle."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import rns_ckks as R
+
+pytestmark = pytest.mark.gpu
+
+
+def _rand_ct(rng, shape, qs):
+    x = np.empty(shape, dtype=np.uint64)
+    for i, q in enumerate(qs):
+        x[..., i, :] = rng.integers(0, q, size=x[..., i, :].shape, dtype=np.uint64)
+    return x
+
+
+@pytest.mark.parametrize("n_ct,chunk", [(37, 8), (5, 32), (1, 1)])
+def test_host_entry_matches_device_entry(cuda, n_ct, chunk):
+    import ckks_b200.ops as ops
+    from ckks_b200.context import Context
+    from ckks_b200.params import CkksParams
+    P = CkksParams.standard(12, 3)
+    ctx = Context.get(12, P.primes, n_special=1)
+    rng = np.random.default_rng(1000 + n_ct)
+    qs = list(P.q)
+    a = _rand_ct(rng, (n_ct, 2, 3, 4096), qs)
+    b = _rand_ct(rng, (n_ct, 2, 3, 4096), qs)
+    ksk = _rand_ct(rng, (3, 2, 4, 4096), qs + [P.special])
+    key = ops.relin_key_prepare(ctx, ops.to_device(ksk))
+    dev = ops.to_host(ops.ct_mul_relin_rescale(ctx, ops.to_device(a), ops.to_device(b), key))
+    ha = torch.from_numpy(a.view(np.int64)).view(torch.uint64).pin_memory()
+    hb = torch.from_numpy(b.view(np.int64)).view(torch.uint64).pin_memory()
+    host = ops.ct_mul_relin_rescale_host(ctx, ha, hb, key, chunk=chunk)
+    torch.cuda.synchronize()
+    got = host.view(torch.int64).numpy().view(np.uint64)
+    assert np.array_equal(got, dev)
+    k = min(n_ct, 2)
+    assert np.array_equal(got[:k], R.ct_mul_relin_rescale(a[:k], b[:k], ksk, qs, P.special))
+
+
+def test_host_entry_empty_and_small_workspace(cuda):
+    import ckks_b200.ops as ops
+    from ckks_b200 import _lib
+    from ckks_b200.context import Context
+    from ckks_b200.params import CkksParams
+    P = CkksParams.standard(12, 3)
+    ctx = Context.get(12, P.primes, n_special=1)
+    key = torch.zeros((3, 2, 4, 4096, 2), dtype=torch.uint64, device="cuda")
+    e = torch.empty((0, 2, 3, 4096), dtype=torch.uint64).pin_memory()
+    out = ops.ct_mul_relin_rescale_host(ctx, e, e, key, chunk=4)
+    assert out.shape == (0, 2, 2, 4096)
+    a = torch.zeros((4, 2, 3, 4096), dtype=torch.uint64).pin_memory()
+    need = ops.ct_mul_host_workspace_bytes(ctx, 4, 3)
+    ws = torch.empty(need // 8 - 1, dtype=torch.uint64, device="cuda")
+    with pytest.raises(_lib.CkksError, match="workspace"):
+        _lib.call("ckks_ct_mul_relin_rescale_host", ctx.handle, a.data_ptr(), a.data_ptr(),
+                  a.data_ptr(), key.data_ptr(), 4, 3, 4, ws.data_ptr(), ws.numel() * 8,
+                  torch.cuda.current_stream().cuda_stream)
