@@ -187,3 +187,35 @@ class BatchExecutor:
                                                                               "count": bk.count}
         self.graph = None
         return choices
+
+
+def main(argv=None) -> int:
+    """Time the batched uneven workload: eager launches, one graph replay per
+    step with the default launch shapes, then after autotuning."""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--items", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--no-autotune", action="store_true")
+    a = ap.parse_args(argv)
+    items = synthetic_workload(a.items, seed=a.seed)
+    ex = BatchExecutor(items)
+    res = {"workload": f"{a.items} items, 60% ct x ct + relin + rescale / 40% ct x pt + rescale, "
+                       "N in {2^12, 2^13}, level uniform in 2..8",
+           "buckets": len(ex.buckets),
+           "ctct_items": sum(b.count for b in ex.buckets if b.shape.op == "ctct"),
+           "eager": ex.time_steps(a.steps, a.warmup, use_graph=False),
+           "graph_default": ex.time_steps(a.steps, a.warmup, use_graph=True)}
+    if not a.no_autotune:
+        res["autotune"] = ex.autotune()
+        res["graph_tuned"] = ex.time_steps(a.steps, a.warmup, use_graph=True)
+    print(json.dumps(res, indent=1))
+    return 0
+
+
+if __name__ == "__main__":
+    import sys
+    sys.exit(main())

@@ -16,5 +16,7 @@ golden vectors generated by importing the reference's own Python functions
 (``tests/golden/make_golden.py``), against the reference's committed twiddle
 and modulus-chain fixtures, and against its known-answer constants.  The RNS
 hybrid keyswitch / RNS rescale / DARE-over-RNS parts have no reference code;
-they are pinned by independent big-integer restatements (``oracle.bigint``).
+they are pinned by an independent big-integer restatement of the whole
+ct-mult (``oracle.rns_ckks.bigint_ct_mul``: CRT-composed integers, schoolbook
+negacyclic products, exact division by the special prime and by q_t).
 """
