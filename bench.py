@@ -45,6 +45,8 @@ def parse():
     ap.add_argument("--levels", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-transforms", action="store_true",
+                    help="skip the standalone NTT / poly-mult measurement")
     ap.add_argument("--e2e-chunk", type=int, default=64,
                     help="pairs per pipelined chunk of the host-buffer call")
     return ap.parse_args()
@@ -192,6 +194,59 @@ def stage_modmuls(stage: int, n: int, level: int) -> int:
     return 2 * (inv + fwd + n + inv + t * (fwd + 3 * n))
 
 
+def measure_transforms(ctx, dev, hbm_peak: float, reps: int = 20) -> dict:
+    """Standalone kernels of the golden path, reported in HBM GB/s:
+    batched forward / inverse NTT (algorithmic bytes 2 x 8N per limb-transform:
+    read + write) and the fused NTT -> pointwise -> INTT product of config 1
+    (3 x 8N per product: two inputs, one output).  Four rotating buffers of
+    1024 polys x 4 limbs (537 MB) keep every launch's data out of L2."""
+    import torch
+    import ckks_b200.ops as ops
+    n, nl, npoly, nbuf = ctx.n, 4, 1024, 4
+    logn = n.bit_length() - 1
+    bufs = [torch.randint(0, 1 << 40, (npoly, nl, n), dtype=torch.int64, device=dev).view(torch.uint64)
+            for _ in range(nbuf)]
+    res = {}
+
+    def timed(fn):
+        for i in range(3):
+            fn(i)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(reps):
+            fn(i)
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps / 1000.0
+
+    for inv in (False, True):
+        s = timed(lambda i: ops.ntt(ctx, bufs[i % nbuf], inverse=inv, n_limbs=nl))
+        byts = 2 * 8 * n * npoly * nl
+        res["intt" if inv else "ntt"] = {
+            "limb_transforms_per_s": npoly * nl / s, "GBps": byts / s / 1e9, "frac_hbm": byts / s / 1e9 / hbm_peak,
+            "Gbutterfly_s": npoly * nl * (n // 2) * logn / s / 1e9}
+    outs = [torch.empty((npoly // 2, nl, n), dtype=torch.uint64, device=dev) for _ in range(nbuf)]
+
+    def pm(i):
+        b = bufs[i % nbuf]
+        _lib_call_poly_mul(ctx, outs[i % nbuf], b[: npoly // 2], b[npoly // 2:], nl)
+    s = timed(pm)
+    byts = 3 * 8 * n * (npoly // 2) * nl
+    res["poly_mul"] = {"products_per_s": npoly // 2 * nl / s, "GBps": byts / s / 1e9,
+                       "frac_hbm": byts / s / 1e9 / hbm_peak}
+    res["shape"] = f"N=2^{logn}, 45-bit primes, {npoly} polys x {nl} limbs per launch, 4 rotating buffers"
+    return res
+
+
+def _lib_call_poly_mul(ctx, out, a, b, nl):
+    import torch
+    from ckks_b200 import _lib
+    _lib.call("ckks_poly_mul", ctx.handle, out.data_ptr(), a.data_ptr(), b.data_ptr(),
+              a.numel() // (ctx.n * nl), 0, nl, 0, torch.cuda.current_stream().cuda_stream)
+
+
 def run_ours(a) -> int:
     import torch
     ws, rank, local = dist_env()
@@ -335,6 +390,7 @@ def run_ours(a) -> int:
         from ckks_b200.peak import modmul_peak
         mm_peak = modmul_peak(kind=1) / 1e12
         mm_ach = stage_modmuls(dom, n, L) * B / (per_launch_ms / 1000.0) / 1e12
+        transforms = measure_transforms(ctx, dev, hbm) if not a.no_transforms else None
         cpu = None
         if ws == 1 and not a.no_cpu_baseline:
             from oracle import cpu_baseline
@@ -356,6 +412,7 @@ def run_ours(a) -> int:
                               "peak": mm_peak, "unit": "Tmodmul/s", "frac": mm_ach / mm_peak,
                               "modmuls_per_launch": stage_modmuls(dom, n, L) * B,
                               "peak_source": "measured live: ckks_modmul_peak kind 1 (FP64 double-word)"},
+            "transforms": transforms,
             "stage_ms_per_step": {names[s]: stages[s][0] / max(1, a.steps) for s in range(3)},
             "stage_share": {names[s]: (stages[s][0] / tot_ms if tot_ms else None) for s in range(3)},
             "cpu_baseline": cpu,

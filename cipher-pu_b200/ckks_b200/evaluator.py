@@ -16,7 +16,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import torch
 
-from . import ops
+from . import _lib, ops
 from .context import Context
 from .params import CkksParams
 
@@ -55,6 +55,7 @@ class Evaluator:
         self.rlk: torch.Tensor | None = None      # prepared relinearisation key
         self.ksk: torch.Tensor | None = None      # raw [L, 2, L+1, N]
         self._scratch: torch.Tensor | None = None
+        self.galois: dict = {}
 
     # ---------------------------------------------------------------- sampling
     def _sid(self) -> int:
@@ -89,12 +90,13 @@ class Evaluator:
         ops.ntt(self.ctx, t, prime_begin=0, n_limbs=n_limbs)
         return t
 
-    def _make_relin_key(self, a: torch.Tensor | None = None, e: torch.Tensor | None = None):
-        """ksk[j] = Enc_s over all L+1 primes of m_j with m_j[i] = delta_ij (P mod q_j) s^2."""
+    def _switch_key(self, target_eval: torch.Tensor, a: torch.Tensor | None = None,
+                    e: torch.Tensor | None = None) -> tuple:
+        """Hybrid key-switching key from `target` (evaluation domain over all
+        L + 1 primes) to s: ksk[j] = Enc_s(m_j), m_j[i] = delta_ij (P mod q_j) target."""
         L = self.params.levels
         n = self.n
         s = self.sk.s_eval
-        s2 = ops.pointwise_mul(self.ctx, s, s, n_limbs=L + 1)
         P = self.params.special
         if a is None:
             a = self.uniform(L, L + 1)
@@ -104,10 +106,52 @@ class Evaluator:
         for j in range(L):
             qj = self.params.q[j]
             c = torch.full((1, n), P % qj, dtype=torch.int64, device=self.device).view(U64)
-            m[j, j] = ops.pointwise_mul(self.ctx, s2[j:j + 1].contiguous(), c, prime_begin=j, n_limbs=1)[0]
-        self.ksk = ops.encrypt(self.ctx, m, s, a.contiguous(), e.contiguous())
-        self.rlk = ops.relin_key_prepare(self.ctx, self.ksk)
-        self._key_samples = (a, e)
+            m[j, j] = ops.pointwise_mul(self.ctx, target_eval[j:j + 1].contiguous(), c, prime_begin=j,
+                                        n_limbs=1)[0]
+        ksk = ops.encrypt(self.ctx, m, s, a.contiguous(), e.contiguous())
+        return ksk, ops.relin_key_prepare(self.ctx, ksk), (a, e)
+
+    def _make_relin_key(self, a: torch.Tensor | None = None, e: torch.Tensor | None = None):
+        """ksk[j] = Enc_s over all L+1 primes of m_j with m_j[i] = delta_ij (P mod q_j) s^2."""
+        L = self.params.levels
+        s = self.sk.s_eval
+        s2 = ops.pointwise_mul(self.ctx, s, s, n_limbs=L + 1)
+        self.ksk, self.rlk, self._key_samples = self._switch_key(s2, a, e)
+        self.galois = {}
+
+    def galois_key(self, nu: int, a: torch.Tensor | None = None, e: torch.Tensor | None = None):
+        """(raw, prepared) Galois key of psi_nu: switches psi_nu(s) to s (cached per nu)."""
+        nu = int(nu) % (2 * self.n)
+        if nu % 2 == 0:
+            raise ValueError("a Galois element must be odd")
+        if nu not in self.galois or a is not None:
+            ps = ops.automorphism(self.ctx, self.sk.s_eval, nu, eval_domain=True,
+                                  n_limbs=self.params.levels + 1)
+            ksk, gk, _ = self._switch_key(ps, a, e)
+            self.galois[nu] = (ksk, gk)
+        return self.galois[nu]
+
+    def rotate(self, ct: Ciphertext, nu: int, out: torch.Tensor | None = None) -> Ciphertext:
+        """psi_nu applied to the plaintext of ct, key-switched back to s (same
+        level and scale).  Slot k of the result holds slot galois_slot_map(nu)[k]
+        of the input (complex-conjugated where the map says so)."""
+        _, gk = self.galois_key(nu)
+        need = int(_lib.raw("ckks_rotate_scratch_bytes")(self.ctx.handle, ct.count, ct.level))
+        if self._scratch is None or self._scratch.numel() * 8 < need:
+            self._scratch = torch.empty((need + 7) // 8, dtype=U64, device=self.device)
+        r = ops.rotate(self.ctx, ct.data, gk, nu, scratch=self._scratch, out=out)
+        return Ciphertext(r, ct.scale)
+
+    def galois_slot_map(self, nu: int) -> tuple[np.ndarray, np.ndarray]:
+        """(src, conj) over the N/2 visible slots: after psi_nu, slot k holds
+        input slot src[k] (conjugated where conj[k]).  Slot k is the evaluation
+        at exp(i pi (2k + 1) / N); conjugates sit at N - 1 - k."""
+        n = self.n
+        k = np.arange(n // 2)
+        e = ((2 * k + 1) * (int(nu) % (2 * n))) % (2 * n)
+        kp = (e - 1) // 2
+        conj = kp >= n // 2
+        return np.where(conj, n - 1 - kp, kp), conj
 
     # ---------------------------------------------------------------- encode / encrypt
     def encode(self, values, level: int | None = None, scale: float | None = None) -> torch.Tensor:

@@ -153,6 +153,39 @@ def ct_mul_relin_rescale(ctx: Context, ct_a: torch.Tensor, ct_b: torch.Tensor,
     return out
 
 
+def automorphism(ctx: Context, x: torch.Tensor, nu: int, eval_domain: bool = False,
+                 prime_begin: int = 0, n_limbs: int | None = None) -> torch.Tensor:
+    """psi_nu(f)(X) = f(X^nu) mod (X^N + 1) of x [..., n_limbs, N]."""
+    npoly, nl = _polys_limbs(x, ctx.n, n_limbs)
+    out = torch.empty_like(x)
+    _lib.call("ckks_automorphism", ctx.handle, _p(out), _p(x), npoly, prime_begin, nl, int(nu),
+              int(eval_domain), _stream())
+    return out
+
+
+def mul_monomial(ctx: Context, x: torch.Tensor, nu: int, prime_begin: int = 0,
+                 n_limbs: int | None = None) -> torch.Tensor:
+    """x * X^nu in the coefficient domain."""
+    npoly, nl = _polys_limbs(x, ctx.n, n_limbs)
+    out = torch.empty_like(x)
+    _lib.call("ckks_mul_monomial", ctx.handle, _p(out), _p(x), npoly, prime_begin, nl, int(nu), _stream())
+    return out
+
+
+def rotate(ctx: Context, ct: torch.Tensor, galois_key_prepared: torch.Tensor, nu: int,
+           scratch: torch.Tensor | None = None, out: torch.Tensor | None = None) -> torch.Tensor:
+    """Key-switched automorphism of ct [n_ct, 2, level, N] (evaluation domain)."""
+    n_ct, two, level, n = ct.shape
+    need = int(_lib.raw("ckks_rotate_scratch_bytes")(ctx.handle, n_ct, level))
+    if scratch is None or scratch.numel() * scratch.element_size() < need:
+        scratch = torch.empty((need + 7) // 8, dtype=U64, device=ct.device)
+    if out is None:
+        out = torch.empty_like(ct)
+    _lib.call("ckks_rotate", ctx.handle, _p(out), _p(ct), _p(galois_key_prepared), n_ct, level, int(nu),
+              _p(scratch), scratch.numel() * scratch.element_size(), _stream())
+    return out
+
+
 def ct_mul_host_workspace_bytes(ctx: Context, chunk: int, level: int) -> int:
     return int(_lib.raw("ckks_ct_mul_host_workspace_bytes")(ctx.handle, chunk, level))
 

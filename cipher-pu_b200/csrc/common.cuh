@@ -112,6 +112,18 @@ __device__ __forceinline__ TwPair ldtw(const TwPair* p) {
 
 __device__ __forceinline__ PrimeInfo ldpi(const PrimeInfo* p) { return *p; }
 
+// ------------------------------------------------------------------ automorphism
+// Evaluation slot i of the merged forward transform holds f(psi^(2 brv(i) + 1));
+// psi_nu(f) = f(X^nu) at slot i is f at the slot returned here (nu odd, given
+// mod 2N as nu2n).
+__device__ __forceinline__ unsigned long long galois_eval_src(unsigned long long i, int log_n,
+                                                              unsigned long long nu2n) {
+  const unsigned long long n = 1ull << log_n;
+  const unsigned long long b = __brev((unsigned)i) >> (32 - log_n);
+  const unsigned long long e = ((2 * b + 1) * nu2n) & (2 * n - 1);
+  return __brev((unsigned)((e - 1) >> 1)) >> (32 - log_n);
+}
+
 // ------------------------------------------------------------------ cache policy
 // Polynomial limbs and key limbs are read once per CTA: load them without
 // allocating in L1, so the L1 keeps the twiddle tables (loaded evict-last),

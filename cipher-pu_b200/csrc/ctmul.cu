@@ -294,6 +294,90 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   }
 }
 
+// ---------------------------------------------------------------- rotation
+// Galois key switch of psi_nu(ct) (ckks_rotate): kernel R1 permutes both
+// polynomials in the evaluation domain (psi(c0) -> d01 slot 0, psi(c1) ->
+// d2n, and its INTT -> d2c, the digits), kernel B above forms the key inner
+// product with the Galois key, kernel R3 divides by the special prime
+// (ModDown, no rescale) and adds psi(c0).
+template <int LOGN, int K, int MINB>
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
+    k_rot_prep(const u64* __restrict__ C, CmScratch S, int level, u64 nu2n,
+               const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw) {
+  extern __shared__ u64 sm[];
+  using Sh = NttShape<LOGN, K>;
+  constexpr int N = Sh::N;
+  const long long ct = blockIdx.x / level;
+  const int j = blockIdx.x % level;
+  const int tid = threadIdx.x;
+  const PrimeInfo P = pi[j];
+  const size_t LN = (size_t)level * N;
+  const u64* c0 = C + ct * 2 * LN + (size_t)j * N;
+  u64 x[Sh::E];
+#pragma unroll
+  for (int e = 0; e < Sh::E; ++e) x[e] = ld_stream(c0 + galois_eval_src(posC<LOGN, K>(tid, e), LOGN, nu2n));
+  store_c<LOGN, K>(x, S.d01 + ct * 2 * LN + (size_t)j * N, tid);
+#pragma unroll
+  for (int e = 0; e < Sh::E; ++e)
+    x[e] = ld_stream(c0 + LN + galois_eval_src(posC<LOGN, K>(tid, e), LOGN, nu2n));
+  store_c<LOGN, K>(x, S.d2n + ct * LN + (size_t)j * N, tid);
+  c_to_z<LOGN, K>(x, sm, tid);
+  ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, j), P);
+  store_c<LOGN, K>(x, S.d2c + ct * LN + (size_t)j * N, tid);
+}
+
+// kernel R3: one CTA per (ct, poly k): v = centred INTT_p(acc_k,p); every
+// limb i: out_k,i = [k == 0] psi(c0)_i + (acc_k,i - NTT_i([v]_i)) p^-1.
+template <int LOGN, int K, int MINB>
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
+    k_ks_down(CmScratch S, u64* __restrict__ out, int level, int nq, const PrimeInfo* __restrict__ pi,
+              const TwD* __restrict__ tw, const TwPair* __restrict__ pinv) {
+  extern __shared__ u64 sm[];
+  using Sh = NttShape<LOGN, K>;
+  constexpr int N = Sh::N;
+  constexpr int T = Sh::T;
+  u64* vs = sm + Sh::SMEM_WORDS;
+  const long long ct = blockIdx.x >> 1;
+  const int k = blockIdx.x & 1;
+  const int tid = threadIdx.x;
+  const size_t LN = (size_t)level * N;
+  const PrimeInfo PP = pi[nq];
+  const u64* d0 = S.d01 + ct * 2 * LN;
+  const u64* ak = S.acc + ct * 2 * LN + (size_t)k * LN;
+  u64* ok = out + ((size_t)ct * 2 + k) * LN;
+  u64 x[Sh::E];
+  load_c<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
+  c_to_z<LOGN, K>(x, sm, tid);
+  ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, nq), PP);
+#pragma unroll
+  for (int e = 0; e < Sh::E; ++e) vs[e * T + tid] = x[e];
+#pragma unroll 1
+  for (int i = 0; i < level; ++i) {
+    const PrimeInfo P = pi[i];
+    const TwPair pv = pinv[i];
+#pragma unroll
+    for (int e = 0; e < Sh::E; ++e) {
+      const u64 v = vs[e * T + tid];
+      x[e] = v > PP.half ? v - PP.q + P.q : v;
+    }
+    ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
+    z_to_c<LOGN, K>(x, sm, tid);
+    u64 av[Sh::E];
+    load_c<LOGN, K>(av, ak + (size_t)i * N, tid);
+    if (k == 0) {
+      u64 dv[Sh::E];
+      load_c<LOGN, K>(dv, d0 + (size_t)i * N, tid);
+#pragma unroll
+      for (int e = 0; e < Sh::E; ++e)
+        x[e] = addmod(dv[e], shoup(av[e] + P.qlazy - x[e], pv.w, pv.ws, P.q), P.q);
+    } else {
+#pragma unroll
+      for (int e = 0; e < Sh::E; ++e) x[e] = shoup(av[e] + P.qlazy - x[e], pv.w, pv.ws, P.q);
+    }
+    store_c<LOGN, K>(x, ok + (size_t)i * N, tid);
+  }
+}
+
 // ---------------------------------------------------------------- key prep
 __global__ void k_key_prepare(ulonglong2* __restrict__ out, const u64* __restrict__ in,
                               long long total, int log_n, int nlimb,
@@ -391,4 +475,65 @@ extern "C" int ckks_ct_mul_relin_rescale(const ckks_ctx* ctx, uint64_t* out, con
                                          void* stream) {
   return ckks_ct_mul_launch(ctx, out, ct_a, ct_b, key, n_ct, level, scratch, scratch_bytes, stream,
                             "ckks_ct_mul_relin_rescale");
+}
+
+extern "C" size_t ckks_rotate_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level) {
+  return ckks_ct_mul_scratch_bytes(ctx, n_ct, level);
+}
+
+extern "C" int ckks_rotate(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct, const uint64_t* key,
+                           int n_ct, int level, uint64_t nu, void* scratch, size_t scratch_bytes,
+                           void* stream) {
+  const char* fn = "ckks_rotate";
+  CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
+  CKKS_REQUIRE(ctx->n_special == 1, "%s: context needs exactly one special prime", fn);
+  CKKS_REQUIRE(level >= 1 && level <= ctx->n_q, "%s: level=%d outside [1, %d]", fn, level, ctx->n_q);
+  CKKS_REQUIRE(ctx->log_n >= 6, "%s: log_n=%d below the supported minimum 6", fn, ctx->log_n);
+  CKKS_REQUIRE(n_ct >= 0, "%s: n_ct < 0", fn);
+  const u64 nu2n = nu & (2ull * ctx->n - 1);
+  CKKS_REQUIRE(nu2n & 1, "%s: nu=%llu must be odd (a Galois element)", fn, (unsigned long long)nu);
+  u64 pmin = ~0ull, pmax = 0;
+  for (int i = 0; i < ctx->n_primes; ++i) {
+    CKKS_REQUIRE(ctx->has_nega[i], "%s: prime %d has no 2N-th root", fn, i);
+    pmin = ctx->primes[i] < pmin ? ctx->primes[i] : pmin;
+    pmax = ctx->primes[i] > pmax ? ctx->primes[i] : pmax;
+  }
+  CKKS_REQUIRE(pmax < 2 * pmin, "%s: primes must satisfy max < 2 min (centred basis conversion)", fn);
+  if (n_ct == 0) return CKKS_OK;
+  CKKS_REQUIRE(out && ct && key && scratch, "%s: NULL pointer argument", fn);
+  CKKS_REQUIRE(out != ct, "%s: out must differ from ct", fn);
+  const size_t need = ckks_rotate_scratch_bytes(ctx, n_ct, level);
+  CKKS_REQUIRE(scratch_bytes >= need, "%s: scratch of %zu bytes < %zu needed", fn, scratch_bytes, need);
+  CmScratch S = cm_carve(scratch, ctx->n, n_ct, level);
+  cudaStream_t st = as_stream(stream);
+  return dispatch_cm(ctx->log_n, ctx->tune_cm_k, ctx->tune_cm_minb, [&]<int L, int K, int MINB>() -> int {
+    using Sh = NttShape<L, K>;
+    const int smem_a = Sh::SMEM_WORDS * 8;
+    const int smem_b = (Sh::SMEM_WORDS + 2 * Sh::N) * 8;
+    const int smem_c = (Sh::SMEM_WORDS + Sh::N) * 8;
+    auto ka = k_rot_prep<L, K, MINB>;
+    auto kb = k_cm_modup<L, K, MINB>;
+    auto kc = k_ks_down<L, K, MINB>;
+    ensure_smem(ka, smem_a);
+    ensure_smem(kb, smem_b);
+    ensure_smem(kc, smem_c);
+    {
+      ProfSpan span(CKKS_STAGE_OTHER, st);
+      ka<<<grid1d((long long)n_ct * level), Sh::T, smem_a, st>>>(reinterpret_cast<const u64*>(ct), S,
+                                                                 level, nu2n, ctx->d_pi, ctx->d_tw);
+    }
+    if (int rc = ckks_check_launch(fn)) return rc;
+    {
+      ProfSpan span(CKKS_STAGE_CM_MODUP, st);
+      kb<<<grid1d((long long)n_ct * (level + 1)), Sh::T, smem_b, st>>>(
+          S, reinterpret_cast<const ulonglong2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw);
+    }
+    if (int rc = ckks_check_launch(fn)) return rc;
+    {
+      ProfSpan span(CKKS_STAGE_CM_DOWN, st);
+      kc<<<grid1d((long long)n_ct * 2), Sh::T, smem_c, st>>>(S, reinterpret_cast<u64*>(out), level,
+                                                             ctx->n_q, ctx->d_pi, ctx->d_tw, ctx->d_pinv);
+    }
+    return ckks_check_launch(fn);
+  }, fn);
 }

@@ -418,6 +418,43 @@ int ckks_ct_mul_plain_rescale(const ckks_ctx* ctx, uint64_t* out, const uint64_t
 int ckks_modmul_peak(uint64_t* out, int n_blocks, int threads, int iters, int kind, uint64_t q,
                      uint64_t w, void* stream);
 
+/*
+ * Ring automorphism psi_nu(f)(X) = f(X^nu) mod (X^N + 1) of n_polys x n_limbs
+ * limbs (primes prime_begin ..), out != in.  Coefficient domain
+ * (eval_domain = 0): any nu >= 0 (coefficient k goes to nu k mod N with sign
+ * (-1)^floor(nu k / N), colliding terms summed), the reference's
+ * scripts/exp_e24_rotation_bootstrap.py:143 automorphism_exact and :167
+ * automorphism_key_exact.  Evaluation domain (eval_domain = 1, bit-reversed
+ * order of ckks_ntt, negacyclic primes): odd nu, a permutation of the slots.
+ */
+int ckks_automorphism(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in, int n_polys,
+                      int prime_begin, int n_limbs, uint64_t nu, int eval_domain, void* stream);
+
+/*
+ * Coefficient-domain product with the monomial X^nu in Z_q[X]/(X^N + 1)
+ * (nu taken mod 2N; X^N = -1), out != in.  Replaces
+ * scripts/exp_e24_rotation_bootstrap.py:189 poly_mul_x_power and :232 rotate
+ * (ct x X^nu), which agree with it for nu < N (they reduce nu mod N first).
+ */
+int ckks_mul_monomial(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in, int n_polys,
+                      int prime_begin, int n_limbs, uint64_t nu, void* stream);
+
+/*
+ * Homomorphic automorphism with key switching ("rotation"): ct [n_ct][2][level][N]
+ * (evaluation domain) -> out [n_ct][2][level][N] decrypting to psi_nu(m) under
+ * the same secret, nu odd.  `key` is a Galois key prepared by
+ * ckks_relin_key_prepare from ksk[j] = (-a_j s + e_j + delta_ij (P mod q_j)
+ * psi_nu(s), a_j) over the L + 1 primes (the relinearisation key with s^2
+ * replaced by psi_nu(s)); hybrid key switching with dnum = level digits, no
+ * rescale.  Scratch: ckks_rotate_scratch_bytes(ctx, n_ct, level) bytes.
+ * The reference rotates coefficient-encoded messages by X^nu without key
+ * switching (scripts/exp_e24_rotation_bootstrap.py:232 rotate); slot
+ * rotations of slot-packed ciphertexts need this Galois form.
+ */
+size_t ckks_rotate_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level);
+int ckks_rotate(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct, const uint64_t* key, int n_ct,
+                int level, uint64_t nu, void* scratch, size_t scratch_bytes, void* stream);
+
 /* Size of the static device scratch used by ckks_ct_mul_relin_rescale_noalloc. */
 #define CKKS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 

@@ -329,5 +329,50 @@ def main() -> int:
     return 0
 
 
+def rotation_vectors() -> int:
+    """Automorphism and monomial-product goldens from
+    scripts/exp_e24_rotation_bootstrap.py:143 automorphism_exact, :167
+    automorphism_key_exact and :189 poly_mul_x_power -> golden_rot.npz/json."""
+    cwd = os.getcwd()
+    try:
+        e24 = load("scripts/exp_e24_rotation_bootstrap.py", "ref_e24")
+    finally:
+        os.chdir(cwd)  # the module changes directory at import
+    arrays: dict[str, np.ndarray] = {}
+    cases = []
+    rng = np.random.default_rng(2024)
+    for n, q, nus in ((16, 113, (3, 5, 4, 0, 31, 17)),
+                      (1024, 998244353, (5, 2047, 6, 1025, 3 * 1024 + 7)),
+                      (4096, 35184371884033, (5, 25, 8191, 12, 4097))):
+        c0 = rng.integers(0, q, n).astype(np.int64)
+        c1 = rng.integers(0, q, n).astype(np.int64)
+        for nu in nus:
+            g0, g1 = e24.automorphism_exact((c0, c1), nu, n, q)
+            tag = f"aut_{n}_{nu}"
+            arrays[tag + "_in"] = np.stack([c0, c1]).astype(np.uint64)
+            arrays[tag + "_out"] = np.stack([np.asarray(g0), np.asarray(g1)]).astype(np.int64).astype(np.uint64)
+            cases.append({"kind": "automorphism_exact", "n": n, "q": q, "nu": nu, "key": tag})
+        for nu in (0, 1, 7, n // 2, n - 1):
+            out = e24.poly_mul_x_power(c0, nu, n, q)
+            tag = f"mono_{n}_{nu}"
+            arrays[tag + "_in"] = c0.astype(np.uint64)
+            arrays[tag + "_out"] = np.asarray(out).astype(np.int64).astype(np.uint64)
+            cases.append({"kind": "poly_mul_x_power", "n": n, "q": q, "nu": nu, "key": tag})
+    s = rng.integers(-1, 2, 1024)
+    ks = e24.automorphism_key_exact(s, 5, 1024, 998244353)
+    arrays["autkey_in"] = s.astype(np.int64)
+    arrays["autkey_out"] = np.asarray(ks).astype(np.int64).astype(np.uint64)
+    cases.append({"kind": "automorphism_key_exact", "n": 1024, "q": 998244353, "nu": 5, "key": "autkey"})
+    np.savez_compressed(OUT / "golden_rot.npz", **arrays)
+    with open(OUT / "golden_rot.json", "w") as f:
+        json.dump({"reference": "YI-HAIBO/cipher-pu", "generator": "tests/golden/make_golden.py --only rot",
+                   "source": "scripts/exp_e24_rotation_bootstrap.py:143,167,189", "cases": cases}, f, indent=1)
+    print("wrote", OUT / "golden_rot.npz")
+    return 0
+
+
 if __name__ == "__main__":
-    sys.exit(main())
+    if sys.argv[1:] == ["--only", "rot"]:
+        sys.exit(rotation_vectors())
+    rc = main()
+    sys.exit(rc or rotation_vectors())

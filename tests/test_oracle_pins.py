@@ -264,3 +264,24 @@ def test_dare_golden_semantics():
     new_c0, new_c1, dec = OE.dare_refresh(c0, c1, s, [(-int(x)) % q for x in a2], ARR["dare_e_new"], q)
     assert dec == [int(x) for x in ARR["dare_dec"]]
     assert new_c0 == [int(x) % q for x in ARR["dare_ct2_b"]]
+
+
+def test_galois_oracle_matches_reference_goldens():
+    """oracle.galois against scripts/exp_e24_rotation_bootstrap.py:143,167,189
+    outputs (tests/golden/golden_rot.npz, made by make_golden.py --only rot)."""
+    from oracle import galois as GA
+    rot = np.load(GD / "golden_rot.npz")
+    meta = json.load(open(GD / "golden_rot.json"))
+    seen = set()
+    for c in meta["cases"]:
+        k, q, nu, n = c["key"], c["q"], c["nu"], c["n"]
+        if c["kind"] == "automorphism_exact":
+            got = GA.automorphism_coef(rot[k + "_in"], nu, q)
+        elif c["kind"] == "poly_mul_x_power":
+            got = GA.mul_monomial(rot[k + "_in"], nu, q)      # nu < N here: same as the reference
+        else:
+            s = np.mod(rot[k + "_in"], q).astype(np.uint64)
+            got = GA.automorphism_coef(s, nu, q)
+        assert np.array_equal(got, rot[k + "_out"]), c
+        seen.add(c["kind"])
+    assert seen == {"automorphism_exact", "poly_mul_x_power", "automorphism_key_exact"}
