@@ -117,12 +117,12 @@ static int dispatch_cm(int log_n, int kreq, int mreq, F&& f, const char* fn) {
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_tensor(const u64* __restrict__ A, const u64* __restrict__ B, CmScratch S, int level,
-                const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw) {
+                const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
-  const long long ct = blockIdx.x / level;
-  const int j = blockIdx.x % level;
+  const int j = blockIdx.x / n_ct;  // limb-major: resident CTAs share q_j's tables
+  const long long ct = blockIdx.x % n_ct;
   const int tid = threadIdx.x;
   const PrimeInfo P = pi[j];
   const size_t LN = (size_t)level * N;
@@ -164,15 +164,15 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_modup(CmScratch S, const ulonglong2* __restrict__ key, int level, int nq,
-               const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw) {
+               const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
   constexpr int T = Sh::T;
   u64* acc0s = sm + Sh::SMEM_WORDS;
   u64* acc1s = acc0s + N;
-  const long long ct = blockIdx.x / (level + 1);
-  const int ti = blockIdx.x % (level + 1);
+  const int ti = blockIdx.x / n_ct;  // target-major: resident CTAs share one prime
+  const long long ct = blockIdx.x % n_ct;
   const bool special = ti == level;
   const int pidx = special ? nq : ti;
   const int tid = threadIdx.x;
@@ -303,12 +303,12 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_rot_prep(const u64* __restrict__ C, CmScratch S, int level, u64 nu2n,
-               const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw) {
+               const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
-  const long long ct = blockIdx.x / level;
-  const int j = blockIdx.x % level;
+  const int j = blockIdx.x / n_ct;
+  const long long ct = blockIdx.x % n_ct;
   const int tid = threadIdx.x;
   const PrimeInfo P = pi[j];
   const size_t LN = (size_t)level * N;
@@ -450,13 +450,13 @@ int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
       ProfSpan span(CKKS_STAGE_CM_TENSOR, st);
       ka<<<grid1d((long long)n_ct * level), Sh::T, smem_a, st>>>(
           reinterpret_cast<const u64*>(ct_a), reinterpret_cast<const u64*>(ct_b), S, level,
-          ctx->d_pi, ctx->d_tw);
+          ctx->d_pi, ctx->d_tw, n_ct);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {
       ProfSpan span(CKKS_STAGE_CM_MODUP, st);
       kb<<<grid1d((long long)n_ct * (level + 1)), Sh::T, smem_bc, st>>>(
-          S, reinterpret_cast<const ulonglong2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw);
+          S, reinterpret_cast<const ulonglong2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {
@@ -520,13 +520,13 @@ extern "C" int ckks_rotate(const ckks_ctx* ctx, uint64_t* out, const uint64_t* c
     {
       ProfSpan span(CKKS_STAGE_OTHER, st);
       ka<<<grid1d((long long)n_ct * level), Sh::T, smem_a, st>>>(reinterpret_cast<const u64*>(ct), S,
-                                                                 level, nu2n, ctx->d_pi, ctx->d_tw);
+                                                                 level, nu2n, ctx->d_pi, ctx->d_tw, n_ct);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {
       ProfSpan span(CKKS_STAGE_CM_MODUP, st);
       kb<<<grid1d((long long)n_ct * (level + 1)), Sh::T, smem_b, st>>>(
-          S, reinterpret_cast<const ulonglong2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw);
+          S, reinterpret_cast<const ulonglong2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {

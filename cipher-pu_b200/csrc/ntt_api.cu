@@ -4,35 +4,43 @@
 #include "profile.hpp"
 
 // ------------------------------------------------------------------ NTT
+// One CTA per limb-transform.  Limb-major grid (blockIdx = limb * n_polys +
+// poly), so the CTAs resident on an SM at a time share one prime's twiddle
+// tables in L1.  Global traffic is lane-contiguous (layout C) both ways; the
+// forward's layout-Z result is re-distributed through shared memory first.
+// CTAs per SM the standalone transform's register budget targets: three
+// 256-thread CTAs (85 registers) where the CTA is small enough.
 template <int LOGN, int K>
-__global__ void __launch_bounds__(NttShape<LOGN, K>::T)
-    k_ntt(u64* __restrict__ data, int n_limbs, int prime_begin, const PrimeInfo* __restrict__ pi,
-          const TwD* __restrict__ tw, int inverse, int cyclic) {
+struct NttMinBlocks {
+  static constexpr int T = NttShape<LOGN, K>::T;
+  static constexpr int value = T >= 512 ? 1 : (768 / T > 8 ? 8 : 768 / T);
+};
+
+template <int LOGN, int K>
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T, (NttMinBlocks<LOGN, K>::value))
+    k_ntt(u64* __restrict__ data, int n_polys, int n_limbs, int prime_begin,
+          const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int inverse, int cyclic) {
   extern __shared__ u64 sm[];
   using S = NttShape<LOGN, K>;
-  const int limb = blockIdx.x % n_limbs;
-  const long long poly = blockIdx.x / n_limbs;
+  const int limb = blockIdx.x / n_polys;
+  const long long poly = blockIdx.x % n_polys;
   const int pidx = prime_begin + limb;
   const PrimeInfo P = pi[pidx];
   u64* d = data + ((size_t)poly * n_limbs + limb) * S::N;
   const TwD* tb = twbase<LOGN>(tw, pidx);
   const int tid = threadIdx.x;
   u64 x[S::E];
-  if (!inverse) {
 #pragma unroll
-    for (int e = 0; e < S::E; ++e) x[e] = reduce_any(d[posC<LOGN, K>(tid, e)], P);
+  for (int e = 0; e < S::E; ++e) x[e] = reduce_any(ld_stream(d + posC<LOGN, K>(tid, e)), P);
+  if (!inverse) {
     ntt_fwd<LOGN, K>(x, sm, tid, tb, P, cyclic);
     if constexpr (S::NP == 0) __syncthreads();
-#pragma unroll
-    for (int e = 0; e < S::E; ++e) d[posZ<LOGN, K>(tid, e)] = x[e];
+    z_to_c<LOGN, K>(x, sm, tid);
   } else {
-#pragma unroll
-    for (int e = 0; e < S::E; ++e) x[e] = reduce_any(d[posZ<LOGN, K>(tid, e)], P);
+    c_to_z<LOGN, K>(x, sm, tid);
     ntt_inv<LOGN, K>(x, sm, tid, tb, P, cyclic);
-    if constexpr (S::NP == 0) __syncthreads();
-#pragma unroll
-    for (int e = 0; e < S::E; ++e) d[posC<LOGN, K>(tid, e)] = x[e];
   }
+  store_c<LOGN, K>(x, d, tid);
 }
 
 static int check_limbs(const ckks_ctx* ctx, int prime_begin, int n_limbs, const char* fn) {
@@ -60,7 +68,8 @@ extern "C" int ckks_ntt(const ckks_ctx* ctx, uint64_t* data, int n_polys, int pr
     ensure_smem(kern, S::SMEM_WORDS * 8);
     ProfSpan span(CKKS_STAGE_NTT, as_stream(stream));
     kern<<<grid1d((long long)n_polys * n_limbs), S::T, S::SMEM_WORDS * 8, as_stream(stream)>>>(
-        reinterpret_cast<u64*>(data), n_limbs, prime_begin, ctx->d_pi, ctx->d_tw, inverse, cyclic);
+        reinterpret_cast<u64*>(data), n_polys, n_limbs, prime_begin, ctx->d_pi, ctx->d_tw, inverse,
+        cyclic);
     return ckks_check_launch("ckks_ntt");
   });
 }
@@ -135,12 +144,12 @@ extern "C" int ckks_vec_addsub(uint64_t* out, const uint64_t* a, const uint64_t*
 template <int LOGN, int K>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     k_poly_mul(u64* __restrict__ out, const u64* __restrict__ a, const u64* __restrict__ b,
-               int n_limbs, int prime_begin, const PrimeInfo* __restrict__ pi,
+               int n_polys, int n_limbs, int prime_begin, const PrimeInfo* __restrict__ pi,
                const TwD* __restrict__ tw, int cyclic) {
   extern __shared__ u64 sm[];
   using S = NttShape<LOGN, K>;
-  const int limb = blockIdx.x % n_limbs;
-  const long long poly = blockIdx.x / n_limbs;
+  const int limb = blockIdx.x / n_polys;  // limb-major, like k_ntt
+  const long long poly = blockIdx.x % n_polys;
   const int pidx = prime_begin + limb;
   const PrimeInfo P = pi[pidx];
   const size_t off = ((size_t)poly * n_limbs + limb) * S::N;
@@ -178,7 +187,7 @@ extern "C" int ckks_poly_mul(const ckks_ctx* ctx, uint64_t* out, const uint64_t*
     ensure_smem(kern, S::SMEM_WORDS * 8);
     kern<<<grid1d((long long)n_polys * n_limbs), S::T, S::SMEM_WORDS * 8, as_stream(stream)>>>(
         reinterpret_cast<u64*>(out), reinterpret_cast<const u64*>(a),
-        reinterpret_cast<const u64*>(b), n_limbs, prime_begin, ctx->d_pi, ctx->d_tw, cyclic);
+        reinterpret_cast<const u64*>(b), n_polys, n_limbs, prime_begin, ctx->d_pi, ctx->d_tw, cyclic);
     return ckks_check_launch("ckks_poly_mul");
   });
 }

@@ -88,8 +88,8 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   u64* dst = out + (size_t)poly * t * S::N;
   const PrimeInfo PT = pi[t];
   u64 w[S::E];
-#pragma unroll
-  for (int e = 0; e < S::E; ++e) w[e] = src[(size_t)t * S::N + posZ<LOGN, K>(tid, e)];
+  load_c<LOGN, K>(w, src + (size_t)t * S::N, tid);
+  c_to_z<LOGN, K>(w, sm, tid);
   ntt_inv<LOGN, K>(w, sm, tid, twbase<LOGN>(tw, t), PT);
 #pragma unroll 1
   for (int i = 0; i < t; ++i) {
@@ -98,15 +98,13 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     u64 x[S::E];
 #pragma unroll
     for (int e = 0; e < S::E; ++e) x[e] = w[e] > PT.half ? w[e] - PT.q + P.q : w[e];  // [w_c]_{q_i}
-    __syncthreads();
     ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
+    z_to_c<LOGN, K>(x, sm, tid);
+    u64 xi[S::E];
+    load_c<LOGN, K>(xi, src + (size_t)i * S::N, tid);
 #pragma unroll
-    for (int e = 0; e < S::E; ++e) {
-      const int p = posZ<LOGN, K>(tid, e);
-      const u64 xi = src[(size_t)i * S::N + p];
-      const u64 d = xi + P.qlazy - x[e];  // (0, 33q)
-      dst[(size_t)i * S::N + p] = shoup(d, ci.w, ci.ws, P.q);
-    }
+    for (int e = 0; e < S::E; ++e) x[e] = shoup(xi[e] + P.qlazy - x[e], ci.w, ci.ws, P.q);
+    store_c<LOGN, K>(x, dst + (size_t)i * S::N, tid);
   }
 }
 
