@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 // thread-private shared-memory slots (index e * T + tid).
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
-    k_cm_modup(CmScratch S, const ulonglong2* __restrict__ key, int level, int nq,
+    k_cm_modup(CmScratch S, const double2* __restrict__ key, int level, int nq,
                const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
@@ -179,27 +179,38 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   const PrimeInfo P = pi[pidx];
   const size_t LN = (size_t)level * N;
   const TwD* tb = twbase<LOGN>(tw, pidx);
+  double* acc0s_d = reinterpret_cast<double*>(acc0s);
+  double* acc1s_d = reinterpret_cast<double*>(acc1s);
 #pragma unroll 1
   for (int j = 0; j < level; ++j) {
-    u64 x[Sh::E];
+    // digit j as exact doubles in layout C: its evaluation-domain residues at
+    // its own prime, else its coefficient residues (< q_j < 2 q_i) transformed
+    // unreduced (|x| < 2^51 on return, fine for fmulmod)
+    double x[Sh::E];
+    u64 xu[Sh::E];
     if (!special && j == ti) {
-      load_c<LOGN, K>(x, S.d2n + ct * LN + (size_t)j * N, tid);
+      load_c<LOGN, K>(xu, S.d2n + ct * LN + (size_t)j * N, tid);
+#pragma unroll
+      for (int e = 0; e < Sh::E; ++e) x[e] = u2d(xu[e]);
     } else {
-      // digit j residues (< q_j < 2 q_i) go into the transform unreduced
-      load_c<LOGN, K>(x, S.d2c + ct * LN + (size_t)j * N, tid);
-      ntt_fwd<LOGN, K>(x, sm, tid, tb, P);
+      load_c<LOGN, K>(xu, S.d2c + ct * LN + (size_t)j * N, tid);
+#pragma unroll
+      for (int e = 0; e < Sh::E; ++e) x[e] = u2d(xu[e]);
+      ntt_fwd_d<LOGN, K>(x, sm, tid, tb, P);
       z_to_c<LOGN, K>(x, sm, tid);
     }
-    // one key polynomial at a time keeps at most E key words in flight
+    // key inner product in exact FP64: key words are (w, w / q) pairs; each
+    // product is within 0.75 q, the sum of `level` of them stays far below 2^51
 #pragma unroll 1
     for (int kk = 0; kk < 2; ++kk) {
-      const ulonglong2* kp = key + (((size_t)j * 2 + kk) * (nq + 1) + pidx) * N;
-      u64* acc = kk ? acc1s : acc0s;
+      const double2* kp = key + (((size_t)j * 2 + kk) * (nq + 1) + pidx) * N;
+      double* acc = kk ? acc1s_d : acc0s_d;
 #pragma unroll
       for (int e = 0; e < Sh::E; ++e) {
-        const ulonglong2 w = ld_stream2(kp + posC<LOGN, K>(tid, e));
+        const double2 w = ld_stream2d(kp + posC<LOGN, K>(tid, e));
         const int s = e * T + tid;
-        acc[s] = (j == 0 ? 0ull : acc[s]) + shoup_lazy(x[e], w.x, w.y, P.q);
+        const double t = fmulmod(x[e], w.x, w.y, P.qd);
+        acc[s] = j == 0 ? t : __dadd_rn(acc[s], t);
       }
     }
   }
@@ -213,7 +224,8 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   for (int k = 0; k < 2; ++k) {
     const u64* a = k ? acc1s : acc0s;
 #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) x[e] = reduce_any(a[e * T + tid], P);
+    for (int e = 0; e < Sh::E; ++e)
+      x[e] = d2canon(reinterpret_cast<const double*>(a)[e * T + tid], P.qd, P.qinv_d);
     store_c<LOGN, K>(x, o + (size_t)k * kstride, tid);
   }
 }
@@ -379,21 +391,15 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 }
 
 // ---------------------------------------------------------------- key prep
-__global__ void k_key_prepare(ulonglong2* __restrict__ out, const u64* __restrict__ in,
+__global__ void k_key_prepare(double2* __restrict__ out, const u64* __restrict__ in,
                               long long total, int log_n, int nlimb,
                               const PrimeInfo* __restrict__ pi) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= total) return;
   const int limb = (int)((idx >> log_n) % nlimb);
   const PrimeInfo P = pi[limb];
-  const u64 w = in[idx] % P.q;
-  // floor(w 2^64 / q) = w * floor(2^64 / q) + floor(w (2^64 mod q) / q)
-  const u64 num_lo = w * P.r_mod;
-  u64 qt = (u64)floor(__dmul_rn(__ull2double_rn(w), __ull2double_rn(P.r_mod)) * P.qinv_d);
-  i64 rem = (i64)(num_lo - qt * P.q);
-  for (int it = 0; it < 3 && rem < 0; ++it) { rem += (i64)P.q; --qt; }
-  for (int it = 0; it < 3 && rem >= (i64)P.q; ++it) { rem -= (i64)P.q; ++qt; }
-  out[idx] = make_ulonglong2(w, w * P.one_s + qt);
+  const double w = u2d(in[idx] % P.q);
+  out[idx] = make_double2(w, __ddiv_rn(w, P.qd));  // (w, w / q), the FP64 product's operands
 }
 
 extern "C" int ckks_relin_key_prepare(const ckks_ctx* ctx, uint64_t* prepared,
@@ -402,7 +408,7 @@ extern "C" int ckks_relin_key_prepare(const ckks_ctx* ctx, uint64_t* prepared,
   CKKS_REQUIRE(ctx->n_special == 1, "ckks_relin_key_prepare: context needs one special prime");
   const long long total = (long long)ctx->n_q * 2 * ctx->n_primes * ctx->n;
   k_key_prepare<<<grid1d((total + 255) / 256), 256, 0, as_stream(stream)>>>(
-      reinterpret_cast<ulonglong2*>(prepared), reinterpret_cast<const u64*>(ksk), total,
+      reinterpret_cast<double2*>(prepared), reinterpret_cast<const u64*>(ksk), total,
       ctx->log_n, ctx->n_primes, ctx->d_pi);
   return ckks_check_launch("ckks_relin_key_prepare");
 }
@@ -456,7 +462,7 @@ int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
     {
       ProfSpan span(CKKS_STAGE_CM_MODUP, st);
       kb<<<grid1d((long long)n_ct * (level + 1)), Sh::T, smem_bc, st>>>(
-          S, reinterpret_cast<const ulonglong2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
+          S, reinterpret_cast<const double2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {
@@ -526,7 +532,7 @@ extern "C" int ckks_rotate(const ckks_ctx* ctx, uint64_t* out, const uint64_t* c
     {
       ProfSpan span(CKKS_STAGE_CM_MODUP, st);
       kb<<<grid1d((long long)n_ct * (level + 1)), Sh::T, smem_b, st>>>(
-          S, reinterpret_cast<const ulonglong2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
+          S, reinterpret_cast<const double2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {

@@ -253,29 +253,31 @@ __device__ __forceinline__ const TwD* twbase(const TwD* tw, int prime) {
   return tw + (size_t)prime * TWF_SLOTS * (1 << LOGN);
 }
 
+// Forward NTT on exact doubles: layout C in (integers of magnitude < 4q),
+// layout Z out, unreduced: |result| < 4q + 0.75 q LOGN < 2^51 (an input to
+// fmulmod or d2canon as it stands).
+template <int LOGN, int K>
+__device__ __forceinline__ void ntt_fwd_d(double (&d)[1 << K], u64* sm, int tid,
+                                          const TwD* __restrict__ tb, const PrimeInfo& P,
+                                          bool cyclic = false) {
+  constexpr int N = 1 << LOGN;
+  static_assert(K <= 4, "forward twiddle layouts exist for K <= 4");
+  const TwD* tw = tb + (cyclic ? (K == 3 ? TWF_FWDC3 : TWF_FWDC4) : (K == 3 ? TWF_FWD3 : TWF_FWD4)) * N;
+  double* smd = reinterpret_cast<double*>(sm);
+  fwd_pass<LOGN, K, 0, K>(d, tid, tw, P.qd);
+  FwdRest<LOGN, K, 1>::run(d, smd, tid, tw, P.qd);
+}
+
 // Forward NTT: layout C in (values < 4q), layout Z out, canonical [0, q).
 template <int LOGN, int K>
 __device__ __forceinline__ void ntt_fwd(u64 (&x)[1 << K], u64* sm, int tid, const TwD* __restrict__ tb,
                                         const PrimeInfo& P, bool cyclic = false) {
-  constexpr int N = 1 << LOGN;
-  static_assert(K <= 4, "forward twiddle layouts exist for K <= 4");
-  const TwD* tw = tb + (cyclic ? (K == 3 ? TWF_FWDC3 : TWF_FWDC4) : (K == 3 ? TWF_FWD3 : TWF_FWD4)) * N;
   double d[1 << K];
 #pragma unroll
   for (int e = 0; e < (1 << K); ++e) d[e] = u2d(x[e]);
-  double* smd = reinterpret_cast<double*>(sm);
-  fwd_pass<LOGN, K, 0, K>(d, tid, tw, P.qd);
-  FwdRest<LOGN, K, 1>::run(d, smd, tid, tw, P.qd);
+  ntt_fwd_d<LOGN, K>(d, sm, tid, tb, P, cyclic);
 #pragma unroll
   for (int e = 0; e < (1 << K); ++e) x[e] = d2canon(d[e], P.qd, P.qinv_d);
-}
-
-// Historical name kept for the call sites: the FP64 forward already returns
-// canonical residues.
-template <int LOGN, int K>
-__device__ __forceinline__ void ntt_fwd_lazy(u64 (&x)[1 << K], u64* sm, int tid,
-                                             const TwD* __restrict__ tb, const PrimeInfo& P) {
-  ntt_fwd<LOGN, K>(x, sm, tid, tb, P);
 }
 
 // Inverse NTT (with N^-1): layout Z in (canonical), layout C out, canonical.

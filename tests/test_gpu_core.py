@@ -179,12 +179,11 @@ def test_ct_mul_relin_rescale_vs_oracle(ck, log_n, levels, level, n_ct):
     a[0, 0, 0, :4] = [0, qs[0] - 1, 1, qs[0] - 2]
     ksk = _rand_ct(rng, (levels, 2, levels + 1, n), list(P.q) + [P.special])
     key = ops.relin_key_prepare(ctx, ops.to_device(ksk))
-    # the prepared key holds (value, floor(value 2^64 / q)) pairs
-    kp = ops.to_host(key)
-    assert np.array_equal(kp[..., 0], ksk)
-    qq = np.array(list(P.q) + [P.special], dtype=object)
-    j, k, l, i = 0, 1, levels, 7
-    assert int(kp[j, k, l, i, 1]) == (int(ksk[j, k, l, i]) << 64) // int(qq[l])
+    # the prepared key holds (value, value / q) pairs of doubles
+    kp = ops.to_host(key).view(np.float64)
+    assert np.array_equal(kp[..., 0], ksk.astype(np.float64))
+    qq = np.array(list(P.q) + [P.special], dtype=np.float64)
+    assert np.array_equal(kp[..., 1], ksk.astype(np.float64) / qq[None, None, :, None])
     got = ops.to_host(ops.ct_mul_relin_rescale(ctx, ops.to_device(a), ops.to_device(b), key))
     sub_ksk = ksk[:level][:, :, list(range(level)) + [levels]]
     exp = R.ct_mul_relin_rescale(a, b, sub_ksk, qs, P.special)
