@@ -33,23 +33,26 @@ def cnn_28x28(seed: int = 0) -> list:
     rng = np.random.default_rng(seed)
     C, K, S, IN, OUT = 8, 5, 2, 28, 12
     kern = rng.standard_normal((C, K, K)) / math.sqrt(K * K)
+    # conv output (c, i, j) is row (i OUT + j) C + c: the C channels of one
+    # output pixel are adjacent, so a 4-row weight block shares one 5x5
+    # receptive field (dense blocks, few input columns per output tile)
     Wc = np.zeros((C * OUT * OUT, IN * IN))
     for c in range(C):
         for i in range(OUT):
             for j in range(OUT):
-                r = (c * OUT + i) * OUT + j
+                r = (i * OUT + j) * C + c
                 for di in range(K):
                     for dj in range(K):
                         Wc[r, (S * i + di) * IN + (S * j + dj)] = kern[c, di, dj]
-    bc = np.repeat(rng.standard_normal(C) * 0.1, OUT * OUT)
+    bc = np.tile(rng.standard_normal(C) * 0.1, OUT * OUT)
     Wfc = rng.standard_normal((10, C * 6 * 6)) / math.sqrt(C * 36)
     bfc = rng.standard_normal(10) * 0.1
-    # fold the 2x2 average pool into the FC: W_eff[o, (c, i, j)] = Wfc[o, (c, i//2, j//2)] / 4
+    # fold the 2x2 average pool into the FC: W_eff[o, (i, j, c)] = Wfc[o, (c, i//2, j//2)] / 4
     We = np.zeros((10, C * OUT * OUT))
     for c in range(C):
         for i in range(OUT):
             for j in range(OUT):
-                We[:, (c * OUT + i) * OUT + j] = Wfc[:, (c * 6 + i // 2) * 6 + j // 2] / 4.0
+                We[:, (i * OUT + j) * C + c] = Wfc[:, (c * 6 + i // 2) * 6 + j // 2] / 4.0
     return [Layer(Wc, bc, "square"), Layer(We, bfc, "none")]
 
 

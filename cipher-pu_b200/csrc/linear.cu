@@ -10,94 +10,204 @@
 // |w| < 2^24 are accumulated in signed 64-bit (|sum| < 2^57 for <= 1024
 // inputs; |sum| < 2^59 for 2048), reduced once per output element.
 //
-// Tiling: one CTA = 16 outputs (four 4-row blocks) x 256 positions, one
-// position per thread; the weight tile and the block-keep mask live in
-// shared memory.  A 4-input column block is loaded only when one of the four
-// row blocks keeps it, and each kept 4x4 block costs 16 x 2 IMAD.WIDE per
-// position, so the work scales with the kept fraction.
+// Tiling (k_linear below): a modular GEMM tile of 32 outputs x 128 positions
+// per CTA, 4 x 4 accumulator pairs per thread, input tiles double-buffered in
+// shared memory by cp.async.  Skipped 4x4 weight blocks cost nothing, and an
+// input column block that no row block of the CTA keeps is never loaded, so
+// both the multiplies and the input traffic scale with the kept fraction.
 #include "dispatch.cuh"
 
-constexpr int LIN_OT = 16;     // outputs per CTA
-constexpr int LIN_THREADS = 256;
+constexpr int LIN_ROWB = 8;                  // 4-row blocks per CTA (one per warp)
+constexpr int LIN_OT = 4 * LIN_ROWB;         // outputs per CTA
+constexpr int LIN_PT = 128;                  // positions per CTA (4 per lane)
+constexpr int LIN_THREADS = 32 * LIN_ROWB;
+constexpr int LIN_CB = 8;                    // column blocks (4 inputs each) per pipeline chunk
 constexpr int LIN_MAX_IN = 2048;
 
-__global__ void __launch_bounds__(LIN_THREADS)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem),
+               "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int NPEND>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPEND)); }
+
+// acc += a * b with a 32 x 32 -> 64-bit signed multiply-add
+__device__ __forceinline__ void mad_wide(long long& acc, int a, int b) {
+  asm("mad.wide.s32 %0, %1, %2, %0;" : "+l"(acc) : "r"(a), "r"(b));
+}
+
+struct LinSmem {
+  u64 x[2][LIN_CB * 4][LIN_PT];   // input tiles: [buffer][input slot][position]
+  int w[2][LIN_CB * 4][LIN_OT];   // weight tiles: [buffer][input slot][output]
+  unsigned char keep[2][LIN_CB][LIN_ROWB];
+  int cbl[LIN_MAX_IN / 4];        // column blocks some row block of the CTA keeps
+  int ncb;
+};
+
+// One CTA = 32 outputs x 128 positions; warp r owns outputs o0 + 4r .. + 3
+// (one 4-row block, so the block-keep test is warp-uniform), lane l owns
+// positions p0 + 2l, +1 and p0 + 64 + 2l, +1 (16-byte shared loads that are
+// contiguous across the warp: no bank conflicts).  The input column blocks that none of the CTA's
+// row blocks keeps are skipped entirely (neither loaded nor multiplied); the
+// others stream through a two-stage cp.async pipeline of LIN_CB blocks.
+__global__ void __launch_bounds__(LIN_THREADS, 2)
     k_linear(u64* __restrict__ out, const u64* __restrict__ in, const int* __restrict__ w,
              const long long* __restrict__ bias, const unsigned char* __restrict__ keep, int n_out,
              int n_in, int level, int log_n, const PrimeInfo* __restrict__ pi) {
-  extern __shared__ int lin_sm[];
+  extern __shared__ __align__(16) unsigned char lin_raw[];
+  LinSmem& S = *reinterpret_cast<LinSmem*>(lin_raw);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int o0 = blockIdx.y * LIN_OT;
+  const long long npos = (2ll * level) << log_n;
+  const long long p0 = (long long)blockIdx.x * LIN_PT;
   const int nb_in = (n_in + 3) / 4;
-  const int ldw = 4 * nb_in;  // padded row length of the weight tile
-  int* ws = lin_sm;                                                   // [LIN_OT][ldw]
-  unsigned char* ks = reinterpret_cast<unsigned char*>(lin_sm + LIN_OT * ldw);  // [4][nb_in]
-  for (int t = threadIdx.x; t < LIN_OT * ldw; t += blockDim.x) {
-    const int r = t / ldw, f = t % ldw;
-    ws[t] = (o0 + r < n_out && f < n_in) ? w[(size_t)(o0 + r) * n_in + f] : 0;
-  }
-  for (int t = threadIdx.x; t < 4 * nb_in; t += blockDim.x) {
-    const int rb = t / nb_in, cb = t % nb_in;
-    const int orb = o0 / 4 + rb;
-    unsigned char k = 0;
-    if (o0 + 4 * rb < n_out) k = keep ? keep[(size_t)orb * nb_in + cb] : 1;
-    ks[t] = k;
+  const int rb0 = o0 / 4;
+  const int nrb = (n_out + 3) / 4;
+  auto kept = [&](int rb, int cb) -> bool {
+    if (rb >= nrb) return false;
+    return keep ? keep[(size_t)rb * nb_in + cb] != 0 : true;
+  };
+  // compact list of the column blocks this CTA needs (warp 0, ballot scan)
+  if (warp == 0) {
+    int base = 0;
+    for (int c0 = 0; c0 < nb_in; c0 += 32) {
+      const int cb = c0 + lane;
+      bool need = false;
+      if (cb < nb_in)
+        for (int r = 0; r < LIN_ROWB; ++r) need |= kept(rb0 + r, cb);
+      const unsigned m = __ballot_sync(0xffffffffu, need);
+      if (need) S.cbl[base + __popc(m & ((1u << lane) - 1))] = cb;
+      base += __popc(m);
+    }
+    if (lane == 0) S.ncb = base;
   }
   __syncthreads();
-  const long long npos = (2ll * level) << log_n;
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= npos) return;
-  const int limb = (int)((p >> log_n) % level);
-  const int comp = (int)(p / ((long long)level << log_n));
-  long long al[LIN_OT], ah[LIN_OT];
+  const int ncb = S.ncb;
+  const int nchunk = (ncb + LIN_CB - 1) / LIN_CB;
+
+  // stage chunk c into buffer b: inputs by cp.async, weights and keep bits by plain loads
+  auto stage_x = [&](int c, int b) {
 #pragma unroll
-  for (int o = 0; o < LIN_OT; ++o) al[o] = ah[o] = 0;
-  const u64 mask23 = (1ull << 23) - 1;
-#pragma unroll 1
-  for (int cb = 0; cb < nb_in; ++cb) {
-    const unsigned char k0 = ks[cb], k1 = ks[nb_in + cb], k2 = ks[2 * nb_in + cb],
-                        k3 = ks[3 * nb_in + cb];
-    if (!(k0 | k1 | k2 | k3)) continue;
-    long long xl[4], xh[4];
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-      const int f = 4 * cb + t;
-      const u64 x = f < n_in ? __ldg(in + (size_t)f * npos + p) : 0ull;
-      xl[t] = (long long)(x & mask23);
-      xh[t] = (long long)(x >> 23);
+    for (int u = 0; u < (LIN_CB * 4 * LIN_PT * 8) / (16 * LIN_THREADS); ++u) {
+      const int idx = tid + LIN_THREADS * u;           // 16-byte piece
+      const int row = idx / (LIN_PT / 2), col = idx % (LIN_PT / 2);
+      const int j = row >> 2, t = row & 3;
+      const int ci = c * LIN_CB + j;
+      const int f = ci < ncb ? 4 * S.cbl[ci] + t : n_in;
+      const long long p = p0 + 2 * col;
+      const bool valid = f < n_in && p < npos;
+      const u64* src = valid ? in + (size_t)f * npos + p : in;
+      cp_async16(&S.x[b][row][2 * col], src, valid);
     }
+  };
+  auto load_w = [&](int c, int (&wr)[(LIN_CB * 4 * LIN_OT) / LIN_THREADS]) {
 #pragma unroll
-    for (int rb = 0; rb < 4; ++rb) {
-      const unsigned char kk = rb == 0 ? k0 : rb == 1 ? k1 : rb == 2 ? k2 : k3;
-      if (!kk) continue;
+    for (int u = 0; u < (LIN_CB * 4 * LIN_OT) / LIN_THREADS; ++u) {
+      const int idx = tid + LIN_THREADS * u;
+      const int row = idx / LIN_OT, o = idx % LIN_OT;
+      const int ci = c * LIN_CB + (row >> 2);
+      const int f = ci < ncb ? 4 * S.cbl[ci] + (row & 3) : n_in;
+      wr[u] = (f < n_in && o0 + o < n_out) ? __ldg(w + (size_t)(o0 + o) * n_in + f) : 0;
+    }
+  };
+  auto store_w = [&](int c, int b, const int (&wr)[(LIN_CB * 4 * LIN_OT) / LIN_THREADS]) {
 #pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        const int o = 4 * rb + r;
+    for (int u = 0; u < (LIN_CB * 4 * LIN_OT) / LIN_THREADS; ++u) {
+      const int idx = tid + LIN_THREADS * u;
+      S.w[b][idx / LIN_OT][idx % LIN_OT] = wr[u];
+    }
+    if (tid < LIN_CB * LIN_ROWB) {
+      const int j = tid / LIN_ROWB, r = tid % LIN_ROWB;
+      const int ci = c * LIN_CB + j;
+      S.keep[b][j][r] = ci < ncb ? (kept(rb0 + r, S.cbl[ci]) ? 1 : 0) : 0;
+    }
+  };
+
+  long long al[4][4], ah[4][4];
 #pragma unroll
-        for (int t = 0; t < 4; ++t) {
-          const long long wv = ws[o * ldw + 4 * cb + t];
-          al[o] += wv * xl[t];
-          ah[o] += wv * xh[t];
+  for (int r = 0; r < 4; ++r)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) al[r][i] = ah[r][i] = 0;
+  const u64 mask23 = (1ull << 23) - 1;
+  int wr[(LIN_CB * 4 * LIN_OT) / LIN_THREADS];
+  if (nchunk > 0) {
+    stage_x(0, 0);
+    cp_async_commit();
+    load_w(0, wr);
+    store_w(0, 0, wr);
+  }
+#pragma unroll 1
+  for (int c = 0; c < nchunk; ++c) {
+    const int b = c & 1;
+    const bool more = c + 1 < nchunk;
+    if (more) {
+      stage_x(c + 1, b ^ 1);
+      cp_async_commit();
+      load_w(c + 1, wr);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int j = 0; j < LIN_CB; ++j) {
+      if (!S.keep[b][j][warp]) continue;  // warp-uniform
+#pragma unroll
+      for (int t = 0; t < 4; ++t) {
+        const int row = 4 * j + t;
+        const int4 wv = *reinterpret_cast<const int4*>(&S.w[b][row][4 * warp]);
+        const ulonglong2 xa = *reinterpret_cast<const ulonglong2*>(&S.x[b][row][2 * lane]);
+        const ulonglong2 xb = *reinterpret_cast<const ulonglong2*>(&S.x[b][row][LIN_PT / 2 + 2 * lane]);
+        const u64 xv[4] = {xa.x, xa.y, xb.x, xb.y};
+        const int wvv[4] = {wv.x, wv.y, wv.z, wv.w};
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          // 32 x 32 -> 64-bit multiply-adds (one IMAD.WIDE each): both halves
+          // of the residue fit in 24 bits, the weights in 24 bits
+          const int xl = (int)(xv[i] & mask23), xh = (int)(xv[i] >> 23);
+#pragma unroll
+          for (int r = 0; r < 4; ++r) {
+            mad_wide(al[r][i], wvv[r], xl);
+            mad_wide(ah[r][i], wvv[r], xh);
+          }
         }
       }
     }
+    if (more) store_w(c + 1, b ^ 1, wr);
+    __syncthreads();
   }
-  const PrimeInfo P = pi[limb];
-  const long long qs = (long long)P.q;
-  const u64 two23 = (1ull << 23) % P.q;
+  // epilogue: reduce, add the bias on component 0, store the two word pairs
 #pragma unroll
-  for (int o = 0; o < LIN_OT; ++o) {
-    if (o0 + o >= n_out) break;
-    long long rl = al[o] % qs;
-    if (rl < 0) rl += qs;
-    long long rh = ah[o] % qs;
-    if (rh < 0) rh += qs;
-    u64 v = addmod(mulmod((u64)rh, two23, P), (u64)rl, P.q);
-    if (bias && comp == 0) {
-      long long b = bias[o0 + o] % qs;
-      if (b < 0) b += qs;
-      v = addmod(v, (u64)b, P.q);
+  for (int h = 0; h < 2; ++h) {
+    const long long pl = p0 + h * (LIN_PT / 2) + 2 * lane;
+    if (pl >= npos) continue;
+    const int limb = (int)((pl >> log_n) % level);
+    const int comp = (int)(pl / ((long long)level << log_n));
+    const PrimeInfo P = pi[limb];
+    const long long qs = (long long)P.q;
+    const u64 two23 = (1ull << 23) % P.q;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      const int o = o0 + 4 * warp + r;
+      if (o >= n_out) break;
+      long long bq = 0;
+      if (bias && comp == 0) {
+        bq = bias[o] % qs;
+        if (bq < 0) bq += qs;
+      }
+      u64 v[2];
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        long long rl = al[r][2 * h + i] % qs;
+        if (rl < 0) rl += qs;
+        long long rh = ah[r][2 * h + i] % qs;
+        if (rh < 0) rh += qs;
+        v[i] = addmod(addmod(mulmod((u64)rh, two23, P), (u64)rl, P.q), (u64)bq, P.q);
+      }
+      *reinterpret_cast<ulonglong2*>(out + (size_t)o * npos + pl) = make_ulonglong2(v[0], v[1]);
     }
-    out[(size_t)(o0 + o) * npos + p] = v;
   }
 }
 
@@ -116,10 +226,9 @@ extern "C" int ckks_linear_plain_weights(const ckks_ctx* ctx, uint64_t* out, con
   CKKS_REQUIRE(out && in && w, "%s: NULL pointer argument", fn);
   CKKS_REQUIRE((const void*)out != (const void*)in, "%s: out must differ from in", fn);
   const long long npos = (2ll * level) << ctx->log_n;
-  dim3 grid((unsigned)((npos + LIN_THREADS - 1) / LIN_THREADS), (unsigned)((n_out + LIN_OT - 1) / LIN_OT));
+  dim3 grid((unsigned)((npos + LIN_PT - 1) / LIN_PT), (unsigned)((n_out + LIN_OT - 1) / LIN_OT));
   CKKS_REQUIRE(grid.y <= 65535, "%s: n_out too large", fn);
-  const int nb_in = (n_in + 3) / 4;
-  const int smem = LIN_OT * 4 * nb_in * (int)sizeof(int) + 4 * nb_in;
+  const int smem = (int)sizeof(LinSmem);
   if (cudaError_t e = ensure_smem(k_linear, smem))
     return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
   k_linear<<<grid, LIN_THREADS, smem, as_stream(stream)>>>(
