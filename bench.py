@@ -237,7 +237,51 @@ def measure_transforms(ctx, dev, hbm_peak: float, reps: int = 20) -> dict:
     res["poly_mul"] = {"products_per_s": npoly // 2 * nl / s, "GBps": byts / s / 1e9,
                        "frac_hbm": byts / s / 1e9 / hbm_peak}
     res["shape"] = f"N=2^{logn}, 45-bit primes, {npoly} polys x {nl} limbs per launch, 4 rotating buffers"
+    res["linear_mlp"] = measure_linear(dev, reps=reps)
     return res
+
+
+def measure_linear(dev, reps: int = 10) -> dict:
+    """Encrypted FC layer of the MLP workload (784 -> 128 at N = 2^13, L = 4,
+    50 % 4x4 block sparsity, weights at 2^20): inputs are 784 ciphertexts
+    (411 MB), one launch of ckks_linear_plain_weights per rep."""
+    import math
+    import numpy as np
+    import torch
+    from ckks_b200 import _lib
+    from ckks_b200.context import Context
+    from ckks_b200.mlp import gear_keep, make_block_sparse
+    from ckks_b200.params import CkksParams
+    P = CkksParams.standard(13, 4)
+    ctx = Context.get(13, P.primes, n_special=1)
+    rng = np.random.default_rng(5)
+    W = make_block_sparse(rng.standard_normal((128, 784)) / math.sqrt(784), 0.5, 6)
+    w = torch.from_numpy(np.round(W * 2 ** 20).astype(np.int32)).to(dev)
+    keep_np = gear_keep(W, 0.0)
+    keep = torch.from_numpy(keep_np).to(dev)
+    npos = 2 * 4 * P.n
+    x = torch.randint(0, 1 << 44, (784, npos), dtype=torch.int64, device=dev).view(torch.uint64)
+    out = torch.empty((128, npos), dtype=torch.uint64, device=dev)
+    bias = torch.zeros(128, dtype=torch.int64, device=dev)
+    st = torch.cuda.current_stream().cuda_stream
+
+    def call():
+        _lib.call("ckks_linear_plain_weights", ctx.handle, out.data_ptr(), x.data_ptr(), w.data_ptr(),
+                  bias.data_ptr(), keep.data_ptr(), 128, 784, 4, st)
+    for _ in range(3):
+        call()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        call()
+    e1.record()
+    torch.cuda.synchronize()
+    s = e0.elapsed_time(e1) / reps / 1000.0
+    macs = 128 * 784 * npos * float(keep_np.mean())
+    return {"ms": s * 1e3, "TMAC_s": macs / s / 1e12, "kept_blocks": float(keep_np.mean()),
+            "shape": "784 -> 128, N=2^13, L=4, 784 input ciphertexts (411 MB)"}
 
 
 def _lib_call_poly_mul(ctx, out, a, b, nl):

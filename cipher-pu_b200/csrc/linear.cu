@@ -59,9 +59,9 @@ __global__ void __launch_bounds__(LIN_THREADS, 2)
   extern __shared__ __align__(16) unsigned char lin_raw[];
   LinSmem& S = *reinterpret_cast<LinSmem*>(lin_raw);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int o0 = blockIdx.y * LIN_OT;
+  const int o0 = blockIdx.x * LIN_OT;  // output tiles vary fastest: they share the input tile in L2
   const long long npos = (2ll * level) << log_n;
-  const long long p0 = (long long)blockIdx.x * LIN_PT;
+  const long long p0 = (long long)blockIdx.y * LIN_PT;
   const int nb_in = (n_in + 3) / 4;
   const int rb0 = o0 / 4;
   const int nrb = (n_out + 3) / 4;
@@ -226,8 +226,8 @@ extern "C" int ckks_linear_plain_weights(const ckks_ctx* ctx, uint64_t* out, con
   CKKS_REQUIRE(out && in && w, "%s: NULL pointer argument", fn);
   CKKS_REQUIRE((const void*)out != (const void*)in, "%s: out must differ from in", fn);
   const long long npos = (2ll * level) << ctx->log_n;
-  dim3 grid((unsigned)((npos + LIN_PT - 1) / LIN_PT), (unsigned)((n_out + LIN_OT - 1) / LIN_OT));
-  CKKS_REQUIRE(grid.y <= 65535, "%s: n_out too large", fn);
+  dim3 grid((unsigned)((n_out + LIN_OT - 1) / LIN_OT), (unsigned)((npos + LIN_PT - 1) / LIN_PT));
+  CKKS_REQUIRE(grid.y <= 65535, "%s: too many positions (2 level N / %d > 65535)", fn, LIN_PT);
   const int smem = (int)sizeof(LinSmem);
   if (cudaError_t e = ensure_smem(k_linear, smem))
     return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
