@@ -125,6 +125,23 @@ def relin(e0, e1, e2, a, b, q: int):
     return addsub(e0, e2b, q, False), addsub(e1, e2a, q, True)
 
 
+def relin_masked(e0, e1, e2, a1, b1, a2, b2, q: int):
+    """First-order masked relin (rtl/m3/keyswitch_pipe_masked.sv:1-27): key
+    shares a = a1 + a2, b = b1 + b2 processed separately; equals relin(e0, e1,
+    e2, a, b, q)."""
+    ops = _ops()
+    n = len(e0)
+    if nega_friendly(q, n):
+        ctx = _ctx(_log2(n), [q])
+        d = [_dev([v % q for v in x]).reshape(1, n) for x in (e0, e1, e2, a1, b1, a2, b2)]
+        f0, f1 = ops.relin_single_masked(ctx, *d)
+        return _list(f0), _list(f1)
+    p_b1, p_b2, p_a1, p_a2 = poly_mult_many([e2] * 4, [b1, b2, a1, a2], q)
+    f0 = addsub(addsub(e0, p_b1, q, False), p_b2, q, False)
+    f1 = addsub(addsub(e1, p_a1, q, True), p_a2, q, True)
+    return f0, f1
+
+
 # ------------------------------------------------------------------ rescale
 def rescale_exact(vals, q_in: int, q_out: int) -> list[int]:
     ops = _ops()

@@ -105,6 +105,15 @@ def relin_single(ctx: Context, e0, e1, e2, ka, kb, prime: int = 0):
     return f0, f1
 
 
+def relin_single_masked(ctx: Context, e0, e1, e2, a1, b1, a2, b2, prime: int = 0):
+    """relin_single with the key as additive shares (a1 + a2, b1 + b2)."""
+    f0 = torch.empty_like(e0)
+    f1 = torch.empty_like(e1)
+    _lib.call("ckks_relin_single_masked", ctx.handle, _p(f0), _p(f1), _p(e0), _p(e1), _p(e2), _p(a1),
+              _p(b1), _p(a2), _p(b2), e0.numel() // ctx.n, prime, _stream())
+    return f0, f1
+
+
 def rescale_exact(x: torch.Tensor, q_in: int, q_out: int) -> torch.Tensor:
     out = torch.empty_like(x)
     _lib.call("ckks_rescale_exact", _p(out), _p(x), x.numel(), int(q_in), int(q_out), _stream())

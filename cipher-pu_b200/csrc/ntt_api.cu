@@ -363,3 +363,75 @@ extern "C" int ckks_relin_single(const ckks_ctx* ctx, uint64_t* f0, uint64_t* f1
     return ckks_check_launch("ckks_relin_single");
   });
 }
+
+// ------------------------------------------------------------------ masked relin
+// First-order masked single-pair relinearisation: the key (a, b) arrives as
+// two additive shares (a1, b1), (a2, b2).  Each share is transformed,
+// multiplied by NTT(e2) and brought back on its own; only the four
+// coefficient-domain products are summed, so no register or buffer ever holds
+// a1 + a2 or b1 + b2 (the two-pass schedule of rtl/m3/keyswitch_pipe_masked.sv:1-27):
+//   f0 = e2 b1 + (e0 + e2 b2),   f1 = (e1 - e2 a1) - e2 a2.
+template <int LOGN, int K>
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T)
+    k_relin_masked(u64* __restrict__ f0, u64* __restrict__ f1, const u64* __restrict__ e0,
+                   const u64* __restrict__ e1, const u64* __restrict__ e2,
+                   const u64* __restrict__ a1, const u64* __restrict__ b1,
+                   const u64* __restrict__ a2, const u64* __restrict__ b2, int prime,
+                   const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw) {
+  extern __shared__ u64 sm[];
+  using S = NttShape<LOGN, K>;
+  const size_t off = (size_t)blockIdx.x * S::N;
+  const PrimeInfo P = pi[prime];
+  const TwD* tb = twbase<LOGN>(tw, prime);
+  const int tid = threadIdx.x;
+  u64 x[S::E], y[S::E], acc[S::E];
+#pragma unroll
+  for (int e = 0; e < S::E; ++e) x[e] = reduce_any(e2[off + posC<LOGN, K>(tid, e)], P);
+  ntt_fwd<LOGN, K>(x, sm, tid, tb, P);
+#pragma unroll 1
+  for (int out = 0; out < 2; ++out) {
+#pragma unroll
+    for (int e = 0; e < S::E; ++e)
+      acc[e] = reduce_any((out == 0 ? e0 : e1)[off + posC<LOGN, K>(tid, e)], P);
+#pragma unroll 1
+    for (int share = 0; share < 2; ++share) {
+      const u64* key = out == 0 ? (share == 0 ? b1 : b2) : (share == 0 ? a1 : a2);
+      __syncthreads();
+#pragma unroll
+      for (int e = 0; e < S::E; ++e) y[e] = reduce_any(key[off + posC<LOGN, K>(tid, e)], P);
+      ntt_fwd<LOGN, K>(y, sm, tid, tb, P);
+#pragma unroll
+      for (int e = 0; e < S::E; ++e) y[e] = mulmod(x[e], y[e], P);
+      __syncthreads();
+      ntt_inv<LOGN, K>(y, sm, tid, tb, P);
+#pragma unroll
+      for (int e = 0; e < S::E; ++e) acc[e] = out == 0 ? addmod(acc[e], y[e], P.q) : submod(acc[e], y[e], P.q);
+    }
+    u64* fo = out == 0 ? f0 : f1;
+#pragma unroll
+    for (int e = 0; e < S::E; ++e) fo[off + posC<LOGN, K>(tid, e)] = acc[e];
+  }
+}
+
+extern "C" int ckks_relin_single_masked(const ckks_ctx* ctx, uint64_t* f0, uint64_t* f1,
+                                        const uint64_t* e0, const uint64_t* e1, const uint64_t* e2,
+                                        const uint64_t* a1, const uint64_t* b1, const uint64_t* a2,
+                                        const uint64_t* b2, int n_polys, int prime, void* stream) {
+  const char* fn = "ckks_relin_single_masked";
+  if (int rc = check_limbs(ctx, prime, 1, fn)) return rc;
+  CKKS_REQUIRE(ctx->has_nega[prime], "%s: prime %d has no 2N-th root", fn, prime);
+  if (n_polys <= 0) return CKKS_OK;
+  CKKS_REQUIRE(f0 && f1 && e0 && e1 && e2 && a1 && b1 && a2 && b2, "%s: NULL pointer argument", fn);
+  return dispatch_logn(ctx->log_n, [&]<int L, int K>() -> int {
+    using S = NttShape<L, K>;
+    auto kern = k_relin_masked<L, K>;
+    ensure_smem(kern, S::SMEM_WORDS * 8);
+    kern<<<grid1d(n_polys), S::T, S::SMEM_WORDS * 8, as_stream(stream)>>>(
+        reinterpret_cast<u64*>(f0), reinterpret_cast<u64*>(f1), reinterpret_cast<const u64*>(e0),
+        reinterpret_cast<const u64*>(e1), reinterpret_cast<const u64*>(e2),
+        reinterpret_cast<const u64*>(a1), reinterpret_cast<const u64*>(b1),
+        reinterpret_cast<const u64*>(a2), reinterpret_cast<const u64*>(b2), prime, ctx->d_pi,
+        ctx->d_tw);
+    return ckks_check_launch(fn);
+  });
+}

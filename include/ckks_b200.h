@@ -456,6 +456,19 @@ size_t ckks_rotate_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level);
 int ckks_rotate(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct, const uint64_t* key, int n_ct,
                 int level, uint64_t nu, void* scratch, size_t scratch_bytes, void* stream);
 
+/*
+ * First-order masked single-pair relinearisation: like ckks_relin_single with
+ * the key given as two additive shares a = a1 + a2, b = b1 + b2 (mod q), each
+ * share processed on its own and only the products combined:
+ * f0 = e0 + e2 b1 + e2 b2, f1 = e1 - e2 a1 - e2 a2 (coefficient domain, one
+ * NTT-friendly prime).  Results equal ckks_relin_single's with (a, b).
+ * Replaces rtl/m3/keyswitch_pipe_masked.sv:1-27 (two-pass arithmetic masking).
+ */
+int ckks_relin_single_masked(const ckks_ctx* ctx, uint64_t* f0, uint64_t* f1, const uint64_t* e0,
+                             const uint64_t* e1, const uint64_t* e2, const uint64_t* a1,
+                             const uint64_t* b1, const uint64_t* a2, const uint64_t* b2, int n_polys,
+                             int prime, void* stream);
+
 /* Size of the static device scratch used by ckks_ct_mul_relin_rescale_noalloc. */
 #define CKKS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 

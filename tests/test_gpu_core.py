@@ -199,3 +199,17 @@ def test_rescale_rns_vs_oracle(ck):
     x = _rand_ct(rng, (3, 2, 3, 4096), list(P.q))
     got = ops.to_host(ops.rescale_rns(ctx, ops.to_device(x)))
     assert np.array_equal(got, R.rescale(x, list(P.q)))
+
+
+@pytest.mark.parametrize("n,q", [(16, 113), (1024, 998244353), (2048, QC)])
+def test_masked_relin_equals_golden_relin(ck, n, q):
+    """rtl/m3/keyswitch_pipe_masked.sv semantics: any additive split of the key
+    gives the unmasked golden relin (scripts/verify_keyswitch.py:62)."""
+    from ckks_b200 import golden_bridge as gb
+    rng = np.random.default_rng(n + 7)
+    e0, e1, e2, a, b, a1, b1 = ([int(v) for v in rng.integers(0, q, n)] for _ in range(7))
+    a2 = [(x - y) % q for x, y in zip(a, a1)]
+    b2 = [(x - y) % q for x, y in zip(b, b1)]
+    want = G.relin(e0, e1, e2, a, b, q)
+    got = gb.relin_masked(e0, e1, e2, a1, b1, a2, b2, q)
+    assert list(got[0]) == list(want[0]) and list(got[1]) == list(want[1])
