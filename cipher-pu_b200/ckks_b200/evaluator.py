@@ -142,6 +142,76 @@ class Evaluator:
         r = ops.rotate(self.ctx, ct.data, gk, nu, scratch=self._scratch, out=out)
         return Ciphertext(r, ct.scale)
 
+    # ---------------------------------------------------------------- polynomials
+    def drop_to(self, ct: Ciphertext, level: int) -> Ciphertext:
+        """The same ciphertext modulo q_0..q_{level-1} (limbs discarded; scale kept)."""
+        if level == ct.level:
+            return ct
+        if not 1 <= level < ct.level:
+            raise ValueError(f"cannot drop level {ct.level} to {level}")
+        return Ciphertext(ct.data[:, :, :level].contiguous(), ct.scale)
+
+    def lift_scale(self, ct: Ciphertext, target: float) -> Ciphertext:
+        """Multiply by the integer floor(target / scale) when that is >= 2: the
+        scale grows toward `target` with no level spent and the relative
+        precision kept (noise and message scale together)."""
+        m = int(target // ct.scale)
+        if m < 2:
+            return ct
+        return Ciphertext(ops.ct_mul_const(self.ctx, ct.data, m), ct.scale * m)
+
+    def mul(self, a: Ciphertext, b: Ciphertext) -> Ciphertext:
+        """ct x ct with relinearisation and rescale at the lower of the two
+        levels.  Both operands are first lifted to a scale near q_{l-1} / 8
+        (messages of magnitude <= 1 keep the product below Q_l / 2 down to
+        two limbs), so repeated products do not drift to small scales where
+        the key-switching noise would dominate."""
+        lv = min(a.level, b.level)
+        tgt = self.params.q[lv - 1] / 8.0
+        a = self.lift_scale(self.drop_to(a, lv), tgt)
+        b = self.lift_scale(self.drop_to(b, lv), tgt)
+        return self.mul_relin_rescale(a, b)
+
+    def poly_eval(self, ct: Ciphertext, coeffs, out_scale: float | None = None) -> Ciphertext:
+        """sum_k coeffs[k] x^k on every slot (real coefficients, ascending).
+        Powers by a doubling tree (depth ceil(log2 d)); each term is brought
+        to the deepest level and multiplied by the integer round(c_k T / s_k),
+        so all terms share the exact scale T = out_scale q_{l-1} (lowered when
+        a term's constant would exceed 2^61); one rescale at the end returns
+        scale T / q_{l-1}.  Needs ceil(log2 d) + 2 levels, and |p(x)| T must
+        stay below the remaining modulus / 2."""
+        coeffs = [float(c) for c in coeffs]
+        d = len(coeffs) - 1
+        while d > 0 and coeffs[d] == 0.0:
+            d -= 1
+        out_scale = float(out_scale or ct.scale)
+        pw = {1: ct}
+        for k in range(2, d + 1):
+            hi = 1 << (k.bit_length() - 1)
+            pw[k] = self.mul(pw[hi // 2], pw[hi // 2]) if k == hi else self.mul(pw[hi], pw[k - hi])
+        terms = [k for k in range(1, d + 1) if coeffs[k] != 0.0]
+        lv = min([pw[k].level for k in terms] + [ct.level])
+        if lv < 2:
+            raise ValueError(f"degree {d} needs more levels than the ciphertext has ({ct.level})")
+        T = out_scale * self.params.q[lv - 1]
+        # keep every term constant below 2^61 (high powers carry small scales)
+        for k in terms:
+            T = min(T, 2.0 ** 61 * pw[k].scale / abs(coeffs[k]))
+        acc = None
+        for k in terms:
+            t = self.drop_to(pw[k], lv)
+            m = int(round(coeffs[k] * T / t.scale))
+            if abs(m) >= 1 << 62:
+                raise ValueError("term constant exceeds 62 bits: lower out_scale")
+            prod = ops.ct_mul_const(self.ctx, t.data, m)
+            acc = prod if acc is None else ops.ct_add(self.ctx, acc, prod, out=acc)
+        if acc is None:
+            acc = torch.zeros_like(self.drop_to(ct, lv).data)
+        c0 = int(round(coeffs[0] * T)) if d >= 0 else 0
+        if c0:
+            ops.ct_add_const(self.ctx, acc, c0, out=acc)
+        return self.rescale(Ciphertext(acc, T))
+
     def galois_slot_map(self, nu: int) -> tuple[np.ndarray, np.ndarray]:
         """(src, conj) over the N/2 visible slots: after psi_nu, slot k holds
         input slot src[k] (conjugated where conj[k]).  Slot k is the evaluation

@@ -162,6 +162,32 @@ def ct_mul_relin_rescale(ctx: Context, ct_a: torch.Tensor, ct_b: torch.Tensor,
     return out
 
 
+def ct_add(ctx: Context, a: torch.Tensor, b: torch.Tensor, subtract: bool = False,
+           out: torch.Tensor | None = None) -> torch.Tensor:
+    """a +- b for ciphertexts [n_ct, 2, level, N]."""
+    out = torch.empty_like(a) if out is None else out
+    n_ct, _, level, _ = a.shape
+    _lib.call("ckks_ct_add", ctx.handle, _p(out), _p(a), _p(b), n_ct, level, int(subtract), _stream())
+    return out
+
+
+def ct_mul_const(ctx: Context, a: torch.Tensor, m: int, out: torch.Tensor | None = None) -> torch.Tensor:
+    out = torch.empty_like(a) if out is None else out
+    n_ct, _, level, _ = a.shape
+    _lib.call("ckks_ct_mul_const", ctx.handle, _p(out), _p(a), n_ct, level, int(m), _stream())
+    return out
+
+
+def ct_add_const(ctx: Context, a: torch.Tensor, c: int, out: torch.Tensor | None = None) -> torch.Tensor:
+    """Adds the (arbitrary-size) integer c to every slot of ciphertexts a."""
+    import ctypes as C
+    out = torch.empty_like(a) if out is None else out
+    n_ct, _, level, _ = a.shape
+    res = (C.c_uint64 * level)(*[int(c) % int(q) for q in ctx.primes[:level]])
+    _lib.call("ckks_ct_add_const", ctx.handle, _p(out), _p(a), n_ct, level, res, _stream())
+    return out
+
+
 def automorphism(ctx: Context, x: torch.Tensor, nu: int, eval_domain: bool = False,
                  prime_begin: int = 0, n_limbs: int | None = None) -> torch.Tensor:
     """psi_nu(f)(X) = f(X^nu) mod (X^N + 1) of x [..., n_limbs, N]."""

@@ -469,6 +469,26 @@ int ckks_relin_single_masked(const ckks_ctx* ctx, uint64_t* f0, uint64_t* f1, co
                              const uint64_t* b1, const uint64_t* a2, const uint64_t* b2, int n_polys,
                              int prime, void* stream);
 
+/*
+ * Elementwise ciphertext arithmetic over ct [n_ct][2][level][N] (any domain,
+ * limbs over q_0 .. q_{level-1}): out = a + b or a - b (subtract != 0);
+ * out = m in (ct x integer constant, every limb times m mod q_i: the scale
+ * is multiplied by m); out = in + c on component 0, c given by its residues
+ * c_res[l] = c mod q_l (host array of `level` words; c may exceed 64 bits):
+ * adds c to the plaintext's every slot in the evaluation domain / to its
+ * constant coefficient in the coefficient domain.  In-place calls (out ==
+ * input) are allowed.
+ * The reference adds polynomials with scripts/verify_keyswitch.py:40
+ * poly_add / :44 poly_sub and scales by integer weights in
+ * scripts/exp_e11_ckks_e2e_real.py:102 rlwe_mul_plain.
+ */
+int ckks_ct_add(const ckks_ctx* ctx, uint64_t* out, const uint64_t* a, const uint64_t* b, int n_ct,
+                int level, int subtract, void* stream);
+int ckks_ct_mul_const(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in, int n_ct, int level,
+                      int64_t m, void* stream);
+int ckks_ct_add_const(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in, int n_ct, int level,
+                      const uint64_t* c_res, void* stream);
+
 /* Size of the static device scratch used by ckks_ct_mul_relin_rescale_noalloc. */
 #define CKKS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 

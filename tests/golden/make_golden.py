@@ -371,8 +371,33 @@ def rotation_vectors() -> int:
     return 0
 
 
+def activation_vectors() -> int:
+    """Degree-5 Chebyshev activation fits of scripts/golden_activation.py
+    (ActivationGoldenModel: _fit_piecewise_chebyshev, approximate) with one
+    segment on [-1, 1] (the form a homomorphic polynomial can evaluate) and the
+    reference's default two segments -> golden_act.json."""
+    act = load("scripts/golden_activation.py", "ref_golden_activation")
+    out = {"reference": "YI-HAIBO/cipher-pu", "generator": "tests/golden/make_golden.py --only act",
+           "source": "scripts/golden_activation.py:28 ActivationGoldenModel", "models": {}}
+    xs = np.linspace(-1, 0.999, 41)
+    for segs in (1, 2):
+        g = act.ActivationGoldenModel(poly_order=5, num_segments=segs)
+        m = {}
+        for name in ("sigmoid", "tanh", "relu"):
+            m[name] = {"segments": g.coeffs[name], "x": xs.tolist(),
+                       "approx": [float(v) for v in g.approximate(xs.copy(), name)],
+                       "exact": [float(v) for v in g.evaluate(xs.copy(), name)]}
+        out["models"][f"order5_segments{segs}"] = m
+    with open(OUT / "golden_act.json", "w") as f:
+        json.dump(out, f, indent=1)
+    print("wrote", OUT / "golden_act.json")
+    return 0
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["--only", "rot"]:
         sys.exit(rotation_vectors())
+    if sys.argv[1:] == ["--only", "act"]:
+        sys.exit(activation_vectors())
     rc = main()
-    sys.exit(rc or rotation_vectors())
+    sys.exit(rc or rotation_vectors() or activation_vectors())

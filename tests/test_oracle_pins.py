@@ -285,3 +285,15 @@ def test_galois_oracle_matches_reference_goldens():
         assert np.array_equal(got, rot[k + "_out"]), c
         seen.add(c["kind"])
     assert seen == {"automorphism_exact", "poly_mul_x_power", "automorphism_key_exact"}
+
+
+def test_activation_golden_fixture_consistent():
+    """golden_act.json (scripts/golden_activation.py run by make_golden.py):
+    with one segment, approximate(x) is the stored polynomial at x."""
+    act = json.load(open(GD / "golden_act.json"))
+    for name, m in act["models"]["order5_segments1"].items():
+        seg = m["segments"][0]
+        got = np.polyval(seg["poly_coeffs"], np.asarray(m["x"]))
+        assert np.allclose(got, m["approx"], rtol=0, atol=1e-12), name
+    sig = act["models"]["order5_segments1"]["sigmoid"]
+    assert np.abs(np.asarray(sig["approx"]) - np.asarray(sig["exact"])).max() < 1e-3
