@@ -45,6 +45,11 @@ SIGNATURES: dict[str, tuple] = {
     "ckks_ct_mul_host_workspace_bytes": (_sz, [_vp, _i32, _i32]),
     "ckks_ct_mul_relin_rescale_host": (_i32, [_vp, _vp, _vp, _vp, _u64p, _i32, _i32, _i32, _vp, _sz,
                                               _vp]),
+    "ckks_unpack48": (_i32, [_u64p, _vp, _i64, _vp]),
+    "ckks_pack48": (_i32, [_vp, _u64p, _i64, _vp]),
+    "ckks_ct_mul_host48_workspace_bytes": (_sz, [_vp, _i32, _i32]),
+    "ckks_ct_mul_relin_rescale_host48": (_i32, [_vp, _vp, _vp, _vp, _u64p, _i32, _i32, _i32, _vp, _sz,
+                                                _vp]),
     "ckks_ct_mul_relin_rescale_noalloc": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _i32, _i32, _vp]),
     "ckks_encode": (_i32, [_vp, _u64p, _vp, _i32, _i32, _i32, C.c_double, _vp]),
     "ckks_decode": (_i32, [_vp, _vp, _u64p, _i32, _i32, _i32, C.c_double, _vp]),

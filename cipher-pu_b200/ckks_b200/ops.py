@@ -246,6 +246,41 @@ def ct_mul_relin_rescale_host(ctx: Context, ct_a: torch.Tensor, ct_b: torch.Tens
     return out
 
 
+def pack48_host(x: torch.Tensor) -> torch.Tensor:
+    """uint64 residues (< 2^47, any shape, CPU) -> uint8 [6 * numel] wire format."""
+    import numpy as np
+    a = x.contiguous().view(torch.int64).numpy().view(np.uint8).reshape(-1, 8)[:, :6]
+    return torch.from_numpy(np.ascontiguousarray(a).reshape(-1))
+
+
+def unpack48_host(b: torch.Tensor, shape) -> torch.Tensor:
+    """uint8 wire format -> uint64 tensor of `shape` (CPU)."""
+    import numpy as np
+    raw = b.contiguous().numpy().reshape(-1, 6)
+    w = np.zeros((raw.shape[0], 8), dtype=np.uint8)
+    w[:, :6] = raw
+    return torch.from_numpy(w.reshape(-1).view(np.int64).copy()).view(U64).reshape(shape)
+
+
+def ct_mul_relin_rescale_host48(ctx: Context, a48: torch.Tensor, b48: torch.Tensor, key_prepared: torch.Tensor,
+                                n_ct: int, level: int, out48: torch.Tensor | None = None, chunk: int = 64,
+                                workspace: torch.Tensor | None = None) -> torch.Tensor:
+    """Host (pinned) packed ciphertexts -> host packed products (uint8 buffers)."""
+    n = ctx.n
+    out_bytes = 6 * n_ct * 2 * (level - 1) * n
+    if a48.numel() != 6 * n_ct * 2 * level * n or b48.numel() != a48.numel():
+        raise ValueError("packed inputs must hold 6 n_ct 2 level N bytes")
+    if out48 is None:
+        out48 = torch.empty(out_bytes, dtype=torch.uint8).pin_memory()
+    need = int(_lib.raw("ckks_ct_mul_host48_workspace_bytes")(ctx.handle, chunk, level))
+    if workspace is None or workspace.numel() * workspace.element_size() < need:
+        workspace = torch.empty((need + 7) // 8, dtype=U64, device=key_prepared.device)
+    _lib.call("ckks_ct_mul_relin_rescale_host48", ctx.handle, out48.data_ptr(), a48.data_ptr(),
+              b48.data_ptr(), _p(key_prepared), n_ct, level, chunk, _p(workspace),
+              workspace.numel() * workspace.element_size(), _stream())
+    return out48
+
+
 # ------------------------------------------------------------------ encode / decode
 def _f64(t: torch.Tensor) -> int:
     if not t.is_cuda or t.dtype not in (torch.float64, torch.complex128) or not t.is_contiguous():

@@ -19,6 +19,8 @@
 int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
                        const uint64_t* ct_b, const uint64_t* key, int n_ct, int level,
                        void* scratch, size_t scratch_bytes, void* stream, const char* fn);
+int ckks_launch_unpack48(uint64_t* out, const void* in, long long n, cudaStream_t st);
+int ckks_launch_pack48(void* out, const uint64_t* in, long long n, cudaStream_t st);
 
 namespace {
 
@@ -56,15 +58,20 @@ int pipe_for_device(Pipe** out, const char* fn) {
 }
 
 struct Slot {
-  size_t a_words, out_words, scratch_bytes, total_bytes;
+  size_t a_words, out_words, scratch_bytes, packed_bytes, total_bytes;
 };
 
-Slot slot_shape(const ckks_ctx* ctx, int chunk, int level) {
+size_t round256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// one stream's share of the workspace: inputs, output, ct-mult scratch and,
+// for the packed wire format, the packed staging of both inputs and the output
+Slot slot_shape(const ckks_ctx* ctx, int chunk, int level, bool packed) {
   Slot s;
   s.a_words = (size_t)chunk * 2 * level * ctx->n;
   s.out_words = (size_t)chunk * 2 * (level - 1) * ctx->n;
   s.scratch_bytes = ckks_ct_mul_scratch_bytes(ctx, chunk, level);
-  s.total_bytes = (2 * s.a_words + s.out_words) * sizeof(uint64_t) + ((s.scratch_bytes + 255) & ~(size_t)255);
+  s.packed_bytes = packed ? round256(6 * (2 * s.a_words + s.out_words)) : 0;
+  s.total_bytes = (2 * s.a_words + s.out_words) * sizeof(uint64_t) + round256(s.scratch_bytes) + s.packed_bytes;
   return s;
 }
 
@@ -72,25 +79,27 @@ Slot slot_shape(const ckks_ctx* ctx, int chunk, int level) {
 
 extern "C" size_t ckks_ct_mul_host_workspace_bytes(const ckks_ctx* ctx, int chunk, int level) {
   if (!ctx || chunk < 1 || level < 2) return 0;
-  return (size_t)kPipe * slot_shape(ctx, chunk, level).total_bytes;
+  return (size_t)kPipe * slot_shape(ctx, chunk, level, false).total_bytes;
 }
 
-extern "C" int ckks_ct_mul_relin_rescale_host(const ckks_ctx* ctx, uint64_t* out_host,
-                                              const uint64_t* a_host, const uint64_t* b_host,
-                                              const uint64_t* key, int n_ct, int level, int chunk,
-                                              void* workspace, size_t workspace_bytes,
-                                              void* stream) {
-  const char* fn = "ckks_ct_mul_relin_rescale_host";
+extern "C" size_t ckks_ct_mul_host48_workspace_bytes(const ckks_ctx* ctx, int chunk, int level) {
+  if (!ctx || chunk < 1 || level < 2) return 0;
+  return (size_t)kPipe * slot_shape(ctx, chunk, level, true).total_bytes;
+}
+
+static int host_pipeline(const ckks_ctx* ctx, void* out_host, const void* a_host, const void* b_host,
+                         const uint64_t* key, int n_ct, int level, int chunk, void* workspace,
+                         size_t workspace_bytes, void* stream, bool packed, const char* fn) {
   CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
   CKKS_REQUIRE(n_ct >= 0, "%s: n_ct < 0", fn);
   CKKS_REQUIRE(chunk >= 1, "%s: chunk=%d must be >= 1", fn, chunk);
   CKKS_REQUIRE(level >= 2 && level <= ctx->n_q, "%s: level=%d outside [2, %d]", fn, level, ctx->n_q);
   if (n_ct == 0) return CKKS_OK;
   CKKS_REQUIRE(out_host && a_host && b_host && key && workspace, "%s: NULL pointer argument", fn);
-  const Slot sl = slot_shape(ctx, chunk, level);
+  const Slot sl = slot_shape(ctx, chunk, level, packed);
   CKKS_REQUIRE(workspace_bytes >= (size_t)kPipe * sl.total_bytes,
-               "%s: workspace of %zu bytes < %zu needed (ckks_ct_mul_host_workspace_bytes)", fn,
-               workspace_bytes, (size_t)kPipe * sl.total_bytes);
+               "%s: workspace of %zu bytes < %zu needed (ckks_ct_mul_host%s_workspace_bytes)", fn,
+               workspace_bytes, (size_t)kPipe * sl.total_bytes, packed ? "48" : "");
   Pipe* p = nullptr;
   if (int rc = pipe_for_device(&p, fn)) return rc;
   // work queued earlier on the caller's stream (e.g. the key preparation)
@@ -101,6 +110,10 @@ extern "C" int ckks_ct_mul_relin_rescale_host(const ckks_ctx* ctx, uint64_t* out
 
   const size_t in_ct = (size_t)2 * level * ctx->n;         // words per input ciphertext
   const size_t out_ct = (size_t)2 * (level - 1) * ctx->n;  // words per output ciphertext
+  const size_t wb = packed ? 6 : sizeof(uint64_t);          // host bytes per word
+  const unsigned char* ah = reinterpret_cast<const unsigned char*>(a_host);
+  const unsigned char* bh = reinterpret_cast<const unsigned char*>(b_host);
+  unsigned char* oh = reinterpret_cast<unsigned char*>(out_host);
   int rc = CKKS_OK;
   for (int c0 = 0, i = 0; c0 < n_ct && rc == CKKS_OK; c0 += chunk, ++i) {
     const int m = n_ct - c0 < chunk ? n_ct - c0 : chunk;
@@ -110,18 +123,32 @@ extern "C" int ckks_ct_mul_relin_rescale_host(const ckks_ctx* ctx, uint64_t* out
     uint64_t* db = da + sl.a_words;
     uint64_t* dout = db + sl.a_words;
     void* scratch = dout + sl.out_words;
-    const size_t in_bytes = (size_t)m * in_ct * sizeof(uint64_t);
-    e = cudaMemcpyAsync(da, a_host + (size_t)c0 * in_ct, in_bytes, cudaMemcpyHostToDevice, st);
+    unsigned char* pk = reinterpret_cast<unsigned char*>(scratch) + round256(sl.scratch_bytes);
+    const size_t in_words = (size_t)m * in_ct;
+    const size_t out_words = (size_t)m * out_ct;
+    // packed staging: a at pk, b at pk + 6 a_words (16-byte aligned: a_words is a multiple of 8)
+    void* sa = packed ? (void*)pk : (void*)da;
+    void* sb = packed ? (void*)(pk + 6 * sl.a_words) : (void*)db;
+    void* so = packed ? (void*)(pk + 12 * sl.a_words) : (void*)dout;
+    e = cudaMemcpyAsync(sa, ah + (size_t)c0 * in_ct * wb, in_words * wb, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(db, b_host + (size_t)c0 * in_ct, in_bytes, cudaMemcpyHostToDevice, st);
+      e = cudaMemcpyAsync(sb, bh + (size_t)c0 * in_ct * wb, in_words * wb, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) {
       rc = ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
       break;
     }
+    if (packed) {
+      rc = ckks_launch_unpack48(da, sa, (long long)in_words, st);
+      if (rc == CKKS_OK) rc = ckks_launch_unpack48(db, sb, (long long)in_words, st);
+      if (rc != CKKS_OK) break;
+    }
     rc = ckks_ct_mul_launch(ctx, dout, da, db, key, m, level, scratch, sl.scratch_bytes, st, fn);
     if (rc != CKKS_OK) break;
-    e = cudaMemcpyAsync(out_host + (size_t)c0 * out_ct, dout, (size_t)m * out_ct * sizeof(uint64_t),
-                        cudaMemcpyDeviceToHost, st);
+    if (packed) {
+      rc = ckks_launch_pack48(so, dout, (long long)out_words, st);
+      if (rc != CKKS_OK) break;
+    }
+    e = cudaMemcpyAsync(oh + (size_t)c0 * out_ct * wb, so, out_words * wb, cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) rc = ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
   }
   for (int i = 0; i < kPipe; ++i) {
@@ -130,4 +157,21 @@ extern "C" int ckks_ct_mul_relin_rescale_host(const ckks_ctx* ctx, uint64_t* out
       rc = ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(es));
   }
   return rc;
+}
+
+extern "C" int ckks_ct_mul_relin_rescale_host(const ckks_ctx* ctx, uint64_t* out_host,
+                                              const uint64_t* a_host, const uint64_t* b_host,
+                                              const uint64_t* key, int n_ct, int level, int chunk,
+                                              void* workspace, size_t workspace_bytes,
+                                              void* stream) {
+  return host_pipeline(ctx, out_host, a_host, b_host, key, n_ct, level, chunk, workspace, workspace_bytes,
+                       stream, false, "ckks_ct_mul_relin_rescale_host");
+}
+
+extern "C" int ckks_ct_mul_relin_rescale_host48(const ckks_ctx* ctx, void* out_host, const void* a_host,
+                                                const void* b_host, const uint64_t* key, int n_ct,
+                                                int level, int chunk, void* workspace,
+                                                size_t workspace_bytes, void* stream) {
+  return host_pipeline(ctx, out_host, a_host, b_host, key, n_ct, level, chunk, workspace, workspace_bytes,
+                       stream, true, "ckks_ct_mul_relin_rescale_host48");
 }

@@ -489,6 +489,28 @@ int ckks_ct_mul_const(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in, in
 int ckks_ct_add_const(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in, int n_ct, int level,
                       const uint64_t* c_res, void* stream);
 
+/*
+ * 48-bit wire format of residues (< 2^47): each word as its 6 low bytes,
+ * little-endian, densely packed (n words <-> 6 n bytes), device to device;
+ * both buffers 16-byte aligned.  Bits above 47 are not carried.
+ */
+int ckks_unpack48(uint64_t* out, const void* in, long long n, void* stream);
+int ckks_pack48(void* out, const uint64_t* in, long long n, void* stream);
+
+/*
+ * ckks_ct_mul_relin_rescale_host with the host ciphertexts in the 48-bit wire
+ * format (6 bytes per residue, 25 % less PCIe traffic both ways): a_host,
+ * b_host hold 6 n_ct 2 level N bytes, out_host receives 6 n_ct 2 (level-1) N
+ * bytes; unpacking and packing run on the GPU inside the call.  Workspace:
+ * ckks_ct_mul_host48_workspace_bytes(ctx, chunk, level) bytes.  Replaces the
+ * host side of scripts/verify_e2e_mult.py:78 e2e_mult for packed batches
+ * (the reference moves vectors as $readmemh hex words, scripts/gen_ntt_vectors.py).
+ */
+size_t ckks_ct_mul_host48_workspace_bytes(const ckks_ctx* ctx, int chunk, int level);
+int ckks_ct_mul_relin_rescale_host48(const ckks_ctx* ctx, void* out_host, const void* a_host,
+                                     const void* b_host, const uint64_t* key, int n_ct, int level,
+                                     int chunk, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Size of the static device scratch used by ckks_ct_mul_relin_rescale_noalloc. */
 #define CKKS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 

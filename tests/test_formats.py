@@ -58,3 +58,12 @@ def test_transform_files_match_golden(cuda, tmp_path):
     write_memh(tmp_path / "a.hex", a)
     got = transform_file(cctx, tmp_path / "a.hex", tmp_path / "A.hex", prime=1)
     assert got.tolist() == ntt_dit([int(v) for v in a], om, q1)
+
+
+def test_pack48_host_round_trip():
+    import torch
+    from ckks_b200 import ops
+    x = torch.tensor([0, 1, (1 << 47) - 1, 35184371884033, 0x123456789ABC], dtype=torch.int64).view(torch.uint64)
+    b = ops.pack48_host(x)
+    assert b.numel() == 30 and b[:6].tolist() == [0] * 6 and b[6:12].tolist() == [1, 0, 0, 0, 0, 0]
+    assert torch.equal(ops.unpack48_host(b, x.shape), x)

@@ -60,3 +60,44 @@ def test_host_entry_empty_and_small_workspace(cuda):
         _lib.call("ckks_ct_mul_relin_rescale_host", ctx.handle, a.data_ptr(), a.data_ptr(),
                   a.data_ptr(), key.data_ptr(), 4, 3, 4, ws.data_ptr(), ws.numel() * 8,
                   torch.cuda.current_stream().cuda_stream)
+
+
+@pytest.mark.parametrize("n_ct,chunk", [(37, 8), (3, 64)])
+def test_host48_entry_matches_device_entry(cuda, n_ct, chunk):
+    """48-bit wire format: packed host inputs -> packed host outputs equal the
+    device entry's results."""
+    import ckks_b200.ops as ops
+    from ckks_b200.context import Context
+    from ckks_b200.params import CkksParams
+    P = CkksParams.standard(12, 3)
+    ctx = Context.get(12, P.primes, n_special=1)
+    rng = np.random.default_rng(2000 + n_ct)
+    qs = list(P.q)
+    a = _rand_ct(rng, (n_ct, 2, 3, 4096), qs)
+    b = _rand_ct(rng, (n_ct, 2, 3, 4096), qs)
+    ksk = _rand_ct(rng, (3, 2, 4, 4096), qs + [P.special])
+    key = ops.relin_key_prepare(ctx, ops.to_device(ksk))
+    dev = ops.to_host(ops.ct_mul_relin_rescale(ctx, ops.to_device(a), ops.to_device(b), key))
+    ta = torch.from_numpy(a.view(np.int64)).view(torch.uint64)
+    tb = torch.from_numpy(b.view(np.int64)).view(torch.uint64)
+    a48 = ops.pack48_host(ta).pin_memory()
+    b48 = ops.pack48_host(tb).pin_memory()
+    out48 = ops.ct_mul_relin_rescale_host48(ctx, a48, b48, key, n_ct, 3, chunk=chunk)
+    torch.cuda.synchronize()
+    got = ops.unpack48_host(out48, dev.shape).view(torch.int64).numpy().view(np.uint64)
+    assert np.array_equal(got, dev)
+
+
+def test_device_pack48_round_trip(cuda):
+    import ckks_b200.ops as ops
+    from ckks_b200 import _lib
+    rng = np.random.default_rng(9)
+    for n in (1, 8, 13, 4096 + 5):
+        x = torch.from_numpy(rng.integers(0, 1 << 47, n, dtype=np.int64)).view(torch.uint64).cuda()
+        packed = torch.empty(6 * n + 16, dtype=torch.uint8, device="cuda")
+        st = torch.cuda.current_stream().cuda_stream
+        _lib.call("ckks_pack48", packed.data_ptr(), x.data_ptr(), n, st)
+        assert torch.equal(packed[:6 * n].cpu(), ops.pack48_host(x.cpu()))
+        back = torch.empty(n + 2, dtype=torch.uint64, device="cuda")
+        _lib.call("ckks_unpack48", back.data_ptr(), packed.data_ptr(), n, st)
+        assert torch.equal(back[:n].cpu(), x.cpu())
