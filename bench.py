@@ -372,6 +372,12 @@ def run_ours(a) -> int:
     # per-kernel durations: the same steps again with the library's event
     # profiler on (its two events per launch cost ~6 % of a step, so they stay
     # out of the headline timing above)
+    # each kernel alone over the whole batch (concurrent sub-batches off), so a
+    # launch's event-measured duration is that kernel's own
+    _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 1)
+    for i in range(3):
+        step(i)
+    torch.cuda.synchronize()
     lib.ckks_profile_reset()
     lib.ckks_profile_enable(1)
     prof_steps = max(20, a.steps // 4)
@@ -379,6 +385,7 @@ def run_ours(a) -> int:
         step(i)
     torch.cuda.synchronize()
     lib.ckks_profile_enable(0)
+    _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 0)
     stages = []
     for s in range(3):
         tot = C.c_double()
@@ -447,14 +454,17 @@ def run_ours(a) -> int:
         dom = max(range(3), key=lambda s: stages[s][0])
         names = ["k_cm_tensor", "k_cm_modup", "k_cm_down"]
         per_launch_ms = stages[dom][0] / max(1, stages[dom][1])
-        alg = stage_bytes(dom, n, L) * B
+        # a call may run its batch as concurrent sub-batches: pairs per launch
+        # from the profiled launch count
+        pairs_per_launch = B * prof_steps / max(1, stages[dom][1])
+        alg = stage_bytes(dom, n, L) * pairs_per_launch
         achieved = alg / (per_launch_ms / 1000.0) / 1e9
         traffic = None
         try:
             tr = json.load(open(ROOT / "profiles" / "ncu_traffic.json"))
             rec = tr.get(names[dom])
             if rec:
-                traffic = rec["bytes_per_pair"] * B
+                traffic = rec["bytes_per_pair"] * pairs_per_launch
         except Exception:
             pass
         tot_ms = sum(s[0] for s in stages)
@@ -462,7 +472,7 @@ def run_ours(a) -> int:
         # the double-word modmul throughput measured on this GPU just now
         from ckks_b200.peak import modmul_peak
         mm_peak = modmul_peak(kind=1) / 1e12
-        mm_ach = stage_modmuls(dom, n, L) * B / (per_launch_ms / 1000.0) / 1e12
+        mm_ach = stage_modmuls(dom, n, L) * pairs_per_launch / (per_launch_ms / 1000.0) / 1e12
         transforms = measure_transforms(ctx, dev, hbm) if not a.no_transforms else None
         cpu = None
         if ws == 1 and not a.no_cpu_baseline:
@@ -479,15 +489,26 @@ def run_ours(a) -> int:
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm,
                          "unit": "GB/s", "frac": achieved / hbm, "traffic": traffic,
                          "peak_source": f"{peak_src} hbm_gbs",
-                         "algorithmic_bytes_per_launch": alg,
+                         "algorithmic_bytes_per_launch": alg, "pairs_per_launch": pairs_per_launch,
                          "avg_launch_ms": per_launch_ms},
             "roofline_fp64": {"bound": "fp64 modmul", "kernel": names[dom], "achieved": mm_ach,
                               "peak": mm_peak, "unit": "Tmodmul/s", "frac": mm_ach / mm_peak,
-                              "modmuls_per_launch": stage_modmuls(dom, n, L) * B,
+                              "modmuls_per_launch": stage_modmuls(dom, n, L) * pairs_per_launch,
                               "peak_source": "measured live: ckks_modmul_peak kind 1 (FP64 double-word)"},
             "transforms": transforms,
             "stage_ms_per_step": {names[s]: stages[s][0] / max(1, prof_steps) for s in range(3)},
-            "stage_timing": f"library event profiler over {prof_steps} identical steps right after the timed region",
+            "stage_timing": (f"library event profiler over {prof_steps} identical steps right after the timed "
+                             "region, each kernel launched alone over the whole batch (the timed region runs "
+                             "the batch as concurrent sub-batches)"),
+            "roofline_step": {
+                "fp64_achieved": sum(stage_modmuls(k, n, L) for k in range(3)) * B / (ms / a.steps / 1000.0) / 1e12,
+                "fp64_peak": mm_peak, "fp64_unit": "Tmodmul/s",
+                "fp64_frac": sum(stage_modmuls(k, n, L) for k in range(3)) * B / (ms / a.steps / 1000.0) / 1e12 / mm_peak,
+                "hbm_achieved": sum(stage_bytes(k, n, L) for k in range(3)) * B / (ms / a.steps / 1000.0) / 1e9,
+                "hbm_peak": hbm, "hbm_unit": "GB/s",
+                "hbm_frac": sum(stage_bytes(k, n, L) for k in range(3)) * B / (ms / a.steps / 1000.0) / 1e9 / hbm,
+                "basis": "whole step: all three kernels' algorithmic modmuls / bytes per pair x pairs per GPU, "
+                         "over the timed step time"},
             "stage_share": {names[s]: (stages[s][0] / tot_ms if tot_ms else None) for s in range(3)},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e48_value, "unit": UNIT,
@@ -500,7 +521,7 @@ def run_ours(a) -> int:
                         "h2d_bytes_per_step": int(ha.numel() * 8 + hb.numel() * 8),
                         "d2h_bytes_per_step": int(hout.numel() * 8),
                         "api": "ckks_ct_mul_relin_rescale_host (pinned host buffers of uint64 words)"},
-            "gpu_launches": 3 * a.steps,
+            "gpu_launches": 3 * (min(4, B // 64) if B >= 128 else 1) * a.steps,
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -98,6 +98,8 @@ class BatchExecutor:
         if bk.shape.op == "ctct":
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 0, bk.tune["k"])
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 1, bk.tune["minb"])
+            # buckets already overlap on the executor's streams: one sub-batch per call
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 1)
             for s in range(0, bk.count, chunk):
                 e = min(bk.count, s + chunk)
                 n = e - s
@@ -106,6 +108,7 @@ class BatchExecutor:
                           bk.scratch.numel() * 8, st)
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 0, 0)
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 1, 0)
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 0)
         else:
             for s in range(0, bk.count, chunk):
                 e = min(bk.count, s + chunk)

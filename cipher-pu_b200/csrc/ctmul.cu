@@ -24,8 +24,47 @@
 // Launch shape: K = log2 coefficients per thread (3: N/8 threads, radix-8
 // passes; 4: N/16 threads, radix-16) and MINB = CTAs per SM the register
 // budget is cut for (__launch_bounds__).  Both are context tuning parameters.
+#include <mutex>
+
 #include "dispatch.cuh"
 #include "profile.hpp"
+
+// Per-device streams and events for concurrent sub-batches (created on first
+// use, kept for the life of the process).  The mutex serialises the
+// fork / launch / join enqueue of calls from different host threads, which
+// share these events.
+namespace {
+constexpr int kMaxSplit = 4;
+constexpr int kSplitDevices = 128;
+struct SplitStreams {
+  bool ready = false;
+  std::mutex mu;
+  cudaStream_t s[kMaxSplit];
+  cudaEvent_t fork, join[kMaxSplit];
+};
+std::mutex g_split_init_mu;
+SplitStreams g_split[kSplitDevices];
+
+int split_streams_for_device(SplitStreams** out, const char* fn) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
+  if (dev < 0 || dev >= kSplitDevices)
+    return ckks_set_error(CKKS_EUNSUPPORTED, "%s: device %d beyond %d", fn, dev, kSplitDevices);
+  std::lock_guard<std::mutex> lock(g_split_init_mu);
+  SplitStreams& ss = g_split[dev];
+  if (!ss.ready) {
+    for (int i = 0; i < kMaxSplit && e == cudaSuccess; ++i) e = cudaStreamCreateWithFlags(&ss.s[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ss.fork, cudaEventDisableTiming);
+    for (int i = 0; i < kMaxSplit && e == cudaSuccess; ++i)
+      e = cudaEventCreateWithFlags(&ss.join[i], cudaEventDisableTiming);
+    if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
+    ss.ready = true;
+  }
+  *out = &ss;
+  return CKKS_OK;
+}
+}  // namespace
 
 struct CmScratch {
   u64* d01;   // [n_ct][2][level][N]  tensor d0, d1 (evaluation)
@@ -418,30 +457,10 @@ extern "C" size_t ckks_ct_mul_scratch_bytes(const ckks_ctx* ctx, int n_ct, int l
   return cm_words(ctx->n, n_ct, level) * sizeof(u64);
 }
 
-int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
-                       const uint64_t* ct_b, const uint64_t* key, int n_ct, int level,
-                       void* scratch, size_t scratch_bytes, void* stream, const char* fn) {
-  CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
-  CKKS_REQUIRE(ctx->n_special == 1, "%s: context needs exactly one special prime", fn);
-  CKKS_REQUIRE(level >= 2 && level <= ctx->n_q, "%s: level=%d outside [2, %d]", fn, level,
-               ctx->n_q);
-  CKKS_REQUIRE(ctx->log_n >= 6, "%s: log_n=%d below the supported minimum 6", fn, ctx->log_n);
-  CKKS_REQUIRE(n_ct >= 0, "%s: n_ct < 0", fn);
-  u64 pmin = ~0ull, pmax = 0;
-  for (int i = 0; i < ctx->n_primes; ++i) {
-    CKKS_REQUIRE(ctx->has_nega[i], "%s: prime %d has no 2N-th root", fn, i);
-    pmin = ctx->primes[i] < pmin ? ctx->primes[i] : pmin;
-    pmax = ctx->primes[i] > pmax ? ctx->primes[i] : pmax;
-  }
-  CKKS_REQUIRE(pmax < 2 * pmin && pmax < (1ull << 61) / 4,
-               "%s: primes must satisfy max < 2 min (centred basis conversion)", fn);
-  if (n_ct == 0) return CKKS_OK;
-  CKKS_REQUIRE(out && ct_a && ct_b && key && scratch, "%s: NULL pointer argument", fn);
-  const size_t need = ckks_ct_mul_scratch_bytes(ctx, n_ct, level);
-  CKKS_REQUIRE(scratch_bytes >= need, "%s: scratch of %zu bytes < %zu needed", fn, scratch_bytes,
-               need);
-  CmScratch S = cm_carve(scratch, ctx->n, n_ct, level);
-  cudaStream_t st = as_stream(stream);
+// The three ct-mult kernels for one sub-batch on one stream.
+static int cm_launch_one(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a, const uint64_t* ct_b,
+                         const uint64_t* key, int n_ct, int level, CmScratch S, cudaStream_t st,
+                         const char* fn) {
   return dispatch_cm(ctx->log_n, ctx->tune_cm_k, ctx->tune_cm_minb, [&]<int L, int K, int MINB>() -> int {
     using Sh = NttShape<L, K>;
     const int smem_a = Sh::SMEM_WORDS * 8;
@@ -473,6 +492,60 @@ int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
     }
     return ckks_check_launch(fn);
   }, fn);
+}
+
+int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
+                       const uint64_t* ct_b, const uint64_t* key, int n_ct, int level,
+                       void* scratch, size_t scratch_bytes, void* stream, const char* fn) {
+  CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
+  CKKS_REQUIRE(ctx->n_special == 1, "%s: context needs exactly one special prime", fn);
+  CKKS_REQUIRE(level >= 2 && level <= ctx->n_q, "%s: level=%d outside [2, %d]", fn, level,
+               ctx->n_q);
+  CKKS_REQUIRE(ctx->log_n >= 6, "%s: log_n=%d below the supported minimum 6", fn, ctx->log_n);
+  CKKS_REQUIRE(n_ct >= 0, "%s: n_ct < 0", fn);
+  u64 pmin = ~0ull, pmax = 0;
+  for (int i = 0; i < ctx->n_primes; ++i) {
+    CKKS_REQUIRE(ctx->has_nega[i], "%s: prime %d has no 2N-th root", fn, i);
+    pmin = ctx->primes[i] < pmin ? ctx->primes[i] : pmin;
+    pmax = ctx->primes[i] > pmax ? ctx->primes[i] : pmax;
+  }
+  CKKS_REQUIRE(pmax < 2 * pmin && pmax < (1ull << 61) / 4,
+               "%s: primes must satisfy max < 2 min (centred basis conversion)", fn);
+  if (n_ct == 0) return CKKS_OK;
+  CKKS_REQUIRE(out && ct_a && ct_b && key && scratch, "%s: NULL pointer argument", fn);
+  const size_t need = ckks_ct_mul_scratch_bytes(ctx, n_ct, level);
+  CKKS_REQUIRE(scratch_bytes >= need, "%s: scratch of %zu bytes < %zu needed", fn, scratch_bytes,
+               need);
+  // default: one sub-batch per 64 pairs, at most 4, from 128 pairs on
+  const int split_req = ctx->tune_cm_split ? ctx->tune_cm_split : (n_ct >= 128 ? (n_ct / 64 < 4 ? n_ct / 64 : 4) : 1);
+  const int split = split_req < n_ct ? split_req : n_ct;
+  cudaStream_t st = as_stream(stream);
+  if (split <= 1) return cm_launch_one(ctx, out, ct_a, ct_b, key, n_ct, level, cm_carve(scratch, ctx->n, n_ct, level), st, fn);
+  // Concurrent sub-batches: the kernels of one sub-batch fill the partial last
+  // waves of another's and overlap the HBM-bound tensor product with the
+  // compute-bound ModUp / ModDown.  Fork / join through events keeps the
+  // caller's stream order (stream capture records them as graph edges).
+  SplitStreams* ss = nullptr;
+  if (int rc = split_streams_for_device(&ss, fn)) return rc;
+  std::lock_guard<std::mutex> lock(ss->mu);
+  cudaError_t e = cudaEventRecord(ss->fork, st);
+  const size_t in_ct = (size_t)2 * level * ctx->n, out_ct = (size_t)2 * (level - 1) * ctx->n;
+  unsigned char* sbase = reinterpret_cast<unsigned char*>(scratch);
+  int rc = CKKS_OK;
+  for (int h = 0; h < split && e == cudaSuccess && rc == CKKS_OK; ++h) {
+    const int c0 = (int)((long long)n_ct * h / split), c1 = (int)((long long)n_ct * (h + 1) / split);
+    const int m = c1 - c0;
+    e = cudaStreamWaitEvent(ss->s[h], ss->fork, 0);
+    if (e != cudaSuccess) break;
+    rc = cm_launch_one(ctx, out + (size_t)c0 * out_ct, ct_a + (size_t)c0 * in_ct, ct_b + (size_t)c0 * in_ct, key,
+                       m, level, cm_carve(sbase, ctx->n, m, level), ss->s[h], fn);
+    sbase += cm_words(ctx->n, m, level) * sizeof(u64);
+    if (rc == CKKS_OK) e = cudaEventRecord(ss->join[h], ss->s[h]);
+    if (rc == CKKS_OK && e == cudaSuccess) e = cudaStreamWaitEvent(st, ss->join[h], 0);
+  }
+  if (rc != CKKS_OK) return rc;
+  if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
+  return CKKS_OK;
 }
 
 extern "C" int ckks_ct_mul_relin_rescale(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,

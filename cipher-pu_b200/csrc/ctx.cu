@@ -280,6 +280,11 @@ extern "C" int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value) {
                    "ckks_ctx_set_tuning: ct-mult register budget must be 0, 1 (balanced) or 2 (tight)");
       ctx->tune_cm_minb = value;
       return CKKS_OK;
+    case CKKS_TUNE_CM_SPLIT:
+      CKKS_REQUIRE(value >= 0 && value <= 4,
+                   "ckks_ctx_set_tuning: ct-mult concurrent sub-batches must be in [0, 4]");
+      ctx->tune_cm_split = value;
+      return CKKS_OK;
     default:
       return ckks_set_error(CKKS_EINVAL, "ckks_ctx_set_tuning: unknown parameter %d", param);
   }

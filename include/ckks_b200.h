@@ -71,10 +71,14 @@ int ckks_ctx_destroy(ckks_ctx* ctx);
  *   CKKS_TUNE_CM_MIN_BLOCKS: register budget of the ct-mult kernels:
  *   1 = balanced (128 registers per thread, max(1, 512 / threads) CTAs per
  *   SM), 2 = tight (64 registers, twice the CTAs); 0 = default (balanced).
+ *   CKKS_TUNE_CM_SPLIT: sub-batches of one ct-mult call run concurrently on
+ *   internal streams (1..4; 0 = default: one per 64 pairs, at most 4, from
+ *   128 pairs on, else 1).  The kernels of one sub-batch fill the partial
+ *   last waves of the others (measured +12 % at 256 pairs, N = 2^12, L = 3).
  * The reference fixes its datapath shape at synthesis time
  * (rtl/m1/ntt_unit.sv:39-52 parameters).
  */
-enum { CKKS_TUNE_CM_LOG_ELEMS = 0, CKKS_TUNE_CM_MIN_BLOCKS = 1 };
+enum { CKKS_TUNE_CM_LOG_ELEMS = 0, CKKS_TUNE_CM_MIN_BLOCKS = 1, CKKS_TUNE_CM_SPLIT = 2 };
 int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value);
 
 /*
