@@ -47,7 +47,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-transforms", action="store_true",
                     help="skip the standalone NTT / poly-mult measurement")
-    ap.add_argument("--e2e-chunk", type=int, default=64,
+    ap.add_argument("--e2e-chunk", type=int, default=48,
                     help="pairs per pipelined chunk of the host-buffer call")
     return ap.parse_args()
 
