@@ -105,7 +105,9 @@ struct CmBlocks {
 };
 
 // ct-mult kernels are instantiated for log N in [6, 14] with K in {3, 4}
-// (K = 3 needs N / 8 <= 1024 threads) and both register budgets.  Defaults:
+// (K = 3 needs N / 8 <= 1024 threads) and both register budgets; N = 2^14
+// needs more shared memory per CTA than B200 offers (the launch paths check
+// and refuse it with a message).  Defaults:
 // K = 4 for log N >= 10 (3 below), balanced budget: measured fastest at
 // N = 2^12 (2 CTAs of 256 threads per SM) and 2^13 (1 CTA of 512).
 // f is called as f.template operator()<L, K, MINB>().
@@ -465,6 +467,7 @@ static int cm_launch_one(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_
     using Sh = NttShape<L, K>;
     const int smem_a = Sh::SMEM_WORDS * 8;
     const int smem_bc = (Sh::SMEM_WORDS + 2 * Sh::N) * 8;
+    if (int rc = require_smem(smem_bc, L, fn)) return rc;
     auto ka = k_cm_tensor<L, K, MINB>;
     auto kb = k_cm_modup<L, K, MINB>;
     auto kc = k_cm_down<L, K, MINB>;
@@ -590,6 +593,7 @@ extern "C" int ckks_rotate(const ckks_ctx* ctx, uint64_t* out, const uint64_t* c
     const int smem_a = Sh::SMEM_WORDS * 8;
     const int smem_b = (Sh::SMEM_WORDS + 2 * Sh::N) * 8;
     const int smem_c = (Sh::SMEM_WORDS + Sh::N) * 8;
+    if (int rc = require_smem(smem_b, L, fn)) return rc;
     auto ka = k_rot_prep<L, K, MINB>;
     auto kb = k_cm_modup<L, K, MINB>;
     auto kc = k_ks_down<L, K, MINB>;

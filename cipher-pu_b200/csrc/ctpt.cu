@@ -75,6 +75,7 @@ extern "C" int ckks_ct_mul_plain_rescale(const ckks_ctx* ctx, uint64_t* out, con
   return dispatch_logn(ctx->log_n, [&]<int L, int K>() -> int {
     using Sh = NttShape<L, K>;
     const int smem = (Sh::SMEM_WORDS + Sh::N) * 8;
+    if (int rc = require_smem(smem, L, fn)) return rc;
     ensure_smem(k_ctpt_rescale<L, K>, smem);
     ProfSpan span(CKKS_STAGE_OTHER, st);
     k_ctpt_rescale<L, K><<<grid1d(2ll * n_ct), Sh::T, smem, st>>>(

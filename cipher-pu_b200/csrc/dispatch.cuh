@@ -45,3 +45,21 @@ static cudaError_t ensure_smem(KernelT kernel, int bytes) {
 }
 
 static inline unsigned grid1d(long long blocks) { return (unsigned)blocks; }
+
+// Largest dynamic shared memory a CTA may opt into on the current device.
+static inline int smem_optin_limit() {
+  int dev = 0, v = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) return 0;
+  return v;
+}
+
+// Error unless `bytes` of dynamic shared memory per CTA fit on this device.
+static inline int require_smem(int bytes, int log_n, const char* fn) {
+  const int lim = smem_optin_limit();
+  if (bytes > lim)
+    return ckks_set_error(CKKS_EUNSUPPORTED,
+                          "%s: N=2^%d needs %d KB of shared memory per CTA, above the device's %d KB",
+                          fn, log_n, bytes / 1024, lim / 1024);
+  return CKKS_OK;
+}

@@ -213,3 +213,46 @@ def test_masked_relin_equals_golden_relin(ck, n, q):
     want = G.relin(e0, e1, e2, a, b, q)
     got = gb.relin_masked(e0, e1, e2, a1, b1, a2, b2, q)
     assert list(got[0]) == list(want[0]) and list(got[1]) == list(want[1])
+
+
+def test_ct_mul_concurrent_sub_batches_identical(ck):
+    """A 256-pair call split into 1, 2, 3 or 4 concurrent sub-batches (internal
+    streams joined by events) gives identical results; pairs from every
+    sub-batch match the oracle."""
+    ops, Context = ck
+    import torch
+    from ckks_b200 import _lib
+    from ckks_b200.params import CkksParams
+    P = CkksParams.standard(12, 3)
+    ctx = Context.get(12, P.primes, n_special=1)
+    qs = list(P.q)
+    rng = np.random.default_rng(77)
+    a = _rand_ct(rng, (256, 2, 3, 4096), qs)
+    b = _rand_ct(rng, (256, 2, 3, 4096), qs)
+    ksk = _rand_ct(rng, (3, 2, 4, 4096), qs + [P.special])
+    key = ops.relin_key_prepare(ctx, ops.to_device(ksk))
+    da, db = ops.to_device(a), ops.to_device(b)
+    outs = []
+    try:
+        for split in (1, 2, 3, 4, 0):
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, split)
+            outs.append(ops.to_host(ops.ct_mul_relin_rescale(ctx, da, db, key)))
+    finally:
+        _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 0)
+    assert all(np.array_equal(o, outs[0]) for o in outs[1:])
+    idx = [0, 85, 170, 255]
+    assert np.array_equal(outs[0][idx], R.ct_mul_relin_rescale(a[idx], b[idx], ksk, qs, P.special))
+
+
+def test_ct_mul_n16384_rejected_with_a_message(ck):
+    """At N = 2^14 the ModUp / ModDown CTAs would need ~400 KB of shared
+    memory: the call returns an error naming the limit instead of launching."""
+    ops, Context = ck
+    from ckks_b200 import _lib
+    from ckks_b200.params import CkksParams
+    P = CkksParams.standard(14, 3)
+    ctx = Context.get(14, P.primes, n_special=1)
+    a = ops.to_device(np.zeros((1, 2, 3, 1 << 14), dtype=np.uint64))
+    key = ops.to_device(np.zeros((3, 2, 4, 1 << 14, 2), dtype=np.uint64))
+    with pytest.raises(_lib.CkksError, match="shared memory"):
+        ops.ct_mul_relin_rescale(ctx, a, a, key)
