@@ -10,6 +10,12 @@ batches rotate between steps (400 MB > the 126 MB L2).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+The line also carries the second half of the metric, `enc_mlp`: encrypted
+MLP 784-128-10 samples/s under the plain SNR-monitor gear controller and the
+learned one (same inputs, equal SNR), plus standalone NTT / product / linear
+layer throughput (`transforms`), the end-to-end host-buffer rate (`e2e`) and
+the CPU restatement (`cpu_baseline`).
+
 Under torchrun each rank processes its own 256 pairs (weak scaling, no
 data-path collective); the step time is the max over ranks.
 `--impl reference` times the CPU restatement of the same path on all host
@@ -47,6 +53,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-transforms", action="store_true",
                     help="skip the standalone NTT / poly-mult measurement")
+    ap.add_argument("--no-enc-mlp", action="store_true",
+                    help="skip the encrypted-MLP learned-vs-plain gear leg")
+    ap.add_argument("--enc-mlp-batches", type=int, default=8)
     ap.add_argument("--e2e-chunk", type=int, default=48,
                     help="pairs per pipelined chunk of the host-buffer call")
     return ap.parse_args()
@@ -474,6 +483,21 @@ def run_ours(a) -> int:
         mm_peak = modmul_peak(kind=1) / 1e12
         mm_ach = stage_modmuls(dom, n, L) * pairs_per_launch / (per_launch_ms / 1000.0) / 1e12
         transforms = measure_transforms(ctx, dev, hbm) if not a.no_transforms else None
+        enc_mlp = None
+        if not a.no_enc_mlp and ws == 1:
+            # second half of the metric: encrypted MLP 784-128-10 (N=2^13, L=4,
+            # batch 1024, DARE between layers) under the plain SNR-monitor
+            # gear controller and the learned one, same inputs
+            from ckks_b200.train_gear import compare
+            r = compare(model="mlp", batches=a.enc_mlp_batches)
+            enc_mlp = {"metric": "enc-MLP samples/s learned vs plain gear", "unit": "samples/s",
+                       "plain": r["plain"]["samples_per_s"], "learned": r["learned"]["samples_per_s"],
+                       "speedup": r["speedup"], "snr_db_plain": r["plain"]["snr_db"],
+                       "snr_db_learned": r["learned"]["snr_db"],
+                       "top1_plain": r["plain"]["top1_agreement"], "top1_learned": r["learned"]["top1_agreement"],
+                       "probes_plain": r["plain"]["probes"], "probes_learned": r["learned"]["probes"],
+                       "workload": f"784-128-10, N=2^13, L=4, {r['batches']} batches of {r['batch']} samples, "
+                                   f"target {r['target_db']} dB, synthetic uniform [0,1] inputs, random weights"}
         cpu = None
         if ws == 1 and not a.no_cpu_baseline:
             from oracle import cpu_baseline
@@ -496,6 +520,7 @@ def run_ours(a) -> int:
                               "modmuls_per_launch": stage_modmuls(dom, n, L) * pairs_per_launch,
                               "peak_source": "measured live: ckks_modmul_peak kind 1 (FP64 double-word)"},
             "transforms": transforms,
+            "enc_mlp": enc_mlp,
             "stage_ms_per_step": {names[s]: stages[s][0] / max(1, prof_steps) for s in range(3)},
             "stage_timing": (f"library event profiler over {prof_steps} identical steps right after the timed "
                              "region, each kernel launched alone over the whole batch (the timed region runs "
