@@ -138,6 +138,11 @@ __device__ __forceinline__ ulonglong2 ld_stream2(const void* p) {
   asm("ld.global.nc.L1::no_allocate.v2.u64 {%0, %1}, [%2];" : "=l"(v.x), "=l"(v.y) : "l"(p));
   return v;
 }
+__device__ __forceinline__ double ld_stream_d(const double* p) {
+  double v;
+  asm("ld.global.nc.L1::no_allocate.f64 %0, [%1];" : "=d"(v) : "l"(p));
+  return v;
+}
 __device__ __forceinline__ double2 ld_stream2d(const void* p) {
   double2 v;
   asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(v.x), "=d"(v.y) : "l"(p));

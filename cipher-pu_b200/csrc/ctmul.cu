@@ -204,7 +204,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 // thread-private shared-memory slots (index e * T + tid).
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
-    k_cm_modup(CmScratch S, const double2* __restrict__ key, int level, int nq,
+    k_cm_modup(CmScratch S, const double* __restrict__ key, int level, int nq,
                const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
@@ -240,18 +240,27 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
       ntt_fwd_d<LOGN, K>(x, sm, tid, tb, P);
       z_to_c<LOGN, K>(x, sm, tid);
     }
-    // key inner product in exact FP64: key words are (w, w / q) pairs; each
-    // product is within 0.75 q, the sum of `level` of them stays far below 2^51
+    // key inner product in exact FP64 on the key values alone (8 bytes per
+    // word): w / q is formed as w * (1/q), two roundings off, so the quotient
+    // estimate may miss by one and each product lands within 1.5 q (still
+    // exact: every intermediate is an integer below 2^53); the running sum is
+    // folded back below q / 2 + 1 every 16 digits so it stays exact
 #pragma unroll 1
     for (int kk = 0; kk < 2; ++kk) {
-      const double2* kp = key + (((size_t)j * 2 + kk) * (nq + 1) + pidx) * N;
+      const double* kp = reinterpret_cast<const double*>(key) + (((size_t)j * 2 + kk) * (nq + 1) + pidx) * (2 * N);
       double* acc = kk ? acc1s_d : acc0s_d;
+      const bool fold = (j & 15) == 15;
 #pragma unroll
       for (int e = 0; e < Sh::E; ++e) {
-        const double2 w = ld_stream2d(kp + posC<LOGN, K>(tid, e));
+        const double w = ld_stream_d(kp + posC<LOGN, K>(tid, e));
         const int s = e * T + tid;
-        const double t = fmulmod(x[e], w.x, w.y, P.qd);
-        acc[s] = j == 0 ? t : __dadd_rn(acc[s], t);
+        const double t = fmulmod(x[e], w, __dmul_rn(w, P.qinv_d), P.qd);
+        double a = j == 0 ? t : __dadd_rn(acc[s], t);
+        if (fold) {
+          const double qt = __dadd_rn(__fma_rn(a, P.qinv_d, CKKS_FP_MAGIC), -CKKS_FP_MAGIC);
+          a = __fma_rn(-qt, P.qd, a);
+        }
+        acc[s] = a;
       }
     }
   }
@@ -432,15 +441,20 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 }
 
 // ---------------------------------------------------------------- key prep
-__global__ void k_key_prepare(double2* __restrict__ out, const u64* __restrict__ in,
+// Prepared key: per (digit, poly, limb) a block of 2N doubles, the N values w
+// followed by their N quotients w / q (the ModUp kernel streams only the
+// values and forms w / q itself; the quotients serve callers that want both).
+__global__ void k_key_prepare(double* __restrict__ out, const u64* __restrict__ in,
                               long long total, int log_n, int nlimb,
                               const PrimeInfo* __restrict__ pi) {
   const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= total) return;
-  const int limb = (int)((idx >> log_n) % nlimb);
-  const PrimeInfo P = pi[limb];
+  const long long blk = idx >> log_n;
+  const long long i = idx & ((1ll << log_n) - 1);
+  const PrimeInfo P = pi[(int)(blk % nlimb)];
   const double w = u2d(in[idx] % P.q);
-  out[idx] = make_double2(w, __ddiv_rn(w, P.qd));  // (w, w / q), the FP64 product's operands
+  out[(blk << (log_n + 1)) + i] = w;
+  out[(blk << (log_n + 1)) + (1ll << log_n) + i] = __ddiv_rn(w, P.qd);
 }
 
 extern "C" int ckks_relin_key_prepare(const ckks_ctx* ctx, uint64_t* prepared,
@@ -449,7 +463,7 @@ extern "C" int ckks_relin_key_prepare(const ckks_ctx* ctx, uint64_t* prepared,
   CKKS_REQUIRE(ctx->n_special == 1, "ckks_relin_key_prepare: context needs one special prime");
   const long long total = (long long)ctx->n_q * 2 * ctx->n_primes * ctx->n;
   k_key_prepare<<<grid1d((total + 255) / 256), 256, 0, as_stream(stream)>>>(
-      reinterpret_cast<double2*>(prepared), reinterpret_cast<const u64*>(ksk), total,
+      reinterpret_cast<double*>(prepared), reinterpret_cast<const u64*>(ksk), total,
       ctx->log_n, ctx->n_primes, ctx->d_pi);
   return ckks_check_launch("ckks_relin_key_prepare");
 }
@@ -484,7 +498,7 @@ static int cm_launch_one(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_
     {
       ProfSpan span(CKKS_STAGE_CM_MODUP, st);
       kb<<<grid1d((long long)n_ct * (level + 1)), Sh::T, smem_bc, st>>>(
-          S, reinterpret_cast<const double2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
+          S, reinterpret_cast<const double*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {
@@ -609,7 +623,7 @@ extern "C" int ckks_rotate(const ckks_ctx* ctx, uint64_t* out, const uint64_t* c
     {
       ProfSpan span(CKKS_STAGE_CM_MODUP, st);
       kb<<<grid1d((long long)n_ct * (level + 1)), Sh::T, smem_b, st>>>(
-          S, reinterpret_cast<const double2*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
+          S, reinterpret_cast<const double*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {

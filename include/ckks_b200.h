@@ -169,9 +169,10 @@ int ckks_rescale_rns(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in, int
 /*
  * Relinearisation key preparation: ksk [dnum = n_q][2][n_q + 1][N]
  * (evaluation domain, digit j, component k (0: b, 1: a), limb over
- * q_0..q_{n_q-1}, special) -> prepared [dnum][2][n_q + 1][N] pairs of
- * doubles (w, w / q) (exact value and its correctly rounded quotient, the
- * operands of the FP64 modular product), i.e. 2x the words.  Context must have one special
+ * q_0..q_{n_q-1}, special) -> prepared [dnum][2][n_q + 1] blocks of 2N
+ * doubles: the N key values w (exact) followed by their N correctly rounded
+ * quotients w / q (the operands of the FP64 modular product), i.e. 2x the
+ * words.  Context must have one special
  * prime.  Key generation itself is host-side (no reference counterpart:
  * the reference keyswitch key is one (a, b) pair, scripts/verify_keyswitch.py:151).
  */

@@ -179,11 +179,11 @@ def test_ct_mul_relin_rescale_vs_oracle(ck, log_n, levels, level, n_ct):
     a[0, 0, 0, :4] = [0, qs[0] - 1, 1, qs[0] - 2]
     ksk = _rand_ct(rng, (levels, 2, levels + 1, n), list(P.q) + [P.special])
     key = ops.relin_key_prepare(ctx, ops.to_device(ksk))
-    # the prepared key holds (value, value / q) pairs of doubles
-    kp = ops.to_host(key).view(np.float64)
-    assert np.array_equal(kp[..., 0], ksk.astype(np.float64))
+    # the prepared key holds, per limb, the N values then their N quotients w / q (doubles)
+    kp = ops.to_host(key).view(np.float64).reshape(levels, 2, levels + 1, 2, n)
+    assert np.array_equal(kp[:, :, :, 0], ksk.astype(np.float64))
     qq = np.array(list(P.q) + [P.special], dtype=np.float64)
-    assert np.array_equal(kp[..., 1], ksk.astype(np.float64) / qq[None, None, :, None])
+    assert np.array_equal(kp[:, :, :, 1], ksk.astype(np.float64) / qq[None, None, :, None])
     got = ops.to_host(ops.ct_mul_relin_rescale(ctx, ops.to_device(a), ops.to_device(b), key))
     sub_ksk = ksk[:level][:, :, list(range(level)) + [levels]]
     exp = R.ct_mul_relin_rescale(a, b, sub_ksk, qs, P.special)
