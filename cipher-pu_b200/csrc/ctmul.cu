@@ -315,17 +315,19 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     x[e] = x[e] > PP.half ? x[e] - PP.q + PT.q : x[e];
   }
   ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, t), PT);
+  z_to_c<LOGN, K>(x, sm, tid);
   {
     const TwPair pt = pinv[t];
     u64 dv[Sh::E], av[Sh::E];
-    load_z<LOGN, K>(dv, dk + (size_t)t * N, tid);
-    load_z<LOGN, K>(av, ak + (size_t)t * N, tid);
+    load_c<LOGN, K>(dv, dk + (size_t)t * N, tid);
+    load_c<LOGN, K>(av, ak + (size_t)t * N, tid);
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) {
       const u64 ks = shoup(av[e] + PT.qlazy - x[e], pt.w, pt.ws, PT.q);
       x[e] = addmod(dv[e], ks, PT.q);
     }
   }
+  c_to_z<LOGN, K>(x, sm, tid);
   ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, t), PT);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) ws[e * T + tid] = x[e];

@@ -28,10 +28,11 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   u64* o = out + (c * 2 + k) * (size_t)t * N;
   const PrimeInfo PT = pi[t];
   u64 x[Sh::E], y[Sh::E];
-  load_z<LOGN, K>(x, a + (size_t)t * N, tid);
-  load_z<LOGN, K>(y, p + (size_t)t * N, tid);
+  load_c<LOGN, K>(x, a + (size_t)t * N, tid);
+  load_c<LOGN, K>(y, p + (size_t)t * N, tid);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) x[e] = mulmod(x[e], y[e], PT);
+  c_to_z<LOGN, K>(x, sm, tid);
   ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, t), PT);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) ws[e * T + tid] = x[e];
@@ -45,15 +46,16 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
       x[e] = w > PT.half ? w - PT.q + P.q : w;
     }
     ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
-    load_z<LOGN, K>(y, a + (size_t)i * N, tid);
+    z_to_c<LOGN, K>(x, sm, tid);
+    load_c<LOGN, K>(y, a + (size_t)i * N, tid);
     u64 pv[Sh::E];
-    load_z<LOGN, K>(pv, p + (size_t)i * N, tid);
+    load_c<LOGN, K>(pv, p + (size_t)i * N, tid);
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) {
       const u64 xi = mulmod(y[e], pv[e], P);
       x[e] = shoup(xi + P.qlazy - x[e], ci.w, ci.ws, P.q);
     }
-    store_z<LOGN, K>(x, o + (size_t)i * N, tid);
+    store_c<LOGN, K>(x, o + (size_t)i * N, tid);
   }
 }
 

@@ -249,11 +249,12 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   const size_t LN = (size_t)level * N;
   const u64* c0 = ct + c * 2 * LN + (size_t)i * N;
   u64 x[Sh::E], y[Sh::E], s[Sh::E];
-  load_z<LOGN, K>(x, c0, tid);
-  load_z<LOGN, K>(y, c0 + LN, tid);
-  load_z<LOGN, K>(s, s_eval + (size_t)i * N, tid);
+  load_c<LOGN, K>(x, c0, tid);
+  load_c<LOGN, K>(y, c0 + LN, tid);
+  load_c<LOGN, K>(s, s_eval + (size_t)i * N, tid);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) x[e] = addmod(x[e], mulmod(y[e], s[e], P), P.q);
+  c_to_z<LOGN, K>(x, sm, tid);
   ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
   store_c<LOGN, K>(x, out + c * LN + (size_t)i * N, tid);
 }
@@ -303,20 +304,21 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     x[e] = (u64)(v < 0 ? v + (long long)P.q : v);
   }
   ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
+  z_to_c<LOGN, K>(x, sm, tid);
   u64 av[Sh::E], sv[Sh::E];
-  load_z<LOGN, K>(av, a + c * LN + (size_t)i * N, tid);
-  load_z<LOGN, K>(sv, s_eval + (size_t)i * N, tid);
+  load_c<LOGN, K>(av, a + c * LN + (size_t)i * N, tid);
+  load_c<LOGN, K>(sv, s_eval + (size_t)i * N, tid);
   if (m_eval) {
     u64 mv[Sh::E];
-    load_z<LOGN, K>(mv, m_eval + c * LN + (size_t)i * N, tid);
+    load_c<LOGN, K>(mv, m_eval + c * LN + (size_t)i * N, tid);
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) x[e] = addmod(x[e], mv[e], P.q);
   }
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) x[e] = submod(x[e], mulmod(av[e], sv[e], P), P.q);
   u64* o0 = out + c * 2 * LN + (size_t)i * N;
-  store_z<LOGN, K>(x, o0, tid);
-  store_z<LOGN, K>(av, o0 + LN, tid);
+  store_c<LOGN, K>(x, o0, tid);
+  store_c<LOGN, K>(av, o0 + LN, tid);
 }
 
 extern "C" int ckks_encrypt(const ckks_ctx* ctx, uint64_t* out, const uint64_t* m_eval,
@@ -420,15 +422,16 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
     x[e] = res;
   }
   ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, j), P);
+  z_to_c<LOGN, K>(x, sm, tid);
   const size_t LN = (size_t)level_out * N;
   u64 av[Sh::E], sv[Sh::E];
-  load_z<LOGN, K>(av, a + c * LN + (size_t)j * N, tid);
-  load_z<LOGN, K>(sv, s_eval + (size_t)j * N, tid);
+  load_c<LOGN, K>(av, a + c * LN + (size_t)j * N, tid);
+  load_c<LOGN, K>(sv, s_eval + (size_t)j * N, tid);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) x[e] = submod(x[e], mulmod(av[e], sv[e], P), P.q);
   u64* o0 = out + c * 2 * LN + (size_t)j * N;
-  store_z<LOGN, K>(x, o0, tid);
-  store_z<LOGN, K>(av, o0 + LN, tid);
+  store_c<LOGN, K>(x, o0, tid);
+  store_c<LOGN, K>(av, o0 + LN, tid);
 }
 
 extern "C" size_t ckks_dare_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level_in) {
