@@ -7,7 +7,7 @@ is one batched launch sequence of the library's kernels (one CTA per
 polynomial limb, so the buckets of different shapes need no padding).  The
 buckets are spread over a pool of streams and the whole plan is captured
 once into a CUDA graph, so a step costs one graph launch.  The autotuner
-times every bucket alone under each launch shape (per-thread radix 2^K,
+times every bucket alone under each launch shape (per-thread radix 2^K, K = 2..5,
 balanced or tight register budget, chunking of the bucket into
 launches) and keeps the fastest; the choice is baked into the graph at
 capture time.
@@ -60,6 +60,23 @@ class Bucket:
     tune: dict = field(default_factory=lambda: {"k": 0, "minb": 0, "chunk": 0})
 
 
+# Per-thread radix 2^K the autotuner sweeps (K = log2 coefficients per thread).
+RADIX_LOG2 = (2, 3, 4, 5)
+
+
+def cm_shape_built(log_n: int, k: int, minb: int) -> bool:
+    """Whether the library builds the ct-mult kernels for (log N, K, budget):
+    K = 3, 4 for log N in [6, 14] (at most 1024 threads), K = 2 for log N in
+    [10, 12], K = 5 for log N in [10, 14] with the balanced budget only."""
+    if not 6 <= log_n <= 14 or ((1 << log_n) >> k) > 1024:
+        return False
+    if k == 2:
+        return 10 <= log_n <= 12
+    if k == 5:
+        return log_n >= 10 and minb == 1
+    return k in (3, 4)
+
+
 class BatchExecutor:
     def __init__(self, items: list, max_level: int = 8, seed: int = 0, n_streams: int = 4, device=None):
         self.device = device or torch.device("cuda", torch.cuda.current_device())
@@ -110,10 +127,12 @@ class BatchExecutor:
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 1, 0)
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 0)
         else:
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 3, bk.tune["k"])
             for s in range(0, bk.count, chunk):
                 e = min(bk.count, s + chunk)
                 _lib.call("ckks_ct_mul_plain_rescale", ctx.handle, bk.out[s:e].data_ptr(), bk.a[s:e].data_ptr(),
                           bk.b[s:e].data_ptr(), 1, e - s, lvl, st)
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 3, 0)
 
     def run_eager(self):
         cur = torch.cuda.current_stream()
@@ -164,13 +183,15 @@ class BatchExecutor:
         """Time each bucket alone under every launch shape; keep the fastest."""
         choices = {}
         for bk in self.buckets:
-            cands = [{"k": 0, "minb": 0, "chunk": 0}]
+            log_n = bk.shape.log_n
             if bk.shape.op == "ctct":
                 cands = [{"k": k, "minb": mb, "chunk": ch}
-                         for k, mb, ch in itertools.product((3, 4), (1, 2), (0, 128))
-                         if ((1 << bk.shape.log_n) >> k) <= 1024
-                         and not (ch and ch >= bk.count)]
+                         for k, mb, ch in itertools.product(RADIX_LOG2, (1, 2), (0, 128))
+                         if cm_shape_built(log_n, k, mb) and not (ch and ch >= bk.count)]
+            else:
+                cands = [{"k": k, "minb": 0, "chunk": 0} for k in RADIX_LOG2 if ((1 << log_n) >> k) <= 1024]
             best = None
+            sweep = {}
             for c in cands:
                 bk.tune = c
                 self.launch(bk)
@@ -183,11 +204,13 @@ class BatchExecutor:
                 e1.record()
                 torch.cuda.synchronize()
                 t = e0.elapsed_time(e1) / reps
+                sweep[f"K{c['k']}/b{c['minb']}/c{c['chunk']}"] = round(t, 4)
                 if best is None or t < best[0]:
                     best = (t, c)
             bk.tune = best[1]
             choices[f"{bk.shape.op}/N=2^{bk.shape.log_n}/L={bk.shape.level}"] = {"ms": best[0], **best[1],
-                                                                              "count": bk.count}
+                                                                              "count": bk.count,
+                                                                              "sweep": sweep}
         self.graph = None
         return choices
 

@@ -31,19 +31,25 @@ struct TwD {
 // with one butterfly block per thread), where group i = block * 2^u + grp is
 // stored at m + grp * 2^S0 + block (S0 = first stage of that pass, u = s - S0)
 // so that the 32 lanes of a warp read 32 consecutive entries.  The last pass
-// depends on the register radix 2^K, so there is one forward table per K.
+// depends on the register radix 2^K, so there is one forward table per K in
+// {2, 3, 4, 5}; each is laid out for K' = min(K, log N), so K = 1 (log N = 1)
+// reads the K = 2 table.
 // Inverse tables: per stage s the h = N / 2^(s+1) twiddles omega^-(k 2^s),
 // k < h, stored at h + k (one contiguous run per stage).
 enum {
-  TWF_FWD3 = 0,      // merged negacyclic forward, last-pass layout of K = 3
-  TWF_FWD4 = 1,      // merged negacyclic forward, last-pass layout of K = min(4, log N)
-  TWF_FWDC3 = 2,     // merged cyclic forward, K = 3
-  TWF_FWDC4 = 3,     // merged cyclic forward, K = min(4, log N)
-  TWF_INV = 4,       // negacyclic inverse DIT twiddles (omega = psi^2), per stage
-  TWF_INV_CYC = 5,   // cyclic inverse DIT twiddles, per stage
-  TWF_POST = 6,      // N^-1 psi^-j, j in [0, N)
-  TWF_POST_CYC = 7,  // N^-1 (every j)
-  TWF_SLOTS = 8
+  TWF_FWD2 = 0,      // merged negacyclic forward, last-pass layout of K = 2
+  TWF_FWD3 = 1,      // ... K = 3
+  TWF_FWD4 = 2,      // ... K = 4
+  TWF_FWD5 = 3,      // ... K = 5
+  TWF_FWDC2 = 4,     // merged cyclic forward, K = 2 .. 5
+  TWF_FWDC3 = 5,
+  TWF_FWDC4 = 6,
+  TWF_FWDC5 = 7,
+  TWF_INV = 8,       // negacyclic inverse DIT twiddles (omega = psi^2), per stage
+  TWF_INV_CYC = 9,   // cyclic inverse DIT twiddles, per stage
+  TWF_POST = 10,     // N^-1 psi^-j, j in [0, N)
+  TWF_POST_CYC = 11, // N^-1 (every j)
+  TWF_SLOTS = 12
 };
 
 // Per-prime constants, one record per prime of a context.

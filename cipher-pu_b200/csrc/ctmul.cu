@@ -95,27 +95,31 @@ static CmScratch cm_carve(void* base, int n, int n_ct, int level) {
 }
 
 // CTAs per SM that the register budget of a launch shape targets: "balanced"
-// gives every thread 128 registers (max(1, 512 / T) CTAs of T threads),
-// "tight" 64 (twice the CTAs; not built for 1024-thread CTAs).
+// gives every thread 128 registers (max(1, 512 / T) CTAs of T threads; 255
+// registers for K = 5, whose 32 values per thread spill at 128), "tight" 64
+// (twice the CTAs; not built for 1024-thread CTAs).
 template <int LOGN, int K, bool TIGHT>
 struct CmBlocks {
   static constexpr int T = (1 << LOGN) >> K;
-  static constexpr int B = T >= 512 ? 1 : 512 / T;
+  static constexpr int THR = K >= 5 ? 256 : 512;  // resident threads per SM of the balanced budget
+  static constexpr int B = T >= THR ? 1 : THR / T;
   static constexpr int value = (TIGHT && T < 1024) ? 2 * B : B;
 };
 
 // ct-mult kernels are instantiated for log N in [6, 14] with K in {3, 4}
-// (K = 3 needs N / 8 <= 1024 threads) and both register budgets; N = 2^14
+// (K = 3 needs N / 8 <= 1024 threads) and both register budgets, for log N
+// in [10, 12] with K = 2 (both budgets) and for log N in [10, 14] with K = 5
+// (balanced only: 32 values per thread do not fit 64 registers).  N = 2^14
 // needs more shared memory per CTA than B200 offers (the launch paths check
-// and refuse it with a message).  Defaults:
-// K = 4 for log N >= 10 (3 below), balanced budget: measured fastest at
-// N = 2^12 (2 CTAs of 256 threads per SM) and 2^13 (1 CTA of 512).
+// and refuse it with a message).  Defaults: K = 4 for log N >= 10 (3 below),
+// balanced budget: measured fastest at N = 2^12 (2 CTAs of 256 threads per
+// SM) and 2^13 (1 CTA of 512).
 // f is called as f.template operator()<L, K, MINB>().
 template <typename F>
 static int dispatch_cm(int log_n, int kreq, int mreq, F&& f, const char* fn) {
   const int k = kreq ? kreq : (log_n >= 10 ? 4 : 3);
   const int budget = mreq ? mreq : 1;
-  if (k != 3 && k != 4) return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=%d not built", fn, k);
+  if (k < 2 || k > 5) return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=%d not built", fn, k);
   if (budget != 1 && budget != 2)
     return ckks_set_error(CKKS_EUNSUPPORTED, "%s: register budget %d not in {1, 2}", fn, budget);
   if (log_n < 6 || log_n > 14)
@@ -123,20 +127,34 @@ static int dispatch_cm(int log_n, int kreq, int mreq, F&& f, const char* fn) {
   if (((1 << log_n) >> k) > 1024)
     return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=%d gives more than 1024 threads at log_n=%d",
                           fn, k, log_n);
+  if ((k == 2 && (log_n < 10 || log_n > 12)) || (k == 5 && log_n < 10))
+    return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=%d not built at log_n=%d", fn, k, log_n);
+  if (k == 5 && budget == 2)
+    return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=5 is built with the balanced budget only", fn);
   const bool tight = budget == 2;
   auto go = [&]<int L>() -> int {
     if constexpr (L < 6) {
       return ckks_set_error(CKKS_EUNSUPPORTED, "%s: log_n=%d outside [6, 14]", fn, log_n);
     } else {
-      if (k == 3) {
+      if (k == 2) {
+        if constexpr (L >= 10 && L <= 12) {
+          return tight ? f.template operator()<L, 2, CmBlocks<L, 2, true>::value>()
+                       : f.template operator()<L, 2, CmBlocks<L, 2, false>::value>();
+        }
+      } else if (k == 3) {
         if constexpr (((1 << L) >> 3) <= 1024) {
           return tight ? f.template operator()<L, 3, CmBlocks<L, 3, true>::value>()
                        : f.template operator()<L, 3, CmBlocks<L, 3, false>::value>();
         }
-        return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=3 not built at log_n=%d", fn, log_n);
+      } else if (k == 5) {
+        if constexpr (L >= 10) {
+          return f.template operator()<L, 5, CmBlocks<L, 5, false>::value>();
+        }
+      } else {
+        return tight ? f.template operator()<L, 4, CmBlocks<L, 4, true>::value>()
+                     : f.template operator()<L, 4, CmBlocks<L, 4, false>::value>();
       }
-      return tight ? f.template operator()<L, 4, CmBlocks<L, 4, true>::value>()
-                   : f.template operator()<L, 4, CmBlocks<L, 4, false>::value>();
+      return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=%d not built at log_n=%d", fn, k, log_n);
     }
   };
   switch (log_n) {

@@ -74,7 +74,7 @@ extern "C" int ckks_ct_mul_plain_rescale(const ckks_ctx* ctx, uint64_t* out, con
   if (n_ct == 0) return CKKS_OK;
   CKKS_REQUIRE(out && ct && pt, "%s: NULL pointer argument", fn);
   cudaStream_t st = as_stream(stream);
-  return dispatch_logn(ctx->log_n, [&]<int L, int K>() -> int {
+  return dispatch_logn_k(ctx->log_n, ctx->tune_ntt_k, [&]<int L, int K>() -> int {
     using Sh = NttShape<L, K>;
     const int smem = (Sh::SMEM_WORDS + Sh::N) * 8;
     if (int rc = require_smem(smem, L, fn)) return rc;
@@ -84,5 +84,5 @@ extern "C" int ckks_ct_mul_plain_rescale(const ckks_ctx* ctx, uint64_t* out, con
         reinterpret_cast<u64*>(out), reinterpret_cast<const u64*>(ct), reinterpret_cast<const u64*>(pt),
         pt_per_ct ? 1 : 0, level, ctx->d_pi, ctx->d_tw, ctx->d_qtinv, ctx->n_q);
     return ckks_check_launch(fn);
-  });
+  }, fn);
 }

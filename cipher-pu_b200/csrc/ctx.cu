@@ -190,12 +190,10 @@ extern "C" int ckks_ctx_create(int log_n, int n_primes, int n_special, const uin
     const u64 oinv = h_invmod(om, q);
     if (nega) {
       const std::vector<u64> pp = h_powers(ps, n, q);
-      fill_fwd(t + TWF_FWD3 * n, log_n, last_pass_s0(log_n, 3), [&](int m, int ii) {
-        return pp[bitrev(m + ii, log_n)];
-      }, q);
-      fill_fwd(t + TWF_FWD4 * n, log_n, last_pass_s0(log_n, 4), [&](int m, int ii) {
-        return pp[bitrev(m + ii, log_n)];
-      }, q);
+      for (int k = 2; k <= 5; ++k)
+        fill_fwd(t + (TWF_FWD2 + k - 2) * n, log_n, last_pass_s0(log_n, k), [&](int m, int ii) {
+          return pp[bitrev(m + ii, log_n)];
+        }, q);
       const u64 pinv = h_invmod(ps, q);
       fill_inv(t + TWF_INV * n, log_n, h_powers(h_mulmod(pinv, pinv, q), n, q), q);
       u64 cur = ninv_q;
@@ -206,8 +204,7 @@ extern "C" int ckks_ctx_create(int log_n, int n_primes, int n_special, const uin
     }
     const std::vector<u64> po = h_powers(om, n, q);
     auto cyc_tw = [&](int m, int ii) { return po[(bitrev(m + ii, log_n) - n / (2 * m)) / 2]; };
-    fill_fwd(t + TWF_FWDC3 * n, log_n, last_pass_s0(log_n, 3), cyc_tw, q);
-    fill_fwd(t + TWF_FWDC4 * n, log_n, last_pass_s0(log_n, 4), cyc_tw, q);
+    for (int k = 2; k <= 5; ++k) fill_fwd(t + (TWF_FWDC2 + k - 2) * n, log_n, last_pass_s0(log_n, k), cyc_tw, q);
     fill_inv(t + TWF_INV_CYC * n, log_n, h_powers(oinv, n, q), q);
     for (int j = 0; j < n; ++j) t[TWF_POST_CYC * n + j] = h_twd(ninv_q, q);
   }
@@ -271,14 +268,19 @@ extern "C" int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value) {
   CKKS_REQUIRE(ctx != nullptr, "ckks_ctx_set_tuning: ctx is NULL");
   switch (param) {
     case CKKS_TUNE_CM_LOG_ELEMS:
-      CKKS_REQUIRE(value == 0 || value == 3 || value == 4,
-                   "ckks_ctx_set_tuning: ct-mult log2 elements per thread must be 0, 3 or 4");
+      CKKS_REQUIRE(value == 0 || (value >= 2 && value <= 5),
+                   "ckks_ctx_set_tuning: ct-mult log2 elements per thread must be 0 or in [2, 5]");
       ctx->tune_cm_k = value;
       return CKKS_OK;
     case CKKS_TUNE_CM_MIN_BLOCKS:
       CKKS_REQUIRE(value == 0 || value == 1 || value == 2,
                    "ckks_ctx_set_tuning: ct-mult register budget must be 0, 1 (balanced) or 2 (tight)");
       ctx->tune_cm_minb = value;
+      return CKKS_OK;
+    case CKKS_TUNE_NTT_LOG_ELEMS:
+      CKKS_REQUIRE(value == 0 || (value >= 2 && value <= 5),
+                   "ckks_ctx_set_tuning: transform log2 elements per thread must be 0 or in [2, 5]");
+      ctx->tune_ntt_k = value;
       return CKKS_OK;
     case CKKS_TUNE_CM_SPLIT:
       CKKS_REQUIRE(value >= 0 && value <= 4,

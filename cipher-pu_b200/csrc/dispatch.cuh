@@ -37,6 +37,41 @@ static int dispatch_logn(int log_n, F&& f) {
   }
 }
 
+// dispatch_logn with a tuned K: k = 0 takes DefaultK, k in [2, 5] is built
+// for log N in [6, 14] with N / 2^K <= 1024 threads.
+template <typename F>
+static int dispatch_logn_k(int log_n, int k, F&& f, const char* fn) {
+  if (k == 0) return dispatch_logn(log_n, f);
+  if (k < 2 || k > 5 || log_n < 6 || log_n > 14 || ((1 << log_n) >> k) > 1024)
+    return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=%d not built at log_n=%d", fn, k, log_n);
+  auto go = [&]<int L>() -> int {
+    switch (k) {
+      case 2:
+        if constexpr (((1 << L) >> 2) <= 1024) return f.template operator()<L, 2>();
+        break;
+      case 3:
+        if constexpr (((1 << L) >> 3) <= 1024) return f.template operator()<L, 3>();
+        break;
+      case 4:
+        return f.template operator()<L, 4>();
+      default:
+        return f.template operator()<L, 5>();
+    }
+    return ckks_set_error(CKKS_EUNSUPPORTED, "%s: K=%d not built at log_n=%d", fn, k, log_n);
+  };
+  switch (log_n) {
+    case 6: return go.template operator()<6>();
+    case 7: return go.template operator()<7>();
+    case 8: return go.template operator()<8>();
+    case 9: return go.template operator()<9>();
+    case 10: return go.template operator()<10>();
+    case 11: return go.template operator()<11>();
+    case 12: return go.template operator()<12>();
+    case 13: return go.template operator()<13>();
+    default: return go.template operator()<14>();
+  }
+}
+
 // Opt a kernel into > 48 KB of dynamic shared memory once per process/device.
 template <typename KernelT>
 static cudaError_t ensure_smem(KernelT kernel, int bytes) {

@@ -261,8 +261,9 @@ __device__ __forceinline__ void ntt_fwd_d(double (&d)[1 << K], u64* sm, int tid,
                                           const TwD* __restrict__ tb, const PrimeInfo& P,
                                           bool cyclic = false) {
   constexpr int N = 1 << LOGN;
-  static_assert(K <= 4, "forward twiddle layouts exist for K <= 4");
-  const TwD* tw = tb + (cyclic ? (K == 3 ? TWF_FWDC3 : TWF_FWDC4) : (K == 3 ? TWF_FWD3 : TWF_FWD4)) * N;
+  static_assert(K >= 1 && K <= 5, "forward twiddle layouts exist for K <= 5");
+  constexpr int kslot = K <= 2 ? 0 : K - 2;  // K = 1 only at log N = 1, where the K = 2 layout is the same
+  const TwD* tw = tb + ((cyclic ? TWF_FWDC2 : TWF_FWD2) + kslot) * N;
   double* smd = reinterpret_cast<double*>(sm);
   fwd_pass<LOGN, K, 0, K>(d, tid, tw, P.qd);
   FwdRest<LOGN, K, 1>::run(d, smd, tid, tw, P.qd);

@@ -9,11 +9,13 @@
 // tables in L1.  Global traffic is lane-contiguous (layout C) both ways; the
 // forward's layout-Z result is re-distributed through shared memory first.
 // CTAs per SM the standalone transform's register budget targets: three
-// 256-thread CTAs (85 registers) where the CTA is small enough.
+// 256-thread CTAs (85 registers) where the CTA is small enough; for K = 5
+// (32 values per thread) 256 resident threads (255 registers).
 template <int LOGN, int K>
 struct NttMinBlocks {
   static constexpr int T = NttShape<LOGN, K>::T;
-  static constexpr int value = T >= 512 ? 1 : (768 / T > 8 ? 8 : 768 / T);
+  static constexpr int THR = K >= 5 ? 256 : 768;
+  static constexpr int value = T >= THR ? 1 : (THR / T > 8 ? 8 : THR / T);
 };
 
 template <int LOGN, int K>
@@ -62,7 +64,7 @@ extern "C" int ckks_ntt(const ckks_ctx* ctx, uint64_t* data, int n_polys, int pr
                    prime_begin + l);
   if (n_polys == 0) return CKKS_OK;
   CKKS_REQUIRE(data != nullptr, "ckks_ntt: data is NULL");
-  return dispatch_logn(ctx->log_n, [&]<int L, int K>() -> int {
+  auto launch = [&]<int L, int K>() -> int {
     using S = NttShape<L, K>;
     auto kern = k_ntt<L, K>;
     ensure_smem(kern, S::SMEM_WORDS * 8);
@@ -71,7 +73,8 @@ extern "C" int ckks_ntt(const ckks_ctx* ctx, uint64_t* data, int n_polys, int pr
         reinterpret_cast<u64*>(data), n_polys, n_limbs, prime_begin, ctx->d_pi, ctx->d_tw, inverse,
         cyclic);
     return ckks_check_launch("ckks_ntt");
-  });
+  };
+  return dispatch_logn_k(ctx->log_n, ctx->tune_ntt_k, launch, "ckks_ntt");
 }
 
 // ------------------------------------------------------------------ bitrev

@@ -65,9 +65,11 @@ int ckks_ctx_destroy(ckks_ctx* ctx);
 
 /*
  * Launch-shape tuning of a context (used by the autotuner).  Parameters:
- *   CKKS_TUNE_CM_LOG_ELEMS: coefficients per thread of the ct-mult kernels
- *   as log2 (3 -> radix-8 passes with N/8 threads, 4 -> radix-16 with N/16;
- *   0 = default: 4 for N >= 2^10, else 3).
+ *   CKKS_TUNE_CM_LOG_ELEMS: coefficients per thread of the ct-mult and
+ *   rotation kernels as log2 K (radix-2^K register passes with N / 2^K
+ *   threads).  Built: K = 3, 4 for log N in [6, 14] (N / 8 <= 1024 threads
+ *   for K = 3); K = 2 for log N in [10, 12]; K = 5 for log N in [10, 14],
+ *   balanced budget only.  0 = default: 4 for N >= 2^10, else 3.
  *   CKKS_TUNE_CM_MIN_BLOCKS: register budget of the ct-mult kernels:
  *   1 = balanced (128 registers per thread, max(1, 512 / threads) CTAs per
  *   SM), 2 = tight (64 registers, twice the CTAs); 0 = default (balanced).
@@ -75,10 +77,18 @@ int ckks_ctx_destroy(ckks_ctx* ctx);
  *   internal streams (1..4; 0 = default: one per 64 pairs, at most 4, from
  *   128 pairs on, else 1).  The kernels of one sub-batch fill the partial
  *   last waves of the others (measured +12 % at 256 pairs, N = 2^12, L = 3).
+ *   CKKS_TUNE_NTT_LOG_ELEMS: K of ckks_ntt and ckks_ct_mul_plain_rescale,
+ *   in [2, 5] for log N in [6, 14] with N / 2^K <= 1024 (0 = default:
+ *   min(4, log N)).
  * The reference fixes its datapath shape at synthesis time
  * (rtl/m1/ntt_unit.sv:39-52 parameters).
  */
-enum { CKKS_TUNE_CM_LOG_ELEMS = 0, CKKS_TUNE_CM_MIN_BLOCKS = 1, CKKS_TUNE_CM_SPLIT = 2 };
+enum {
+  CKKS_TUNE_CM_LOG_ELEMS = 0,
+  CKKS_TUNE_CM_MIN_BLOCKS = 1,
+  CKKS_TUNE_CM_SPLIT = 2,
+  CKKS_TUNE_NTT_LOG_ELEMS = 3
+};
 int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value);
 
 /*
