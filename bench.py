@@ -198,9 +198,9 @@ def stage_modmuls(stage: int, n: int, level: int) -> int:
         return level * (3 * n + inv)
     if stage == 1:   # L^2 NTTs (each digit to every other prime and p) + 2 key products per digit and prime
         return level * level * fwd + (level + 1) * level * 2 * n
-    # per poly: INTT_p, NTT_t, p^-1, INTT_t, then per limb i < t: NTT_i + 3 products
+    # per poly: INTT_p, p^-1 on limb t, INTT_t, [v]_t p^-1, then per limb i < t: NTT_i + 3 products
     t = level - 1
-    return 2 * (inv + fwd + n + inv + t * (fwd + 3 * n))
+    return 2 * (inv + n + inv + n + t * (fwd + 3 * n))
 
 
 def measure_transforms(ctx, dev, hbm_peak: float, reps: int = 20) -> dict:

@@ -11,19 +11,20 @@
 //                          (digit j at its own prime reuses the NTT-domain d2).
 //   C  moddown+rescale (ct, k):
 //                          v = centred(INTT_p(acc_k,p))        (coefficient)
-//                          limb t : o_t = d_k,t + (acc_k,t - NTT_t([v]_t)) p^-1
-//                                   w = centred(INTT_t(o_t))
+//                          limb t : w = centred(INTT_t(d_k,t + acc_k,t p^-1)
+//                                               - [v]_t p^-1)
 //                          limb i<t: out = (d_k,i + acc_k,i p^-1
 //                                           - NTT_i([v]_i p^-1 + [w]_i)) q_t^-1
 //                          (ModDown and rescale conversions merged into one
-//                          NTT per limb by linearity; bit-identical to doing
-//                          them one after the other).
-// Transforms per ct-mult at level L: L + (L-1)L + L + 2(L + 2) = 22 at L = 3
+//                          NTT per limb, and limb t's ModDown done in the
+//                          coefficient domain, by linearity of the NTT;
+//                          bit-identical to doing them one after the other).
+// Transforms per ct-mult at level L: L + (L-1)L + L + 2(L + 1) = 20 at L = 3
 // (vs 26 for the unmerged sequence).
 //
-// Launch shape: K = log2 coefficients per thread (3: N/8 threads, radix-8
-// passes; 4: N/16 threads, radix-16) and MINB = CTAs per SM the register
-// budget is cut for (__launch_bounds__).  Both are context tuning parameters.
+// Launch shape: K = log2 coefficients per thread (2..5: N/2^K threads,
+// radix-2^K register passes) and MINB = CTAs per SM the register budget is
+// cut for (__launch_bounds__).  Both are context tuning parameters.
 #include <mutex>
 
 #include "dispatch.cuh"
@@ -188,27 +189,31 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   const u64* a0 = A + ct * 2 * LN + (size_t)j * N;
   const u64* b0 = B + ct * 2 * LN + (size_t)j * N;
   u64* d0 = S.d01 + ct * 2 * LN + (size_t)j * N;
+  // Products in FP64 (exact two-product + rounded quotient, fmulmod_var):
+  // d2 = a1 b1, d0 = a0 b0, d1 = (a0 + a1)(b0 + b1) - d0 - d2, each partial
+  // result below 2^48 in magnitude, reduced to [0, q) once at the end.
   u64 x[Sh::E], y[Sh::E];
-  // d2 = a1 b1
   load_c<LOGN, K>(x, a0 + LN, tid);
   load_c<LOGN, K>(y, b0 + LN, tid);
-  u64 m2[Sh::E];
+  double m2d[Sh::E];
 #pragma unroll
-  for (int e = 0; e < Sh::E; ++e) m2[e] = mulmod(x[e], y[e], P);
-  // d0 = a0 b0 ; d1 = (a0 + a1)(b0 + b1) - d0 - d2
+  for (int e = 0; e < Sh::E; ++e) m2d[e] = fmulmod_var(u2d(x[e]), u2d(y[e]), P.qd, P.qinv_d);
   u64 a0v[Sh::E], b0v[Sh::E];
   load_c<LOGN, K>(a0v, a0, tid);
   load_c<LOGN, K>(b0v, b0, tid);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) {
-    const u64 m0 = mulmod(a0v[e], b0v[e], P);
-    u64 m1 = mulmod(addmod(a0v[e], x[e], P.q), addmod(b0v[e], y[e], P.q), P);
-    m1 = submod(submod(m1, m0, P.q), m2[e], P.q);
-    a0v[e] = m0;
-    b0v[e] = m1;
+    const double a0d = u2d(a0v[e]), b0d = u2d(b0v[e]);
+    const double m0 = fmulmod_var(a0d, b0d, P.qd, P.qinv_d);
+    const double s1 = fmulmod_var(__dadd_rn(a0d, u2d(x[e])), __dadd_rn(b0d, u2d(y[e])), P.qd, P.qinv_d);
+    a0v[e] = d2canon(m0, P.qd, P.qinv_d);
+    b0v[e] = d2canon(__dadd_rn(__dadd_rn(s1, -m0), -m2d[e]), P.qd, P.qinv_d);  // |.| < 3 2^48
   }
   store_c<LOGN, K>(a0v, d0, tid);
   store_c<LOGN, K>(b0v, d0 + LN, tid);
+  u64 m2[Sh::E];
+#pragma unroll
+  for (int e = 0; e < Sh::E; ++e) m2[e] = d2canon(m2d[e], P.qd, P.qinv_d);
   store_c<LOGN, K>(m2, S.d2n + ct * LN + (size_t)j * N, tid);
   c_to_z<LOGN, K>(m2, sm, tid);
   ntt_inv<LOGN, K>(m2, sm, tid, twbase<LOGN>(tw, j), P);
@@ -328,27 +333,26 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   c_to_z<LOGN, K>(x, sm, tid);
   ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, nq), PP);
 #pragma unroll
-  for (int e = 0; e < Sh::E; ++e) {
-    vs[e * T + tid] = x[e];
-    x[e] = x[e] > PP.half ? x[e] - PP.q + PT.q : x[e];
-  }
-  ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, t), PT);
-  z_to_c<LOGN, K>(x, sm, tid);
+  for (int e = 0; e < Sh::E; ++e) vs[e * T + tid] = x[e];
+  // Rescale limb t in the coefficient domain without a transform of v:
+  // w = INTT_t(d_t + acc_t P^-1) - [v]_t P^-1, equal mod q_t to
+  // INTT_t(d_t + (acc_t - NTT_t([v]_t)) P^-1) by linearity of the NTT.
+  const TwPair pt = pinv[t];
   {
-    const TwPair pt = pinv[t];
-    u64 dv[Sh::E], av[Sh::E];
+    u64 dv[Sh::E];
     load_c<LOGN, K>(dv, dk + (size_t)t * N, tid);
-    load_c<LOGN, K>(av, ak + (size_t)t * N, tid);
+    load_c<LOGN, K>(x, ak + (size_t)t * N, tid);
 #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) {
-      const u64 ks = shoup(av[e] + PT.qlazy - x[e], pt.w, pt.ws, PT.q);
-      x[e] = addmod(dv[e], ks, PT.q);
-    }
+    for (int e = 0; e < Sh::E; ++e) x[e] = addmod(dv[e], shoup(x[e], pt.w, pt.ws, PT.q), PT.q);
   }
   c_to_z<LOGN, K>(x, sm, tid);
   ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, t), PT);
 #pragma unroll
-  for (int e = 0; e < Sh::E; ++e) ws[e * T + tid] = x[e];
+  for (int e = 0; e < Sh::E; ++e) {
+    const u64 v = vs[e * T + tid];
+    const u64 vt = v > PP.half ? v - PP.q + PT.q : v;
+    ws[e * T + tid] = submod(x[e], shoup(vt, pt.w, pt.ws, PT.q), PT.q);
+  }
 #pragma unroll 1
   for (int i = 0; i < t; ++i) {
     const PrimeInfo P = pi[i];

@@ -8,8 +8,17 @@
 #include "dispatch.cuh"
 #include "profile.hpp"
 
+// Register budget: resident threads per SM targeted per K (128 registers a
+// thread at K = 4, 64 at K <= 3, ~240 for the 32 values a thread of K = 5).
 template <int LOGN, int K>
-__global__ void __launch_bounds__(NttShape<LOGN, K>::T)
+struct CtptBlocks {
+  static constexpr int T = NttShape<LOGN, K>::T;
+  static constexpr int THR = K >= 5 ? 256 : (K == 4 ? 512 : 1024);
+  static constexpr int value = T >= THR ? 1 : THR / T;
+};
+
+template <int LOGN, int K>
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T, (CtptBlocks<LOGN, K>::value))
     k_ctpt_rescale(u64* __restrict__ out, const u64* __restrict__ ct, const u64* __restrict__ pt,
                    int pt_stride, int level, const PrimeInfo* __restrict__ pi,
                    const TwD* __restrict__ tw, const TwPair* __restrict__ qtinv, int nq) {
