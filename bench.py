@@ -13,8 +13,9 @@ batches rotate between steps (400 MB > the 126 MB L2).
 The line also carries the second half of the metric, `enc_mlp`: encrypted
 MLP 784-128-10 samples/s under the plain SNR-monitor gear controller and the
 learned one (same inputs, equal SNR), plus standalone NTT / product / linear
-layer throughput (`transforms`), the end-to-end host-buffer rate (`e2e`) and
-the CPU restatement (`cpu_baseline`).
+layer throughput (`transforms`), the fused conv + GAP inner-product rate on
+coefficient-encoded images (`convgap`), the end-to-end host-buffer rate
+(`e2e`) and the CPU restatement (`cpu_baseline`).
 
 Under torchrun each rank processes its own 256 pairs (weak scaling, no
 data-path collective); the step time is the max over ranks.
@@ -56,6 +57,8 @@ def parse():
     ap.add_argument("--no-enc-mlp", action="store_true",
                     help="skip the encrypted-MLP learned-vs-plain gear leg")
     ap.add_argument("--enc-mlp-batches", type=int, default=8)
+    ap.add_argument("--no-convgap", action="store_true",
+                    help="skip the fused conv+GAP (coefficient-encoded inner product) leg")
     ap.add_argument("--e2e-chunk", type=int, default=48,
                     help="pairs per pipelined chunk of the host-buffer call")
     return ap.parse_args()
@@ -247,6 +250,72 @@ def measure_transforms(ctx, dev, hbm_peak: float, reps: int = 20) -> dict:
                        "frac_hbm": byts / s / 1e9 / hbm_peak}
     res["shape"] = f"N=2^{logn}, 45-bit primes, {npoly} polys x {nl} limbs per launch, 4 rotating buffers"
     res["linear_mlp"] = measure_linear(dev, reps=reps)
+    return res
+
+
+def measure_convgap(dev, hbm_peak: float, with_cpu: bool, reps: int = 20) -> dict:
+    """Fused Conv + GAP on coefficient-encoded images (N = 1024,
+    q = 998244353, Delta = 1024, 4 filters): one ciphertext x plaintext product
+    per filter (ckks_mul_plain_multi) and the decrypted constant coefficients
+    (ckks_decrypt_coef0) for 8192 images per launch pair; inputs 134 MB and
+    products 537 MB, both above L2.  Algorithmic bytes per image: the
+    ciphertext read once, 4 products written, their a halves read back by the
+    decryption -> (2 + 8 + 4) x 8N = 112 KB."""
+    import time
+    import numpy as np
+    import torch
+    from ckks_b200 import convgap as G
+    from ckks_b200.context import Context
+    n, q, scale, bsz = 1024, 998244353, 1024, 8192
+    ctx = Context.get(10, [q])
+    rng = np.random.default_rng(77)
+    s = rng.integers(-1, 2, n)
+    s_res = G.secret_residues(s, q, dev)
+    model = G.ConvGapModel.random(0)
+    x = rng.uniform(0, 1, (bsz, 784))
+    ct = G.encrypt(ctx, x, s_res, scale, seed=78)
+    w_hat = G.weight_polys(ctx, model, scale)
+    out = torch.empty((bsz, 4, 2, n), dtype=torch.uint64, device=dev)
+    dec = torch.empty((bsz, 4), dtype=torch.int64, device=dev)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps / 1000.0
+
+    sec_mul = timed(lambda: G.mul_plain_multi(ctx, ct, w_hat, out=out))
+    sec_dec = timed(lambda: G.decrypt_coef0(ctx, out, s_res, out=dec))
+    sec = timed(lambda: (G.mul_plain_multi(ctx, ct, w_hat, out=out), G.decrypt_coef0(ctx, out, s_res, out=dec)))
+    # ciphertext in, 4 products out, the products' a halves (and b_0) read back
+    byts = bsz * (2 * 8 * n + 4 * 2 * 8 * n + 4 * 8 * n)
+    t0 = time.perf_counter()
+    logits = G.fused_inference(ctx, ct, model, s_res, scale, w_hat=w_hat)
+    host_sec = time.perf_counter() - t0
+    res = {"metric": "fused conv+GAP encrypted images/s", "unit": "images/s",
+           "device_images_per_s": bsz / sec, "ms_per_launch_pair": sec * 1000.0,
+           "ms_mul_plain_multi": sec_mul * 1000.0, "ms_decrypt_coef0": sec_dec * 1000.0,
+           "mul_plain_Gbutterfly_s": bsz * 2 * 5 * (n // 2) * 10 / sec_mul / 1e9,
+           "GBps": byts / sec / 1e9, "frac_hbm": byts / sec / 1e9 / hbm_peak,
+           "with_host_fc_images_per_s": bsz / host_sec,
+           "max_abs_logit_vs_plain": float(np.max(np.abs(logits - model.plain_forward(x)))),
+           "workload": f"{bsz} images 28x28, Conv(1->4,3x3,s4,p1)+GAP+FC(4->10), N=1024, q=998244353, "
+                       "Delta=1024, synthetic uniform [0,1] images, random weights"}
+    if with_cpu:
+        from oracle import convgap as OC
+        host = ct[:4].cpu().numpy().astype(np.uint64)
+        t0 = time.perf_counter()
+        for i in range(4):
+            OC.fused_inference(host[i], s, q, scale, model.conv_w, model.conv_b, model.fc_w, model.fc_b)
+        res["cpu_port_images_per_s"] = 4 / (time.perf_counter() - t0)
+        res["cpu_port_sample"] = "4 images through the numpy oracle (NTT-based exact products), 1 core"
     return res
 
 
@@ -483,6 +552,8 @@ def run_ours(a) -> int:
         mm_peak = modmul_peak(kind=1) / 1e12
         mm_ach = stage_modmuls(dom, n, L) * pairs_per_launch / (per_launch_ms / 1000.0) / 1e12
         transforms = measure_transforms(ctx, dev, hbm) if not a.no_transforms else None
+        convgap = (measure_convgap(dev, hbm, with_cpu=not a.no_cpu_baseline)
+                   if not a.no_convgap and ws == 1 else None)
         enc_mlp = None
         if not a.no_enc_mlp and ws == 1:
             # second half of the metric: encrypted MLP 784-128-10 (N=2^13, L=4,
@@ -520,6 +591,7 @@ def run_ours(a) -> int:
                               "modmuls_per_launch": stage_modmuls(dom, n, L) * pairs_per_launch,
                               "peak_source": "measured live: ckks_modmul_peak kind 1 (FP64 double-word)"},
             "transforms": transforms,
+            "convgap": convgap,
             "enc_mlp": enc_mlp,
             "stage_ms_per_step": {names[s]: stages[s][0] / max(1, prof_steps) for s in range(3)},
             "stage_timing": (f"library event profiler over {prof_steps} identical steps right after the timed "

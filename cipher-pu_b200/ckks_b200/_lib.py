@@ -72,6 +72,8 @@ SIGNATURES: dict[str, tuple] = {
     "ckks_ct_mul_const": (_i32, [_vp, _u64p, _u64p, _i32, _i32, _i64, _vp]),
     "ckks_ct_add_const": (_i32, [_vp, _u64p, _u64p, _i32, _i32, C.POINTER(_u64), _vp]),
     "ckks_automorphism": (_i32, [_vp, _u64p, _u64p, _i32, _i32, _i32, _u64, _i32, _vp]),
+    "ckks_mul_plain_multi": (_i32, [_vp, _u64p, _u64p, _u64p, _i32, _i32, _i32, _vp]),
+    "ckks_decrypt_coef0": (_i32, [_vp, _u64p, _u64p, _u64p, C.c_longlong, _i32, _vp]),
     "ckks_mul_monomial": (_i32, [_vp, _u64p, _u64p, _i32, _i32, _i32, _u64, _vp]),
     "ckks_rotate_scratch_bytes": (_sz, [_vp, _i32, _i32]),
     "ckks_rotate": (_i32, [_vp, _u64p, _u64p, _u64p, _i32, _i32, _u64, _vp, _sz, _vp]),

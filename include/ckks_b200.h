@@ -77,9 +77,9 @@ int ckks_ctx_destroy(ckks_ctx* ctx);
  *   internal streams (1..4; 0 = default: one per 64 pairs, at most 4, from
  *   128 pairs on, else 1).  The kernels of one sub-batch fill the partial
  *   last waves of the others (measured +12 % at 256 pairs, N = 2^12, L = 3).
- *   CKKS_TUNE_NTT_LOG_ELEMS: K of ckks_ntt and ckks_ct_mul_plain_rescale,
- *   in [2, 5] for log N in [6, 14] with N / 2^K <= 1024 (0 = default:
- *   min(4, log N)).
+ *   CKKS_TUNE_NTT_LOG_ELEMS: K of ckks_ntt, ckks_ct_mul_plain_rescale and
+ *   ckks_mul_plain_multi, in [2, 5] for log N in [6, 14] with
+ *   N / 2^K <= 1024 (0 = default: min(4, log N)).
  * The reference fixes its datapath shape at synthesis time
  * (rtl/m1/ntt_unit.sv:39-52 parameters).
  */
@@ -454,6 +454,30 @@ int ckks_automorphism(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in, in
  */
 int ckks_mul_monomial(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in, int n_polys,
                       int prime_begin, int n_limbs, uint64_t nu, void* stream);
+
+/*
+ * Coefficient-encoded inner products (the Conv + GAP fusion): every
+ * ciphertext (b, a) of ct [n_ct][2][N] (coefficient domain, residues mod
+ * primes[prime]) times every plaintext polynomial of w_hat [n_w][N], given in
+ * the evaluation domain (negacyclic forward ckks_ntt of the scattered weight
+ * polynomials, once per model) -> out [n_ct][n_w][2][N], coefficient domain,
+ * canonical.  One NTT per ciphertext polynomial, one INTT per filter.
+ * Replaces scripts/exp_e24_rotation_bootstrap.py:136 mul_plain_exact as
+ * :615 encrypted_inference_fused calls it once per filter (through :263
+ * inner_product, whose weights :241 scatter_w places).
+ */
+int ckks_mul_plain_multi(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct, const uint64_t* w_hat,
+                         int n_ct, int n_w, int prime, void* stream);
+
+/*
+ * Constant coefficient of the decryption (b - a s) mod q of each ciphertext
+ * of ct [n_ct][2][N] (coefficient domain), centred to (-q/2, q/2] (q odd),
+ * with s the N residues of the secret key mod q = primes[prime].  Replaces
+ * dec[0] of scripts/exp_e24_rotation_bootstrap.py:109 decrypt_exact, the one
+ * coefficient :263 inner_product and :278 coef_sum read.
+ */
+int ckks_decrypt_coef0(const ckks_ctx* ctx, int64_t* out, const uint64_t* ct, const uint64_t* s,
+                       long long n_ct, int prime, void* stream);
 
 /*
  * Homomorphic automorphism with key switching ("rotation"): ct [n_ct][2][level][N]

@@ -394,10 +394,91 @@ def activation_vectors() -> int:
     return 0
 
 
+def convgap_vectors() -> int:
+    """Inner-product / Conv + GAP goldens from
+    scripts/exp_e24_rotation_bootstrap.py:241 scatter_w, :136 mul_plain_exact,
+    :109 decrypt_exact, :263 inner_product, :278 coef_sum, :307 enc_msg and
+    :615 encrypted_inference_fused (ConvGAPNet without ReLU, seeded random
+    initialisation, synthetic images) -> golden_convgap.npz/json."""
+    import torch
+    cwd = os.getcwd()
+    try:
+        e24 = load("scripts/exp_e24_rotation_bootstrap.py", "ref_e24")
+    finally:
+        os.chdir(cwd)
+    n, q, scale = e24.N, e24.Q, e24.SCALE
+    arrays: dict[str, np.ndarray] = {}
+    meta = {"reference": "YI-HAIBO/cipher-pu", "generator": "tests/golden/make_golden.py --only convgap",
+            "source": "scripts/exp_e24_rotation_bootstrap.py:109,136,241,263,278,307,615",
+            "N": n, "q": q, "scale": scale, "scatter": [], "inner": [], "fused": []}
+    rng = np.random.default_rng(4040)
+    # scatter_w: index 0 (negated), repeats, indices past N (wrap), half-way roundings
+    sc_cases = [(list(range(10)), rng.uniform(-1, 1, 10)),
+                ([0, 0, 5, 5, 5, 1023, 1024, 2049], [0.25, -0.5, 1.0, 2.0 / scale, 1.5 / scale,
+                                                     -2.5 / scale, 0.75, -1.0]),
+                (list(rng.integers(0, 784, 300)), rng.normal(0, 0.3, 300))]
+    for k, (idx, w) in enumerate(sc_cases):
+        m_w = e24.scatter_w([int(i) for i in idx], np.asarray(w, dtype=np.float64), scale, q, n)
+        arrays[f"sc{k}_idx"] = np.asarray(idx, dtype=np.int64)
+        arrays[f"sc{k}_w"] = np.asarray(w, dtype=np.float64)
+        arrays[f"sc{k}_out"] = np.asarray(m_w, dtype=np.int64).astype(np.uint64)
+        meta["scatter"].append(f"sc{k}")
+    # mul_plain_exact and decrypt_exact on a uniform ciphertext
+    s = rng.integers(-1, 2, n).astype(np.int64)
+    arrays["s"] = s
+    b = rng.integers(0, q, n).astype(np.int64)
+    a = rng.integers(0, q, n).astype(np.int64)
+    pb, pa = e24.mul_plain_exact((b, a), arrays["sc2_out"].astype(np.int64), q)
+    arrays["mp_in"] = np.stack([b, a]).astype(np.uint64)
+    arrays["mp_out"] = np.stack([np.asarray(pb), np.asarray(pa)]).astype(np.int64).astype(np.uint64)
+    arrays["mp_dec"] = np.asarray(e24.decrypt_exact_int((pb, pa), s, q), dtype=np.int64)
+    # inner_product / coef_sum on encrypted messages
+    for k, dim in enumerate((16, 100, 784)):
+        np.random.seed(500 + k)
+        x = rng.uniform(0, 1, dim)
+        w = rng.normal(0, 0.5, dim)
+        e = rng.integers(-1, 2, n).astype(np.int64)
+        ctb, cta = e24.enc_msg(x, s, e, q, scale)
+        arrays[f"ip{k}_ct"] = np.stack([np.asarray(ctb), np.asarray(cta)]).astype(np.int64).astype(np.uint64)
+        arrays[f"ip{k}_w"] = w
+        meta["inner"].append({"key": f"ip{k}", "dim": dim,
+                              "inner_product": e24.inner_product((ctb, cta), w, s, q, scale),
+                              "coef_sum": e24.coef_sum((ctb, cta), dim, s, q, scale),
+                              "plain_dot": float(np.dot(x, w)), "plain_sum": float(np.sum(x))})
+    # fused Conv + GAP inference (noise argument 1 as the reference's run uses)
+    torch.manual_seed(0)
+    model = e24.ConvGAPNet(use_relu=False)
+    arrays["conv_w"] = model.conv1.weight.detach().numpy().astype(np.float64)
+    arrays["conv_b"] = model.conv1.bias.detach().numpy().astype(np.float64)
+    arrays["fc_w"] = model.fc1.weight.detach().numpy().astype(np.float64)
+    arrays["fc_b"] = model.fc1.bias.detach().numpy().astype(np.float64)
+    for k in range(3):
+        x = rng.uniform(0, 1, 784)
+        np.random.seed(900 + k)
+        logits, mc = e24.encrypted_inference_fused(model, x, s, q, scale, 1, np.random.default_rng(700 + k))
+        np.random.seed(900 + k)
+        e = np.random.default_rng(700 + k).integers(-1, 2, size=n).astype(np.int64)
+        ctb, cta = e24.enc_msg(x, s, e, q, scale)
+        with torch.no_grad():
+            plain = model(torch.tensor(x, dtype=torch.float32).reshape(1, 1, 28, 28)).numpy()[0]
+        arrays[f"fu{k}_x"] = x
+        arrays[f"fu{k}_ct"] = np.stack([np.asarray(ctb), np.asarray(cta)]).astype(np.int64).astype(np.uint64)
+        arrays[f"fu{k}_logits"] = np.asarray(logits, dtype=np.float64)
+        arrays[f"fu{k}_plain"] = plain.astype(np.float64)
+        meta["fused"].append({"key": f"fu{k}", "mult_count": int(mc)})
+    np.savez_compressed(OUT / "golden_convgap.npz", **arrays)
+    with open(OUT / "golden_convgap.json", "w") as f:
+        json.dump(meta, f, indent=1)
+    print("wrote", OUT / "golden_convgap.npz")
+    return 0
+
+
 if __name__ == "__main__":
+    if sys.argv[1:] == ["--only", "convgap"]:
+        sys.exit(convgap_vectors())
     if sys.argv[1:] == ["--only", "rot"]:
         sys.exit(rotation_vectors())
     if sys.argv[1:] == ["--only", "act"]:
         sys.exit(activation_vectors())
     rc = main()
-    sys.exit(rc or rotation_vectors() or activation_vectors())
+    sys.exit(rc or rotation_vectors() or activation_vectors() or convgap_vectors())

@@ -297,3 +297,27 @@ def test_activation_golden_fixture_consistent():
         assert np.allclose(got, m["approx"], rtol=0, atol=1e-12), name
     sig = act["models"]["order5_segments1"]["sigmoid"]
     assert np.abs(np.asarray(sig["approx"]) - np.asarray(sig["exact"])).max() < 1e-3
+
+
+def test_convgap_oracle_matches_reference_goldens():
+    """scatter_w, mul_plain_exact, decrypt_exact, inner_product, coef_sum and
+    the fused Conv + GAP inference of scripts/exp_e24_rotation_bootstrap.py
+    (golden_convgap.*): integers bit-exact, floats identical."""
+    from oracle import convgap as C
+    d = np.load(GD / "golden_convgap.npz")
+    m = json.load(open(GD / "golden_convgap.json"))
+    q, n, sc = m["q"], m["N"], m["scale"]
+    for k in m["scatter"]:
+        assert np.array_equal(C.scatter_w(d[k + "_idx"], d[k + "_w"], sc, q, n), d[k + "_out"]), k
+    assert np.array_equal(C.mul_plain(d["mp_in"], d["sc2_out"], q), d["mp_out"])
+    assert np.array_equal(C.decrypt(d["mp_out"], d["s"], q), d["mp_dec"])
+    for r in m["inner"]:
+        ct = d[r["key"] + "_ct"]
+        assert C.inner_product(ct, d[r["key"] + "_w"], d["s"], q, sc) == r["inner_product"]
+        assert C.coef_sum(ct, r["dim"], d["s"], q, sc) == r["coef_sum"]
+        assert abs(r["inner_product"] - r["plain_dot"]) < 0.05
+    for r in m["fused"]:
+        k = r["key"]
+        lg, mc = C.fused_inference(d[k + "_ct"], d["s"], q, sc, d["conv_w"], d["conv_b"], d["fc_w"], d["fc_b"])
+        assert np.array_equal(lg, d[k + "_logits"]) and mc == r["mult_count"]
+        assert np.max(np.abs(lg - d[k + "_plain"])) < 5e-3
