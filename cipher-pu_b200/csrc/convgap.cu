@@ -12,9 +12,20 @@
 #include "profile.hpp"
 
 // One CTA per (ciphertext, polynomial k); all global traffic lane-contiguous
-// (layout C).  The transformed polynomial stays in registers across filters.
+// (layout C).  The transformed polynomial stays in registers across filters
+// as exact doubles; each product is an FP64 modular multiply with w / q
+// formed as w * (1 / q) (exact, within 1.5 q), fed to the inverse unreduced.
+// Register budget: 512 resident threads per SM (128 registers a thread),
+// 256 for K = 5 (255 registers).
 template <int LOGN, int K>
-__global__ void __launch_bounds__(NttShape<LOGN, K>::T)
+struct MpmBlocks {
+  static constexpr int T = NttShape<LOGN, K>::T;
+  static constexpr int THR = K >= 5 ? 256 : 512;
+  static constexpr int value = T >= THR ? 1 : (THR / T > 16 ? 16 : THR / T);
+};
+
+template <int LOGN, int K>
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T, (MpmBlocks<LOGN, K>::value))
     k_mul_plain_multi(u64* __restrict__ out, const u64* __restrict__ ct, const u64* __restrict__ w_hat,
                       int n_w, int prime, const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw) {
   extern __shared__ u64 sm[];
@@ -25,27 +36,35 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   const int tid = threadIdx.x;
   const PrimeInfo P = pi[prime];
   const TwD* tb = twbase<LOGN>(tw, prime);
-  u64 x[S::E];
-  load_c<LOGN, K>(x, ct + ((size_t)c * 2 + k) * N, tid);
+  double x[S::E];
+  {
+    u64 xu[S::E];
+    load_c<LOGN, K>(xu, ct + ((size_t)c * 2 + k) * N, tid);
 #pragma unroll
-  for (int e = 0; e < S::E; ++e) x[e] = reduce_any(x[e], P);
-  ntt_fwd<LOGN, K>(x, sm, tid, tb, P);
+    for (int e = 0; e < S::E; ++e) x[e] = u2d(reduce_any(xu[e], P));
+  }
+  ntt_fwd_d<LOGN, K>(x, sm, tid, tb, P);  // unreduced, |x| < 2^51
   if constexpr (S::NP == 0) __syncthreads();
   z_to_c<LOGN, K>(x, sm, tid);
 #pragma unroll 1
   for (int f = 0; f < n_w; ++f) {
-    u64 y[S::E];
+    double y[S::E];
 #pragma unroll
-    for (int e = 0; e < S::E; ++e)
-      y[e] = mulmod(x[e], reduce_any(w_hat[(size_t)f * N + posC<LOGN, K>(tid, e)], P), P);
+    for (int e = 0; e < S::E; ++e) {
+      const double w = u2d(reduce_any(w_hat[(size_t)f * N + posC<LOGN, K>(tid, e)], P));
+      y[e] = fmulmod(x[e], w, __dmul_rn(w, P.qinv_d), P.qd);
+    }
     __syncthreads();  // the previous filter's INTT is done with shared memory
     c_to_z<LOGN, K>(y, sm, tid);
-    ntt_inv<LOGN, K>(y, sm, tid, tb, P);
-    store_c<LOGN, K>(y, out + (((size_t)c * n_w + f) * 2 + k) * N, tid);
+    u64 yu[S::E];
+    ntt_inv_d<LOGN, K>(y, yu, sm, tid, tb, P);
+    store_c<LOGN, K>(yu, out + (((size_t)c * n_w + f) * 2 + k) * N, tid);
   }
 }
 
-// One warp per ciphertext.
+// One warp per ciphertext.  Products are summed as exact 128-bit integers
+// (residues below 2^52, at most N / 32 <= 512 terms a lane: below 2^113) and
+// reduced once per lane.
 __global__ void k_decrypt_coef0(long long* __restrict__ out, const u64* __restrict__ ct,
                                 const u64* __restrict__ s, long long n_ct, int log_n, PrimeInfo P) {
   const long long c = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -54,9 +73,14 @@ __global__ void k_decrypt_coef0(long long* __restrict__ out, const u64* __restri
   const int n = 1 << log_n;
   const u64* b = ct + (size_t)c * 2 * n;
   const u64* a = b + n;
-  u64 acc = 0;  // sum_{i >= 1} a_i s_{N-i}
-  for (int i = lane; i < n; i += 32)
-    if (i) acc = addmod(acc, mulmod(reduce_any(a[i], P), reduce_any(s[n - i], P), P), P.q);
+  u64 lo = 0, hi = 0;  // sum_{i >= 1} a_i s_{N-i}
+  for (int i = lane ? lane : 32; i < n; i += 32) {
+    const u64 av = ld_stream(a + i), sv = s[n - i];
+    const u64 pl = av * sv;
+    lo += pl;
+    hi += __umul64hi(av, sv) + (lo < pl ? 1ull : 0ull);
+  }
+  u64 acc = addmod(reduce_any(lo, P), mulmod(reduce_any(hi, P), P.r_mod, P), P.q);
 #pragma unroll
   for (int off = 16; off; off >>= 1) acc = addmod(acc, __shfl_down_sync(0xffffffffu, acc, off), P.q);
   if (lane == 0) {

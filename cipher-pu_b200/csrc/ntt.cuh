@@ -292,16 +292,15 @@ __device__ __forceinline__ void ntt_fwd(u64 (&x)[1 << K], u64* sm, int tid, cons
   for (int e = 0; e < (1 << K); ++e) x[e] = d2canon(d[e], P.qd, P.qinv_d);
 }
 
-// Inverse NTT (with N^-1): layout Z in (canonical), layout C out, canonical.
+// Inverse NTT (with N^-1) on exact doubles: layout Z in (|d| <= 1.5 q),
+// layout C out in x, canonical.  Each stage adds at most q to the magnitude,
+// so |d| stays below (1.5 + log N) q < 2^51 for q < 2^47.
 template <int LOGN, int K>
-__device__ __forceinline__ void ntt_inv(u64 (&x)[1 << K], u64* sm, int tid, const TwD* __restrict__ tb,
-                                        const PrimeInfo& P, bool cyclic = false) {
+__device__ __forceinline__ void ntt_inv_d(double (&d)[1 << K], u64 (&x)[1 << K], u64* sm, int tid,
+                                          const TwD* __restrict__ tb, const PrimeInfo& P, bool cyclic = false) {
   constexpr int N = 1 << LOGN;
   const TwD* itw = tb + (cyclic ? TWF_INV_CYC : TWF_INV) * N;
   const TwD* post = tb + (cyclic ? TWF_POST_CYC : TWF_POST) * N;
-  double d[1 << K];
-#pragma unroll
-  for (int e = 0; e < (1 << K); ++e) d[e] = u2d(x[e]);
   double* smd = reinterpret_cast<double*>(sm);
   InvRest<LOGN, K, NttShape<LOGN, K>::NP>::run(d, smd, tid, itw, P.qd);
   inv_pass<LOGN, K, 0, K>(d, tid, itw, P.qd);
@@ -310,6 +309,16 @@ __device__ __forceinline__ void ntt_inv(u64 (&x)[1 << K], u64* sm, int tid, cons
     const TwD pw = ldtwd(post + posC<LOGN, K>(tid, e));
     x[e] = d2canon(fmulmod(d[e], pw.w, pw.wq, P.qd), P.qd, P.qinv_d);
   }
+}
+
+// Inverse NTT (with N^-1): layout Z in (canonical), layout C out, canonical.
+template <int LOGN, int K>
+__device__ __forceinline__ void ntt_inv(u64 (&x)[1 << K], u64* sm, int tid, const TwD* __restrict__ tb,
+                                        const PrimeInfo& P, bool cyclic = false) {
+  double d[1 << K];
+#pragma unroll
+  for (int e = 0; e < (1 << K); ++e) d[e] = u2d(x[e]);
+  ntt_inv_d<LOGN, K>(d, x, sm, tid, tb, P, cyclic);
 }
 
 // Layout-Z global access: the last pass has unit stride inside each run, so

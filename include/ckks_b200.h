@@ -472,7 +472,8 @@ int ckks_mul_plain_multi(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct,
 /*
  * Constant coefficient of the decryption (b - a s) mod q of each ciphertext
  * of ct [n_ct][2][N] (coefficient domain), centred to (-q/2, q/2] (q odd),
- * with s the N residues of the secret key mod q = primes[prime].  Replaces
+ * with s the N residues of the secret key mod q = primes[prime]; the a and s
+ * words must be below 2^52 (residues in [0, q) are).  Replaces
  * dec[0] of scripts/exp_e24_rotation_bootstrap.py:109 decrypt_exact, the one
  * coefficient :263 inner_product and :278 coef_sum read.
  */
