@@ -235,7 +235,10 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   constexpr int T = Sh::T;
   u64* acc0s = sm + Sh::SMEM_WORDS;
   u64* acc1s = acc0s + N;
-  const int ti = blockIdx.x / n_ct;  // target-major: resident CTAs share one prime
+  // target-major (resident CTAs share one prime), special prime first: its
+  // CTAs transform every digit, one more than the others, so they go first
+  // and the shorter ones fill the last wave
+  const int ti = level - (int)(blockIdx.x / n_ct);
   const long long ct = blockIdx.x % n_ct;
   const bool special = ti == level;
   const int pidx = special ? nq : ti;
