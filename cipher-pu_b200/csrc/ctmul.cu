@@ -307,8 +307,13 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 }
 
 // ---------------------------------------------------------------- kernel C
-// One CTA per (ct, poly k).  The centred special-prime accumulator v and the
-// rescale limb w are kept in thread-private shared-memory slots (layout C).
+// One CTA per (ct, poly k), all in FP64 on exact doubles: the special-prime
+// part v and the rescale limb w are kept centred (signed, |v| <= p / 2,
+// |w| <= q_t / 2) in thread-private shared-memory slots (layout C), so they
+// lift to any prime as they are.  Products by p^-1 and q_t^-1 are fmulmod
+// with w / q correctly rounded (|result| <= q).  Bounds: the forward
+// transform gets |x| < 2 q_i (q_t < 2 q_i) and returns |x| < 13.75 q; the
+// combination stays below 16 q < 2^51; the inverses get |x| <= 1.5 q.
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_down(CmScratch S, u64* __restrict__ out, int level, int nq,
@@ -318,8 +323,8 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
   constexpr int T = Sh::T;
-  u64* vs = sm + Sh::SMEM_WORDS;
-  u64* ws = vs + N;
+  double* vs = reinterpret_cast<double*>(sm + Sh::SMEM_WORDS);
+  double* ws = vs + N;
   const long long ct = blockIdx.x >> 1;
   const int k = blockIdx.x & 1;
   const int t = level - 1;
@@ -331,53 +336,56 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   const u64* ak = S.acc + ct * 2 * LN + (size_t)k * LN;
   u64* ok = out + ((size_t)ct * 2 + k) * (size_t)t * N;
 
+  double d[Sh::E];
   u64 x[Sh::E];
   load_c<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
-  c_to_z<LOGN, K>(x, sm, tid);
-  ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, nq), PP);
 #pragma unroll
-  for (int e = 0; e < Sh::E; ++e) vs[e * T + tid] = x[e];
+  for (int e = 0; e < Sh::E; ++e) d[e] = u2d(x[e]);
+  c_to_z<LOGN, K>(d, sm, tid);
+  ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, nq), PP);
+#pragma unroll
+  for (int e = 0; e < Sh::E; ++e) vs[e * T + tid] = x[e] > PP.half ? u2d(x[e]) - PP.qd : u2d(x[e]);
   // Rescale limb t in the coefficient domain without a transform of v:
-  // w = INTT_t(d_t + acc_t P^-1) - [v]_t P^-1, equal mod q_t to
-  // INTT_t(d_t + (acc_t - NTT_t([v]_t)) P^-1) by linearity of the NTT.
-  const TwPair pt = pinv[t];
+  // w = INTT_t(d_t + acc_t p^-1) - v p^-1, equal mod q_t to
+  // INTT_t(d_t + (acc_t - NTT_t([v]_t)) p^-1) by linearity of the NTT.
+  const double ptw = (double)pinv[t].w;
+  const double ptq = __ddiv_rn(ptw, PT.qd);
   {
     u64 dv[Sh::E];
     load_c<LOGN, K>(dv, dk + (size_t)t * N, tid);
     load_c<LOGN, K>(x, ak + (size_t)t * N, tid);
 #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) x[e] = addmod(dv[e], shoup(x[e], pt.w, pt.ws, PT.q), PT.q);
+    for (int e = 0; e < Sh::E; ++e) {
+      const double dc = dv[e] > PT.half ? u2d(dv[e]) - PT.qd : u2d(dv[e]);
+      d[e] = __dadd_rn(fmulmod(u2d(x[e]), ptw, ptq, PT.qd), dc);
+    }
   }
-  c_to_z<LOGN, K>(x, sm, tid);
-  ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, t), PT);
+  c_to_z<LOGN, K>(d, sm, tid);
+  ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, t), PT);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) {
-    const u64 v = vs[e * T + tid];
-    const u64 vt = v > PP.half ? v - PP.q + PT.q : v;
-    ws[e * T + tid] = submod(x[e], shoup(vt, pt.w, pt.ws, PT.q), PT.q);
+    const u64 w = d2canon(__dadd_rn(u2d(x[e]), -fmulmod(vs[e * T + tid], ptw, ptq, PT.qd)), PT.qd, PT.qinv_d);
+    ws[e * T + tid] = w > PT.half ? u2d(w) - PT.qd : u2d(w);
   }
 #pragma unroll 1
   for (int i = 0; i < t; ++i) {
     const PrimeInfo P = pi[i];
-    const TwPair pv = pinv[i];
-    const TwPair ci = qtinv[(size_t)t * nq + i];
+    const double pvw = (double)pinv[i].w;
+    const double pvq = __ddiv_rn(pvw, P.qd);
+    const double ciw = (double)qtinv[(size_t)t * nq + i].w;
+    const double ciq = __ddiv_rn(ciw, P.qd);
 #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) {
-      const u64 v = vs[e * T + tid];
-      const u64 w = ws[e * T + tid];
-      const u64 vi = v > PP.half ? v - PP.q + P.q : v;
-      const u64 wi = w > PT.half ? w - PT.q + P.q : w;
-      x[e] = shoup_lazy(vi, pv.w, pv.ws, P.q) + wi;  // [0, 3q)
-    }
-    ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
-    z_to_c<LOGN, K>(x, sm, tid);
+    for (int e = 0; e < Sh::E; ++e)
+      d[e] = __dadd_rn(fmulmod(vs[e * T + tid], pvw, pvq, P.qd), ws[e * T + tid]);  // |.| < 2 q_i
+    ntt_fwd_d<LOGN, K>(d, sm, tid, twbase<LOGN>(tw, i), P);
+    z_to_c<LOGN, K>(d, sm, tid);
     u64 dv[Sh::E], av[Sh::E];
     load_c<LOGN, K>(dv, dk + (size_t)i * N, tid);
     load_c<LOGN, K>(av, ak + (size_t)i * N, tid);
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) {
-      const u64 s = dv[e] + shoup_lazy(av[e], pv.w, pv.ws, P.q) + P.qlazy - x[e];  // (0, 35q)
-      x[e] = shoup(s, ci.w, ci.ws, P.q);
+      const double sd = __dadd_rn(__dadd_rn(u2d(dv[e]), fmulmod(u2d(av[e]), pvw, pvq, P.qd)), -d[e]);
+      x[e] = d2canon(fmulmod(sd, ciw, ciq, P.qd), P.qd, P.qinv_d);
     }
     store_c<LOGN, K>(x, ok + (size_t)i * N, tid);
   }
