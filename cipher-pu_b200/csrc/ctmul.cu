@@ -424,7 +424,8 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 }
 
 // kernel R3: one CTA per (ct, poly k): v = centred INTT_p(acc_k,p); every
-// limb i: out_k,i = [k == 0] psi(c0)_i + (acc_k,i - NTT_i([v]_i)) p^-1.
+// limb i: out_k,i = [k == 0] psi(c0)_i + (acc_k,i - NTT_i(v)) p^-1, in FP64
+// like kernel C (v kept signed in shared memory; |v| < q_i since p < 2 q_i).
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_ks_down(CmScratch S, u64* __restrict__ out, int level, int nq, const PrimeInfo* __restrict__ pi,
@@ -433,7 +434,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
   constexpr int T = Sh::T;
-  u64* vs = sm + Sh::SMEM_WORDS;
+  double* vs = reinterpret_cast<double*>(sm + Sh::SMEM_WORDS);
   const long long ct = blockIdx.x >> 1;
   const int k = blockIdx.x & 1;
   const int tid = threadIdx.x;
@@ -442,35 +443,35 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   const u64* d0 = S.d01 + ct * 2 * LN;
   const u64* ak = S.acc + ct * 2 * LN + (size_t)k * LN;
   u64* ok = out + ((size_t)ct * 2 + k) * LN;
+  double d[Sh::E];
   u64 x[Sh::E];
   load_c<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
-  c_to_z<LOGN, K>(x, sm, tid);
-  ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, nq), PP);
 #pragma unroll
-  for (int e = 0; e < Sh::E; ++e) vs[e * T + tid] = x[e];
+  for (int e = 0; e < Sh::E; ++e) d[e] = u2d(x[e]);
+  c_to_z<LOGN, K>(d, sm, tid);
+  ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, nq), PP);
+#pragma unroll
+  for (int e = 0; e < Sh::E; ++e) vs[e * T + tid] = x[e] > PP.half ? u2d(x[e]) - PP.qd : u2d(x[e]);
 #pragma unroll 1
   for (int i = 0; i < level; ++i) {
     const PrimeInfo P = pi[i];
-    const TwPair pv = pinv[i];
+    const double pvw = (double)pinv[i].w;
+    const double pvq = __ddiv_rn(pvw, P.qd);
 #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) {
-      const u64 v = vs[e * T + tid];
-      x[e] = v > PP.half ? v - PP.q + P.q : v;
-    }
-    ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
-    z_to_c<LOGN, K>(x, sm, tid);
+    for (int e = 0; e < Sh::E; ++e) d[e] = vs[e * T + tid];
+    ntt_fwd_d<LOGN, K>(d, sm, tid, twbase<LOGN>(tw, i), P);  // |d| < 13.75 q
+    z_to_c<LOGN, K>(d, sm, tid);
     u64 av[Sh::E];
     load_c<LOGN, K>(av, ak + (size_t)i * N, tid);
+#pragma unroll
+    for (int e = 0; e < Sh::E; ++e) d[e] = fmulmod(__dadd_rn(u2d(av[e]), -d[e]), pvw, pvq, P.qd);
     if (k == 0) {
-      u64 dv[Sh::E];
-      load_c<LOGN, K>(dv, d0 + (size_t)i * N, tid);
+      load_c<LOGN, K>(av, d0 + (size_t)i * N, tid);
 #pragma unroll
-      for (int e = 0; e < Sh::E; ++e)
-        x[e] = addmod(dv[e], shoup(av[e] + P.qlazy - x[e], pv.w, pv.ws, P.q), P.q);
-    } else {
-#pragma unroll
-      for (int e = 0; e < Sh::E; ++e) x[e] = shoup(av[e] + P.qlazy - x[e], pv.w, pv.ws, P.q);
+      for (int e = 0; e < Sh::E; ++e) d[e] = __dadd_rn(d[e], u2d(av[e]));
     }
+#pragma unroll
+    for (int e = 0; e < Sh::E; ++e) x[e] = d2canon(d[e], P.qd, P.qinv_d);
     store_c<LOGN, K>(x, ok + (size_t)i * N, tid);
   }
 }

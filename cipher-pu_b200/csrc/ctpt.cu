@@ -26,7 +26,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, (CtptBlocks<LOGN, K>::va
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
   constexpr int T = Sh::T;
-  u64* ws = sm + Sh::SMEM_WORDS;
+  double* ws = reinterpret_cast<double*>(sm + Sh::SMEM_WORDS);
   const long long c = blockIdx.x >> 1;
   const int k = blockIdx.x & 1;
   const int t = level - 1;
@@ -36,33 +36,33 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, (CtptBlocks<LOGN, K>::va
   const u64* p = pt + (size_t)c * pt_stride * LN;
   u64* o = out + (c * 2 + k) * (size_t)t * N;
   const PrimeInfo PT = pi[t];
+  // FP64 throughout: products by fmulmod_var (|.| < 0.6 q), the rescale limb
+  // w kept centred and signed (|w| <= q_t / 2 < q_i), q_t^-1 by fmulmod.
+  double d[Sh::E];
   u64 x[Sh::E], y[Sh::E];
   load_c<LOGN, K>(x, a + (size_t)t * N, tid);
   load_c<LOGN, K>(y, p + (size_t)t * N, tid);
 #pragma unroll
-  for (int e = 0; e < Sh::E; ++e) x[e] = mulmod(x[e], y[e], PT);
-  c_to_z<LOGN, K>(x, sm, tid);
-  ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, t), PT);
+  for (int e = 0; e < Sh::E; ++e) d[e] = fmulmod_var(u2d(x[e]), u2d(y[e]), PT.qd, PT.qinv_d);
+  c_to_z<LOGN, K>(d, sm, tid);
+  ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, t), PT);
 #pragma unroll
-  for (int e = 0; e < Sh::E; ++e) ws[e * T + tid] = x[e];
+  for (int e = 0; e < Sh::E; ++e) ws[e * T + tid] = x[e] > PT.half ? u2d(x[e]) - PT.qd : u2d(x[e]);
 #pragma unroll 1
   for (int i = 0; i < t; ++i) {
     const PrimeInfo P = pi[i];
-    const TwPair ci = qtinv[(size_t)t * nq + i];
+    const double ciw = (double)qtinv[(size_t)t * nq + i].w;
+    const double ciq = __ddiv_rn(ciw, P.qd);
+#pragma unroll
+    for (int e = 0; e < Sh::E; ++e) d[e] = ws[e * T + tid];
+    ntt_fwd_d<LOGN, K>(d, sm, tid, twbase<LOGN>(tw, i), P);  // |d| < 13.75 q
+    z_to_c<LOGN, K>(d, sm, tid);
+    load_c<LOGN, K>(x, a + (size_t)i * N, tid);
+    load_c<LOGN, K>(y, p + (size_t)i * N, tid);
 #pragma unroll
     for (int e = 0; e < Sh::E; ++e) {
-      const u64 w = ws[e * T + tid];
-      x[e] = w > PT.half ? w - PT.q + P.q : w;
-    }
-    ntt_fwd<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, i), P);
-    z_to_c<LOGN, K>(x, sm, tid);
-    load_c<LOGN, K>(y, a + (size_t)i * N, tid);
-    u64 pv[Sh::E];
-    load_c<LOGN, K>(pv, p + (size_t)i * N, tid);
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e) {
-      const u64 xi = mulmod(y[e], pv[e], P);
-      x[e] = shoup(xi + P.qlazy - x[e], ci.w, ci.ws, P.q);
+      const double sd = __dadd_rn(fmulmod_var(u2d(x[e]), u2d(y[e]), P.qd, P.qinv_d), -d[e]);
+      x[e] = d2canon(fmulmod(sd, ciw, ciq, P.qd), P.qd, P.qinv_d);
     }
     store_c<LOGN, K>(x, o + (size_t)i * N, tid);
   }
