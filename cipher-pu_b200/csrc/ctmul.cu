@@ -215,8 +215,8 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) m2[e] = d2canon(m2d[e], P.qd, P.qinv_d);
   store_c<LOGN, K>(m2, S.d2n + ct * LN + (size_t)j * N, tid);
-  c_to_z<LOGN, K>(m2, sm, tid);
-  ntt_inv<LOGN, K>(m2, sm, tid, twbase<LOGN>(tw, j), P);
+  c_to_z<LOGN, K>(m2d, sm, tid);  // |m2d| < 0.6 q: straight into the FP64 inverse
+  ntt_inv_d<LOGN, K>(m2d, m2, sm, tid, twbase<LOGN>(tw, j), P);
   store_c<LOGN, K>(m2, S.d2c + ct * LN + (size_t)j * N, tid);
 }
 
