@@ -8,9 +8,9 @@ polynomial limb, so the buckets of different shapes need no padding).  The
 buckets are spread over a pool of streams and the whole plan is captured
 once into a CUDA graph, so a step costs one graph launch.  The autotuner
 times every bucket alone under each launch shape (per-thread radix 2^K, K = 2..5,
-balanced or tight register budget, chunking of the bucket into
-launches) and keeps the fastest; the choice is baked into the graph at
-capture time.
+balanced or tight register budget, limbs / work units per CTA, chunking of
+the bucket into launches) and keeps the fastest; the choice is baked into the
+graph at capture time.
 
 The reference's batching is time multiplexing of four poly-mult instances on
 one FPGA (rtl/m4/e2e_ckks_mult_ctrl_m4.sv:368-482, TIME_MULT = 4 in
@@ -57,11 +57,13 @@ class Bucket:
     b: torch.Tensor = None          # second ciphertext (ctct) or plaintext (ctpt)
     out: torch.Tensor = None
     scratch: torch.Tensor = None
-    tune: dict = field(default_factory=lambda: {"k": 0, "minb": 0, "chunk": 0})
+    tune: dict = field(default_factory=lambda: {"k": 0, "minb": 0, "chunk": 0, "upc": 0})
 
 
 # Per-thread radix 2^K the autotuner sweeps (K = log2 coefficients per thread).
 RADIX_LOG2 = (2, 3, 4, 5)
+# Work units (limbs, target primes, output polynomials) per CTA of the ct-mult kernels.
+UNITS_PER_CTA = (1, 2, 4)
 
 
 def cm_shape_built(log_n: int, k: int, minb: int) -> bool:
@@ -115,6 +117,7 @@ class BatchExecutor:
         if bk.shape.op == "ctct":
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 0, bk.tune["k"])
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 1, bk.tune["minb"])
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 4, bk.tune.get("upc", 0))
             # buckets already overlap on the executor's streams: one sub-batch per call
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 1)
             for s in range(0, bk.count, chunk):
@@ -126,6 +129,7 @@ class BatchExecutor:
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 0, 0)
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 1, 0)
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 0)
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 4, 0)
         else:
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 3, bk.tune["k"])
             for s in range(0, bk.count, chunk):
@@ -185,13 +189,14 @@ class BatchExecutor:
         choices = {}
         for bk in self.buckets:
             log_n = bk.shape.log_n
-            cands = [{"k": 0, "minb": 0, "chunk": 0}]  # the library's default shape first
+            cands = [{"k": 0, "minb": 0, "chunk": 0, "upc": 0}]  # the library's default shape first
             if bk.shape.op == "ctct":
-                cands += [{"k": k, "minb": mb, "chunk": ch}
-                          for k, mb, ch in itertools.product(RADIX_LOG2, (1, 2), (0, 128))
+                cands += [{"k": k, "minb": mb, "chunk": ch, "upc": u}
+                          for k, mb, ch, u in itertools.product(RADIX_LOG2, (1, 2), (0, 128), UNITS_PER_CTA)
                           if cm_shape_built(log_n, k, mb) and not (ch and ch >= bk.count)]
             else:
-                cands += [{"k": k, "minb": 0, "chunk": 0} for k in RADIX_LOG2 if ((1 << log_n) >> k) <= 1024]
+                cands += [{"k": k, "minb": 0, "chunk": 0, "upc": 0} for k in RADIX_LOG2
+                          if ((1 << log_n) >> k) <= 1024]
             best = None
             sweep = {}
             default_ms = None
@@ -207,7 +212,7 @@ class BatchExecutor:
                 e1.record()
                 torch.cuda.synchronize()
                 t = e0.elapsed_time(e1) / reps
-                sweep[f"K{c['k']}/b{c['minb']}/c{c['chunk']}"] = round(t, 4)
+                sweep[f"K{c['k']}/b{c['minb']}/c{c['chunk']}/u{c['upc']}"] = round(t, 4)
                 if c is cands[0]:
                     default_ms = t
                 if best is None or t < best[0]:

@@ -177,47 +177,54 @@ static int dispatch_cm(int log_n, int kreq, int mreq, F&& f, const char* fn) {
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_tensor(const u64* __restrict__ A, const u64* __restrict__ B, CmScratch S, int level,
-                const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct) {
+                const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct,
+                long long n_units, int upc) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
-  const int j = blockIdx.x / n_ct;  // limb-major: resident CTAs share q_j's tables
-  const long long ct = blockIdx.x % n_ct;
-  const int tid = threadIdx.x;
-  const PrimeInfo P = pi[j];
-  const size_t LN = (size_t)level * N;
-  const u64* a0 = A + ct * 2 * LN + (size_t)j * N;
-  const u64* b0 = B + ct * 2 * LN + (size_t)j * N;
-  u64* d0 = S.d01 + ct * 2 * LN + (size_t)j * N;
-  // Products in FP64 (exact two-product + rounded quotient, fmulmod_var):
-  // d2 = a1 b1, d0 = a0 b0, d1 = (a0 + a1)(b0 + b1) - d0 - d2, each partial
-  // result below 2^48 in magnitude, reduced to [0, q) once at the end.
-  u64 x[Sh::E], y[Sh::E];
-  load_c<LOGN, K>(x, a0 + LN, tid);
-  load_c<LOGN, K>(y, b0 + LN, tid);
-  double m2d[Sh::E];
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) m2d[e] = fmulmod_var(u2d(x[e]), u2d(y[e]), P.qd, P.qinv_d);
-  u64 a0v[Sh::E], b0v[Sh::E];
-  load_c<LOGN, K>(a0v, a0, tid);
-  load_c<LOGN, K>(b0v, b0, tid);
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) {
-    const double a0d = u2d(a0v[e]), b0d = u2d(b0v[e]);
-    const double m0 = fmulmod_var(a0d, b0d, P.qd, P.qinv_d);
-    const double s1 = fmulmod_var(__dadd_rn(a0d, u2d(x[e])), __dadd_rn(b0d, u2d(y[e])), P.qd, P.qinv_d);
-    a0v[e] = d2canon(m0, P.qd, P.qinv_d);
-    b0v[e] = d2canon(__dadd_rn(__dadd_rn(s1, -m0), -m2d[e]), P.qd, P.qinv_d);  // |.| < 3 2^48
+  // `upc` work units per CTA, consecutive in the unit order
+  for (int r = 0; r < upc; ++r) {
+    const long long unit = (long long)blockIdx.x * upc + r;
+    if (unit >= n_units) return;  // uniform across the CTA
+    if (r) __syncthreads();       // the previous unit is done with shared memory
+    const int j = unit / n_ct;  // limb-major: resident CTAs share q_j's tables
+    const long long ct = unit % n_ct;
+    const int tid = threadIdx.x;
+    const PrimeInfo P = pi[j];
+    const size_t LN = (size_t)level * N;
+    const u64* a0 = A + ct * 2 * LN + (size_t)j * N;
+    const u64* b0 = B + ct * 2 * LN + (size_t)j * N;
+    u64* d0 = S.d01 + ct * 2 * LN + (size_t)j * N;
+    // Products in FP64 (exact two-product + rounded quotient, fmulmod_var):
+    // d2 = a1 b1, d0 = a0 b0, d1 = (a0 + a1)(b0 + b1) - d0 - d2, each partial
+    // result below 2^48 in magnitude, reduced to [0, q) once at the end.
+    u64 x[Sh::E], y[Sh::E];
+    load_c<LOGN, K>(x, a0 + LN, tid);
+    load_c<LOGN, K>(y, b0 + LN, tid);
+    double m2d[Sh::E];
+  #pragma unroll
+    for (int e = 0; e < Sh::E; ++e) m2d[e] = fmulmod_var(u2d(x[e]), u2d(y[e]), P.qd, P.qinv_d);
+    u64 a0v[Sh::E], b0v[Sh::E];
+    load_c<LOGN, K>(a0v, a0, tid);
+    load_c<LOGN, K>(b0v, b0, tid);
+  #pragma unroll
+    for (int e = 0; e < Sh::E; ++e) {
+      const double a0d = u2d(a0v[e]), b0d = u2d(b0v[e]);
+      const double m0 = fmulmod_var(a0d, b0d, P.qd, P.qinv_d);
+      const double s1 = fmulmod_var(__dadd_rn(a0d, u2d(x[e])), __dadd_rn(b0d, u2d(y[e])), P.qd, P.qinv_d);
+      a0v[e] = d2canon(m0, P.qd, P.qinv_d);
+      b0v[e] = d2canon(__dadd_rn(__dadd_rn(s1, -m0), -m2d[e]), P.qd, P.qinv_d);  // |.| < 3 2^48
+    }
+    store_c<LOGN, K>(a0v, d0, tid);
+    store_c<LOGN, K>(b0v, d0 + LN, tid);
+    u64 m2[Sh::E];
+  #pragma unroll
+    for (int e = 0; e < Sh::E; ++e) m2[e] = d2canon(m2d[e], P.qd, P.qinv_d);
+    store_c<LOGN, K>(m2, S.d2n + ct * LN + (size_t)j * N, tid);
+    c_to_z<LOGN, K>(m2d, sm, tid);  // |m2d| < 0.6 q: straight into the FP64 inverse
+    ntt_inv_d<LOGN, K>(m2d, m2, sm, tid, twbase<LOGN>(tw, j), P);
+    store_c<LOGN, K>(m2, S.d2c + ct * LN + (size_t)j * N, tid);
   }
-  store_c<LOGN, K>(a0v, d0, tid);
-  store_c<LOGN, K>(b0v, d0 + LN, tid);
-  u64 m2[Sh::E];
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) m2[e] = d2canon(m2d[e], P.qd, P.qinv_d);
-  store_c<LOGN, K>(m2, S.d2n + ct * LN + (size_t)j * N, tid);
-  c_to_z<LOGN, K>(m2d, sm, tid);  // |m2d| < 0.6 q: straight into the FP64 inverse
-  ntt_inv_d<LOGN, K>(m2d, m2, sm, tid, twbase<LOGN>(tw, j), P);
-  store_c<LOGN, K>(m2, S.d2c + ct * LN + (size_t)j * N, tid);
 }
 
 // ---------------------------------------------------------------- kernel B
@@ -228,7 +235,8 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_modup(CmScratch S, const double* __restrict__ key, int level, int nq,
-               const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct) {
+               const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct,
+                long long n_units, int upc) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
@@ -238,71 +246,77 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   // target-major (resident CTAs share one prime), special prime first: its
   // CTAs transform every digit, one more than the others, so they go first
   // and the shorter ones fill the last wave
-  const int ti = level - (int)(blockIdx.x / n_ct);
-  const long long ct = blockIdx.x % n_ct;
-  const bool special = ti == level;
-  const int pidx = special ? nq : ti;
-  const int tid = threadIdx.x;
-  const PrimeInfo P = pi[pidx];
-  const size_t LN = (size_t)level * N;
-  const TwD* tb = twbase<LOGN>(tw, pidx);
-  double* acc0s_d = reinterpret_cast<double*>(acc0s);
-  double* acc1s_d = reinterpret_cast<double*>(acc1s);
-#pragma unroll 1
-  for (int j = 0; j < level; ++j) {
-    // digit j as exact doubles in layout C: its evaluation-domain residues at
-    // its own prime, else its coefficient residues (< q_j < 2 q_i) transformed
-    // unreduced (|x| < 2^51 on return, fine for fmulmod)
-    double x[Sh::E];
-    u64 xu[Sh::E];
-    if (!special && j == ti) {
-      load_c<LOGN, K>(xu, S.d2n + ct * LN + (size_t)j * N, tid);
-#pragma unroll
-      for (int e = 0; e < Sh::E; ++e) x[e] = u2d(xu[e]);
-    } else {
-      load_c<LOGN, K>(xu, S.d2c + ct * LN + (size_t)j * N, tid);
-#pragma unroll
-      for (int e = 0; e < Sh::E; ++e) x[e] = u2d(xu[e]);
-      ntt_fwd_d<LOGN, K>(x, sm, tid, tb, P);
-      z_to_c<LOGN, K>(x, sm, tid);
-    }
-    // key inner product in exact FP64 on the key values alone (8 bytes per
-    // word): w / q is formed as w * (1/q), two roundings off, so the quotient
-    // estimate may miss by one and each product lands within 1.5 q (still
-    // exact: every intermediate is an integer below 2^53); the running sum is
-    // folded back below q / 2 + 1 every 16 digits so it stays exact
-#pragma unroll 1
-    for (int kk = 0; kk < 2; ++kk) {
-      const double* kp = reinterpret_cast<const double*>(key) + (((size_t)j * 2 + kk) * (nq + 1) + pidx) * (2 * N);
-      double* acc = kk ? acc1s_d : acc0s_d;
-      const bool fold = (j & 15) == 15;
-#pragma unroll
-      for (int e = 0; e < Sh::E; ++e) {
-        const double w = ld_stream_d(kp + posC<LOGN, K>(tid, e));
-        const int s = e * T + tid;
-        const double t = fmulmod(x[e], w, __dmul_rn(w, P.qinv_d), P.qd);
-        double a = j == 0 ? t : __dadd_rn(acc[s], t);
-        if (fold) {
-          const double qt = __dadd_rn(__fma_rn(a, P.qinv_d, CKKS_FP_MAGIC), -CKKS_FP_MAGIC);
-          a = __fma_rn(-qt, P.qd, a);
+  // `upc` work units per CTA, consecutive in the unit order
+  for (int r = 0; r < upc; ++r) {
+    const long long unit = (long long)blockIdx.x * upc + r;
+    if (unit >= n_units) return;  // uniform across the CTA
+    if (r) __syncthreads();       // the previous unit is done with shared memory
+    const int ti = level - (int)(unit / n_ct);
+    const long long ct = unit % n_ct;
+    const bool special = ti == level;
+    const int pidx = special ? nq : ti;
+    const int tid = threadIdx.x;
+    const PrimeInfo P = pi[pidx];
+    const size_t LN = (size_t)level * N;
+    const TwD* tb = twbase<LOGN>(tw, pidx);
+    double* acc0s_d = reinterpret_cast<double*>(acc0s);
+    double* acc1s_d = reinterpret_cast<double*>(acc1s);
+  #pragma unroll 1
+    for (int j = 0; j < level; ++j) {
+      // digit j as exact doubles in layout C: its evaluation-domain residues at
+      // its own prime, else its coefficient residues (< q_j < 2 q_i) transformed
+      // unreduced (|x| < 2^51 on return, fine for fmulmod)
+      double x[Sh::E];
+      u64 xu[Sh::E];
+      if (!special && j == ti) {
+        load_c<LOGN, K>(xu, S.d2n + ct * LN + (size_t)j * N, tid);
+  #pragma unroll
+        for (int e = 0; e < Sh::E; ++e) x[e] = u2d(xu[e]);
+      } else {
+        load_c<LOGN, K>(xu, S.d2c + ct * LN + (size_t)j * N, tid);
+  #pragma unroll
+        for (int e = 0; e < Sh::E; ++e) x[e] = u2d(xu[e]);
+        ntt_fwd_d<LOGN, K>(x, sm, tid, tb, P);
+        z_to_c<LOGN, K>(x, sm, tid);
+      }
+      // key inner product in exact FP64 on the key values alone (8 bytes per
+      // word): w / q is formed as w * (1/q), two roundings off, so the quotient
+      // estimate may miss by one and each product lands within 1.5 q (still
+      // exact: every intermediate is an integer below 2^53); the running sum is
+      // folded back below q / 2 + 1 every 16 digits so it stays exact
+  #pragma unroll 1
+      for (int kk = 0; kk < 2; ++kk) {
+        const double* kp = reinterpret_cast<const double*>(key) + (((size_t)j * 2 + kk) * (nq + 1) + pidx) * (2 * N);
+        double* acc = kk ? acc1s_d : acc0s_d;
+        const bool fold = (j & 15) == 15;
+  #pragma unroll
+        for (int e = 0; e < Sh::E; ++e) {
+          const double w = ld_stream_d(kp + posC<LOGN, K>(tid, e));
+          const int s = e * T + tid;
+          const double t = fmulmod(x[e], w, __dmul_rn(w, P.qinv_d), P.qd);
+          double a = j == 0 ? t : __dadd_rn(acc[s], t);
+          if (fold) {
+            const double qt = __dadd_rn(__fma_rn(a, P.qinv_d, CKKS_FP_MAGIC), -CKKS_FP_MAGIC);
+            a = __fma_rn(-qt, P.qd, a);
+          }
+          acc[s] = a;
         }
-        acc[s] = a;
       }
     }
-  }
-  // Special-prime accumulators stay in the evaluation domain here; kernel C
-  // (one CTA per output polynomial) brings each back with one INTT, which
-  // keeps the per-CTA work of this kernel within one transform of each other.
-  u64 x[Sh::E];
-  u64* o = special ? S.accp + ct * 2 * N : S.acc + ct * 2 * LN + (size_t)ti * N;
-  const size_t kstride = special ? (size_t)N : LN;
-#pragma unroll 1
-  for (int k = 0; k < 2; ++k) {
-    const u64* a = k ? acc1s : acc0s;
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e)
-      x[e] = d2canon(reinterpret_cast<const double*>(a)[e * T + tid], P.qd, P.qinv_d);
-    store_c<LOGN, K>(x, o + (size_t)k * kstride, tid);
+    // Special-prime accumulators stay in the evaluation domain here; kernel C
+    // (one CTA per output polynomial) brings each back with one INTT, which
+    // keeps the per-CTA work of this kernel within one transform of each other.
+    u64 x[Sh::E];
+    u64* o = special ? S.accp + ct * 2 * N : S.acc + ct * 2 * LN + (size_t)ti * N;
+    const size_t kstride = special ? (size_t)N : LN;
+  #pragma unroll 1
+    for (int k = 0; k < 2; ++k) {
+      const u64* a = k ? acc1s : acc0s;
+  #pragma unroll
+      for (int e = 0; e < Sh::E; ++e)
+        x[e] = d2canon(reinterpret_cast<const double*>(a)[e * T + tid], P.qd, P.qinv_d);
+      store_c<LOGN, K>(x, o + (size_t)k * kstride, tid);
+    }
   }
 }
 
@@ -314,80 +328,87 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 // with w / q correctly rounded (|result| <= q).  Bounds: the forward
 // transform gets |x| < 2 q_i (q_t < 2 q_i) and returns |x| < 13.75 q; the
 // combination stays below 16 q < 2^51; the inverses get |x| <= 1.5 q.
-template <int LOGN, int K, int MINB>
+template <int LOGN, int K, int MINB, bool MULTI>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_down(CmScratch S, u64* __restrict__ out, int level, int nq,
               const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw,
-              const TwPair* __restrict__ pinv, const TwPair* __restrict__ qtinv) {
+              const TwPair* __restrict__ pinv, const TwPair* __restrict__ qtinv, long long n_units,
+              int upc) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
   constexpr int T = Sh::T;
   double* vs = reinterpret_cast<double*>(sm + Sh::SMEM_WORDS);
   double* ws = vs + N;
-  const long long ct = blockIdx.x >> 1;
-  const int k = blockIdx.x & 1;
-  const int t = level - 1;
-  const int tid = threadIdx.x;
-  const size_t LN = (size_t)level * N;
-  const PrimeInfo PP = pi[nq];
-  const PrimeInfo PT = pi[t];
-  const u64* dk = S.d01 + ct * 2 * LN + (size_t)k * LN;
-  const u64* ak = S.acc + ct * 2 * LN + (size_t)k * LN;
-  u64* ok = out + ((size_t)ct * 2 + k) * (size_t)t * N;
+  // `upc` work units per CTA, consecutive in the unit order
+  for (int r = 0; r < (MULTI ? upc : 1); ++r) {
+    const long long unit = (long long)blockIdx.x * upc + r;
+    if (MULTI && unit >= n_units) return;  // uniform across the CTA
+    if (r) __syncthreads();       // the previous unit is done with shared memory
+    const long long ct = unit >> 1;
+    const int k = unit & 1;
+    const int t = level - 1;
+    const int tid = threadIdx.x;
+    const size_t LN = (size_t)level * N;
+    const PrimeInfo PP = pi[nq];
+    const PrimeInfo PT = pi[t];
+    const u64* dk = S.d01 + ct * 2 * LN + (size_t)k * LN;
+    const u64* ak = S.acc + ct * 2 * LN + (size_t)k * LN;
+    u64* ok = out + ((size_t)ct * 2 + k) * (size_t)t * N;
 
-  double d[Sh::E];
-  u64 x[Sh::E];
-  load_c<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) d[e] = u2d(x[e]);
-  c_to_z<LOGN, K>(d, sm, tid);
-  ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, nq), PP);
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) vs[e * T + tid] = x[e] > PP.half ? u2d(x[e]) - PP.qd : u2d(x[e]);
-  // Rescale limb t in the coefficient domain without a transform of v:
-  // w = INTT_t(d_t + acc_t p^-1) - v p^-1, equal mod q_t to
-  // INTT_t(d_t + (acc_t - NTT_t([v]_t)) p^-1) by linearity of the NTT.
-  const double ptw = (double)pinv[t].w;
-  const double ptq = __ddiv_rn(ptw, PT.qd);
-  {
-    u64 dv[Sh::E];
-    load_c<LOGN, K>(dv, dk + (size_t)t * N, tid);
-    load_c<LOGN, K>(x, ak + (size_t)t * N, tid);
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e) {
-      const double dc = dv[e] > PT.half ? u2d(dv[e]) - PT.qd : u2d(dv[e]);
-      d[e] = __dadd_rn(fmulmod(u2d(x[e]), ptw, ptq, PT.qd), dc);
+    double d[Sh::E];
+    u64 x[Sh::E];
+    load_c<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
+  #pragma unroll
+    for (int e = 0; e < Sh::E; ++e) d[e] = u2d(x[e]);
+    c_to_z<LOGN, K>(d, sm, tid);
+    ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, nq), PP);
+  #pragma unroll
+    for (int e = 0; e < Sh::E; ++e) vs[e * T + tid] = x[e] > PP.half ? u2d(x[e]) - PP.qd : u2d(x[e]);
+    // Rescale limb t in the coefficient domain without a transform of v:
+    // w = INTT_t(d_t + acc_t p^-1) - v p^-1, equal mod q_t to
+    // INTT_t(d_t + (acc_t - NTT_t([v]_t)) p^-1) by linearity of the NTT.
+    const double ptw = (double)pinv[t].w;
+    const double ptq = __ddiv_rn(ptw, PT.qd);
+    {
+      u64 dv[Sh::E];
+      load_c<LOGN, K>(dv, dk + (size_t)t * N, tid);
+      load_c<LOGN, K>(x, ak + (size_t)t * N, tid);
+  #pragma unroll
+      for (int e = 0; e < Sh::E; ++e) {
+        const double dc = dv[e] > PT.half ? u2d(dv[e]) - PT.qd : u2d(dv[e]);
+        d[e] = __dadd_rn(fmulmod(u2d(x[e]), ptw, ptq, PT.qd), dc);
+      }
     }
-  }
-  c_to_z<LOGN, K>(d, sm, tid);
-  ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, t), PT);
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) {
-    const u64 w = d2canon(__dadd_rn(u2d(x[e]), -fmulmod(vs[e * T + tid], ptw, ptq, PT.qd)), PT.qd, PT.qinv_d);
-    ws[e * T + tid] = w > PT.half ? u2d(w) - PT.qd : u2d(w);
-  }
-#pragma unroll 1
-  for (int i = 0; i < t; ++i) {
-    const PrimeInfo P = pi[i];
-    const double pvw = (double)pinv[i].w;
-    const double pvq = __ddiv_rn(pvw, P.qd);
-    const double ciw = (double)qtinv[(size_t)t * nq + i].w;
-    const double ciq = __ddiv_rn(ciw, P.qd);
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e)
-      d[e] = __dadd_rn(fmulmod(vs[e * T + tid], pvw, pvq, P.qd), ws[e * T + tid]);  // |.| < 2 q_i
-    ntt_fwd_d<LOGN, K>(d, sm, tid, twbase<LOGN>(tw, i), P);
-    z_to_c<LOGN, K>(d, sm, tid);
-    u64 dv[Sh::E], av[Sh::E];
-    load_c<LOGN, K>(dv, dk + (size_t)i * N, tid);
-    load_c<LOGN, K>(av, ak + (size_t)i * N, tid);
-#pragma unroll
+    c_to_z<LOGN, K>(d, sm, tid);
+    ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, t), PT);
+  #pragma unroll
     for (int e = 0; e < Sh::E; ++e) {
-      const double sd = __dadd_rn(__dadd_rn(u2d(dv[e]), fmulmod(u2d(av[e]), pvw, pvq, P.qd)), -d[e]);
-      x[e] = d2canon(fmulmod(sd, ciw, ciq, P.qd), P.qd, P.qinv_d);
+      const u64 w = d2canon(__dadd_rn(u2d(x[e]), -fmulmod(vs[e * T + tid], ptw, ptq, PT.qd)), PT.qd, PT.qinv_d);
+      ws[e * T + tid] = w > PT.half ? u2d(w) - PT.qd : u2d(w);
     }
-    store_c<LOGN, K>(x, ok + (size_t)i * N, tid);
+  #pragma unroll 1
+    for (int i = 0; i < t; ++i) {
+      const PrimeInfo P = pi[i];
+      const double pvw = (double)pinv[i].w;
+      const double pvq = __ddiv_rn(pvw, P.qd);
+      const double ciw = (double)qtinv[(size_t)t * nq + i].w;
+      const double ciq = __ddiv_rn(ciw, P.qd);
+  #pragma unroll
+      for (int e = 0; e < Sh::E; ++e)
+        d[e] = __dadd_rn(fmulmod(vs[e * T + tid], pvw, pvq, P.qd), ws[e * T + tid]);  // |.| < 2 q_i
+      ntt_fwd_d<LOGN, K>(d, sm, tid, twbase<LOGN>(tw, i), P);
+      z_to_c<LOGN, K>(d, sm, tid);
+      u64 dv[Sh::E], av[Sh::E];
+      load_c<LOGN, K>(dv, dk + (size_t)i * N, tid);
+      load_c<LOGN, K>(av, ak + (size_t)i * N, tid);
+  #pragma unroll
+      for (int e = 0; e < Sh::E; ++e) {
+        const double sd = __dadd_rn(__dadd_rn(u2d(dv[e]), fmulmod(u2d(av[e]), pvw, pvq, P.qd)), -d[e]);
+        x[e] = d2canon(fmulmod(sd, ciw, ciq, P.qd), P.qd, P.qinv_d);
+      }
+      store_c<LOGN, K>(x, ok + (size_t)i * N, tid);
+    }
   }
 }
 
@@ -400,79 +421,93 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_rot_prep(const u64* __restrict__ C, CmScratch S, int level, u64 nu2n,
-               const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct) {
+               const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct,
+                long long n_units, int upc) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
-  const int j = blockIdx.x / n_ct;
-  const long long ct = blockIdx.x % n_ct;
-  const int tid = threadIdx.x;
-  const PrimeInfo P = pi[j];
-  const size_t LN = (size_t)level * N;
-  const u64* c0 = C + ct * 2 * LN + (size_t)j * N;
-  u64 x[Sh::E];
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) x[e] = ld_stream(c0 + galois_eval_src(posC<LOGN, K>(tid, e), LOGN, nu2n));
-  store_c<LOGN, K>(x, S.d01 + ct * 2 * LN + (size_t)j * N, tid);
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e)
-    x[e] = ld_stream(c0 + LN + galois_eval_src(posC<LOGN, K>(tid, e), LOGN, nu2n));
-  store_c<LOGN, K>(x, S.d2n + ct * LN + (size_t)j * N, tid);
-  c_to_z<LOGN, K>(x, sm, tid);
-  ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, j), P);
-  store_c<LOGN, K>(x, S.d2c + ct * LN + (size_t)j * N, tid);
+  // `upc` work units per CTA, consecutive in the unit order
+  for (int r = 0; r < upc; ++r) {
+    const long long unit = (long long)blockIdx.x * upc + r;
+    if (unit >= n_units) return;  // uniform across the CTA
+    if (r) __syncthreads();       // the previous unit is done with shared memory
+    const int j = unit / n_ct;
+    const long long ct = unit % n_ct;
+    const int tid = threadIdx.x;
+    const PrimeInfo P = pi[j];
+    const size_t LN = (size_t)level * N;
+    const u64* c0 = C + ct * 2 * LN + (size_t)j * N;
+    u64 x[Sh::E];
+  #pragma unroll
+    for (int e = 0; e < Sh::E; ++e) x[e] = ld_stream(c0 + galois_eval_src(posC<LOGN, K>(tid, e), LOGN, nu2n));
+    store_c<LOGN, K>(x, S.d01 + ct * 2 * LN + (size_t)j * N, tid);
+  #pragma unroll
+    for (int e = 0; e < Sh::E; ++e)
+      x[e] = ld_stream(c0 + LN + galois_eval_src(posC<LOGN, K>(tid, e), LOGN, nu2n));
+    store_c<LOGN, K>(x, S.d2n + ct * LN + (size_t)j * N, tid);
+    c_to_z<LOGN, K>(x, sm, tid);
+    ntt_inv<LOGN, K>(x, sm, tid, twbase<LOGN>(tw, j), P);
+    store_c<LOGN, K>(x, S.d2c + ct * LN + (size_t)j * N, tid);
+  }
 }
 
 // kernel R3: one CTA per (ct, poly k): v = centred INTT_p(acc_k,p); every
 // limb i: out_k,i = [k == 0] psi(c0)_i + (acc_k,i - NTT_i(v)) p^-1, in FP64
 // like kernel C (v kept signed in shared memory; |v| < q_i since p < 2 q_i).
-template <int LOGN, int K, int MINB>
+template <int LOGN, int K, int MINB, bool MULTI>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_ks_down(CmScratch S, u64* __restrict__ out, int level, int nq, const PrimeInfo* __restrict__ pi,
-              const TwD* __restrict__ tw, const TwPair* __restrict__ pinv) {
+              const TwD* __restrict__ tw, const TwPair* __restrict__ pinv, long long n_units,
+              int upc) {
   extern __shared__ u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
   constexpr int T = Sh::T;
   double* vs = reinterpret_cast<double*>(sm + Sh::SMEM_WORDS);
-  const long long ct = blockIdx.x >> 1;
-  const int k = blockIdx.x & 1;
-  const int tid = threadIdx.x;
-  const size_t LN = (size_t)level * N;
-  const PrimeInfo PP = pi[nq];
-  const u64* d0 = S.d01 + ct * 2 * LN;
-  const u64* ak = S.acc + ct * 2 * LN + (size_t)k * LN;
-  u64* ok = out + ((size_t)ct * 2 + k) * LN;
-  double d[Sh::E];
-  u64 x[Sh::E];
-  load_c<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) d[e] = u2d(x[e]);
-  c_to_z<LOGN, K>(d, sm, tid);
-  ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, nq), PP);
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) vs[e * T + tid] = x[e] > PP.half ? u2d(x[e]) - PP.qd : u2d(x[e]);
-#pragma unroll 1
-  for (int i = 0; i < level; ++i) {
-    const PrimeInfo P = pi[i];
-    const double pvw = (double)pinv[i].w;
-    const double pvq = __ddiv_rn(pvw, P.qd);
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e) d[e] = vs[e * T + tid];
-    ntt_fwd_d<LOGN, K>(d, sm, tid, twbase<LOGN>(tw, i), P);  // |d| < 13.75 q
-    z_to_c<LOGN, K>(d, sm, tid);
-    u64 av[Sh::E];
-    load_c<LOGN, K>(av, ak + (size_t)i * N, tid);
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e) d[e] = fmulmod(__dadd_rn(u2d(av[e]), -d[e]), pvw, pvq, P.qd);
-    if (k == 0) {
-      load_c<LOGN, K>(av, d0 + (size_t)i * N, tid);
-#pragma unroll
-      for (int e = 0; e < Sh::E; ++e) d[e] = __dadd_rn(d[e], u2d(av[e]));
+  // `upc` work units per CTA, consecutive in the unit order
+  for (int r = 0; r < (MULTI ? upc : 1); ++r) {
+    const long long unit = (long long)blockIdx.x * upc + r;
+    if (MULTI && unit >= n_units) return;  // uniform across the CTA
+    if (r) __syncthreads();       // the previous unit is done with shared memory
+    const long long ct = unit >> 1;
+    const int k = unit & 1;
+    const int tid = threadIdx.x;
+    const size_t LN = (size_t)level * N;
+    const PrimeInfo PP = pi[nq];
+    const u64* d0 = S.d01 + ct * 2 * LN;
+    const u64* ak = S.acc + ct * 2 * LN + (size_t)k * LN;
+    u64* ok = out + ((size_t)ct * 2 + k) * LN;
+    double d[Sh::E];
+    u64 x[Sh::E];
+    load_c<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
+  #pragma unroll
+    for (int e = 0; e < Sh::E; ++e) d[e] = u2d(x[e]);
+    c_to_z<LOGN, K>(d, sm, tid);
+    ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, nq), PP);
+  #pragma unroll
+    for (int e = 0; e < Sh::E; ++e) vs[e * T + tid] = x[e] > PP.half ? u2d(x[e]) - PP.qd : u2d(x[e]);
+  #pragma unroll 1
+    for (int i = 0; i < level; ++i) {
+      const PrimeInfo P = pi[i];
+      const double pvw = (double)pinv[i].w;
+      const double pvq = __ddiv_rn(pvw, P.qd);
+  #pragma unroll
+      for (int e = 0; e < Sh::E; ++e) d[e] = vs[e * T + tid];
+      ntt_fwd_d<LOGN, K>(d, sm, tid, twbase<LOGN>(tw, i), P);  // |d| < 13.75 q
+      z_to_c<LOGN, K>(d, sm, tid);
+      u64 av[Sh::E];
+      load_c<LOGN, K>(av, ak + (size_t)i * N, tid);
+  #pragma unroll
+      for (int e = 0; e < Sh::E; ++e) d[e] = fmulmod(__dadd_rn(u2d(av[e]), -d[e]), pvw, pvq, P.qd);
+      if (k == 0) {
+        load_c<LOGN, K>(av, d0 + (size_t)i * N, tid);
+  #pragma unroll
+        for (int e = 0; e < Sh::E; ++e) d[e] = __dadd_rn(d[e], u2d(av[e]));
+      }
+  #pragma unroll
+      for (int e = 0; e < Sh::E; ++e) x[e] = d2canon(d[e], P.qd, P.qinv_d);
+      store_c<LOGN, K>(x, ok + (size_t)i * N, tid);
     }
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e) x[e] = d2canon(d[e], P.qd, P.qinv_d);
-    store_c<LOGN, K>(x, ok + (size_t)i * N, tid);
   }
 }
 
@@ -515,33 +550,38 @@ static int cm_launch_one(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_
                          const char* fn) {
   return dispatch_cm(ctx->log_n, ctx->tune_cm_k, ctx->tune_cm_minb, [&]<int L, int K, int MINB>() -> int {
     using Sh = NttShape<L, K>;
+    const int upc = ctx->tune_cm_upc ? ctx->tune_cm_upc : 1;
     const int smem_a = Sh::SMEM_WORDS * 8;
     const int smem_bc = (Sh::SMEM_WORDS + 2 * Sh::N) * 8;
     if (int rc = require_smem(smem_bc, L, fn)) return rc;
     auto ka = k_cm_tensor<L, K, MINB>;
     auto kb = k_cm_modup<L, K, MINB>;
-    auto kc = k_cm_down<L, K, MINB>;
+    // one unit per CTA builds without the unit loop (it costs ModDown registers)
+    auto kc = upc > 1 ? k_cm_down<L, K, MINB, true> : k_cm_down<L, K, MINB, false>;
     ensure_smem(ka, smem_a);
     ensure_smem(kb, smem_bc);
     ensure_smem(kc, smem_bc);
     {
       ProfSpan span(CKKS_STAGE_CM_TENSOR, st);
-      ka<<<grid1d((long long)n_ct * level), Sh::T, smem_a, st>>>(
+      const long long nu_a = (long long)n_ct * level;
+      ka<<<grid1d((nu_a + upc - 1) / upc), Sh::T, smem_a, st>>>(
           reinterpret_cast<const u64*>(ct_a), reinterpret_cast<const u64*>(ct_b), S, level,
-          ctx->d_pi, ctx->d_tw, n_ct);
+          ctx->d_pi, ctx->d_tw, n_ct, nu_a, upc);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {
       ProfSpan span(CKKS_STAGE_CM_MODUP, st);
-      kb<<<grid1d((long long)n_ct * (level + 1)), Sh::T, smem_bc, st>>>(
-          S, reinterpret_cast<const double*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
+      const long long nu_b = (long long)n_ct * (level + 1);
+      kb<<<grid1d((nu_b + upc - 1) / upc), Sh::T, smem_bc, st>>>(
+          S, reinterpret_cast<const double*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct, nu_b, upc);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {
       ProfSpan span(CKKS_STAGE_CM_DOWN, st);
-      kc<<<grid1d((long long)n_ct * 2), Sh::T, smem_bc, st>>>(
+      const long long nu_c = (long long)n_ct * 2;
+      kc<<<grid1d((nu_c + upc - 1) / upc), Sh::T, smem_bc, st>>>(
           S, reinterpret_cast<u64*>(out), level, ctx->n_q, ctx->d_pi, ctx->d_tw, ctx->d_pinv,
-          ctx->d_qtinv);
+          ctx->d_qtinv, nu_c, upc);
     }
     return ckks_check_launch(fn);
   }, fn);
@@ -640,32 +680,36 @@ extern "C" int ckks_rotate(const ckks_ctx* ctx, uint64_t* out, const uint64_t* c
   cudaStream_t st = as_stream(stream);
   return dispatch_cm(ctx->log_n, ctx->tune_cm_k, ctx->tune_cm_minb, [&]<int L, int K, int MINB>() -> int {
     using Sh = NttShape<L, K>;
+    const int upc = ctx->tune_cm_upc ? ctx->tune_cm_upc : 1;
     const int smem_a = Sh::SMEM_WORDS * 8;
     const int smem_b = (Sh::SMEM_WORDS + 2 * Sh::N) * 8;
     const int smem_c = (Sh::SMEM_WORDS + Sh::N) * 8;
     if (int rc = require_smem(smem_b, L, fn)) return rc;
     auto ka = k_rot_prep<L, K, MINB>;
     auto kb = k_cm_modup<L, K, MINB>;
-    auto kc = k_ks_down<L, K, MINB>;
+    auto kc = upc > 1 ? k_ks_down<L, K, MINB, true> : k_ks_down<L, K, MINB, false>;
     ensure_smem(ka, smem_a);
     ensure_smem(kb, smem_b);
     ensure_smem(kc, smem_c);
     {
       ProfSpan span(CKKS_STAGE_OTHER, st);
-      ka<<<grid1d((long long)n_ct * level), Sh::T, smem_a, st>>>(reinterpret_cast<const u64*>(ct), S,
-                                                                 level, nu2n, ctx->d_pi, ctx->d_tw, n_ct);
+      const long long nu_a = (long long)n_ct * level;
+      ka<<<grid1d((nu_a + upc - 1) / upc), Sh::T, smem_a, st>>>(reinterpret_cast<const u64*>(ct), S, level,
+                                                                nu2n, ctx->d_pi, ctx->d_tw, n_ct, nu_a, upc);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {
       ProfSpan span(CKKS_STAGE_CM_MODUP, st);
-      kb<<<grid1d((long long)n_ct * (level + 1)), Sh::T, smem_b, st>>>(
-          S, reinterpret_cast<const double*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct);
+      const long long nu_b = (long long)n_ct * (level + 1);
+      kb<<<grid1d((nu_b + upc - 1) / upc), Sh::T, smem_b, st>>>(
+          S, reinterpret_cast<const double*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct, nu_b, upc);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {
       ProfSpan span(CKKS_STAGE_CM_DOWN, st);
-      kc<<<grid1d((long long)n_ct * 2), Sh::T, smem_c, st>>>(S, reinterpret_cast<u64*>(out), level,
-                                                             ctx->n_q, ctx->d_pi, ctx->d_tw, ctx->d_pinv);
+      const long long nu_c = (long long)n_ct * 2;
+      kc<<<grid1d((nu_c + upc - 1) / upc), Sh::T, smem_c, st>>>(S, reinterpret_cast<u64*>(out), level, ctx->n_q,
+                                                                ctx->d_pi, ctx->d_tw, ctx->d_pinv, nu_c, upc);
     }
     return ckks_check_launch(fn);
   }, fn);

@@ -282,6 +282,11 @@ extern "C" int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value) {
                    "ckks_ctx_set_tuning: transform log2 elements per thread must be 0 or in [2, 5]");
       ctx->tune_ntt_k = value;
       return CKKS_OK;
+    case CKKS_TUNE_CM_UNITS_PER_CTA:
+      CKKS_REQUIRE(value >= 0 && value <= 8,
+                   "ckks_ctx_set_tuning: ct-mult work units per CTA must be in [0, 8]");
+      ctx->tune_cm_upc = value;
+      return CKKS_OK;
     case CKKS_TUNE_CM_SPLIT:
       CKKS_REQUIRE(value >= 0 && value <= 4,
                    "ckks_ctx_set_tuning: ct-mult concurrent sub-batches must be in [0, 4]");

@@ -77,6 +77,10 @@ int ckks_ctx_destroy(ckks_ctx* ctx);
  *   internal streams (1..4; 0 = default: one per 64 pairs, at most 4, from
  *   128 pairs on, else 1).  The kernels of one sub-batch fill the partial
  *   last waves of the others (measured +12 % at 256 pairs, N = 2^12, L = 3).
+ *   CKKS_TUNE_CM_UNITS_PER_CTA: work units (limbs, target primes, output
+ *   polynomials) each CTA of the ct-mult and rotation kernels processes in
+ *   turn, 1..8 (0 = default 1: one CTA per unit); the grid shrinks by the
+ *   same factor.
  *   CKKS_TUNE_NTT_LOG_ELEMS: K of ckks_ntt, ckks_ct_mul_plain_rescale and
  *   ckks_mul_plain_multi, in [2, 5] for log N in [6, 14] with
  *   N / 2^K <= 1024 (0 = default: min(4, log N)).
@@ -87,7 +91,8 @@ enum {
   CKKS_TUNE_CM_LOG_ELEMS = 0,
   CKKS_TUNE_CM_MIN_BLOCKS = 1,
   CKKS_TUNE_CM_SPLIT = 2,
-  CKKS_TUNE_NTT_LOG_ELEMS = 3
+  CKKS_TUNE_NTT_LOG_ELEMS = 3,
+  CKKS_TUNE_CM_UNITS_PER_CTA = 4
 };
 int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value);
 

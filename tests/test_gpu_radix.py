@@ -12,7 +12,7 @@ from oracle.modmath import mulmod
 pytestmark = pytest.mark.gpu
 
 # ckks_ctx_set_tuning parameters
-CM_K, CM_MINB, CM_SPLIT, NTT_K = 0, 1, 2, 3
+CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC = 0, 1, 2, 3, 4
 
 
 def _rand(rng, shape, basis):
@@ -31,7 +31,7 @@ def ck(cuda):
 
 
 def _reset(_lib, ctx):
-    for p in (CM_K, CM_MINB, CM_SPLIT, NTT_K):
+    for p in (CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC):
         _lib.call("ckks_ctx_set_tuning", ctx.handle, p, 0)
 
 
@@ -171,6 +171,9 @@ def test_unbuilt_shapes_refused(ck):
         for param in (CM_K, NTT_K):
             with pytest.raises(CkksError):
                 _lib.call("ckks_ctx_set_tuning", ctx.handle, param, bad)
+    for bad in (9, -1):
+        with pytest.raises(CkksError):
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_UPC, bad)
     P = CkksParams.standard(13, 3)
     ctx = Context.get(13, P.primes, n_special=1)
     rng = np.random.default_rng(1)
@@ -182,5 +185,34 @@ def test_unbuilt_shapes_refused(ck):
             _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_MINB, mb)
             with pytest.raises(CkksError):
                 ops.ct_mul_relin_rescale(ctx, a, a, key)
+    finally:
+        _reset(_lib, ctx)
+
+
+def test_units_per_cta_identical(ck):
+    """Several work units per CTA (the grid shrinks, a CTA loops) give the
+    same ct-mult and rotation results, including a unit count that is not a
+    multiple of the units per CTA (37 pairs)."""
+    ops, _lib, Context = ck
+    from ckks_b200.params import CkksParams
+    P = CkksParams.standard(12, 3)
+    ctx = Context.get(12, P.primes, n_special=1)
+    qs = list(P.q)
+    rng = np.random.default_rng(515)
+    a = _rand(rng, (37, 2, 3, 4096), qs)
+    b = _rand(rng, (37, 2, 3, 4096), qs)
+    ksk = _rand(rng, (3, 2, 4, 4096), qs + [P.special])
+    key = ops.relin_key_prepare(ctx, ops.to_device(ksk))
+    da, db = ops.to_device(a), ops.to_device(b)
+    base = ops.to_host(ops.ct_mul_relin_rescale(ctx, da, db, key))
+    rot = ops.to_host(ops.rotate(ctx, da, key, 5))
+    assert np.array_equal(base[36:], R.ct_mul_relin_rescale(a[36:], b[36:], ksk, qs, P.special))
+    try:
+        for upc in (1, 2, 3, 4, 8):
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_UPC, upc)
+            for k in (3, 4):
+                _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_K, k)
+                assert np.array_equal(ops.to_host(ops.ct_mul_relin_rescale(ctx, da, db, key)), base), (upc, k)
+            assert np.array_equal(ops.to_host(ops.rotate(ctx, da, key, 5)), rot), upc
     finally:
         _reset(_lib, ctx)
