@@ -8,8 +8,8 @@ polynomial limb, so the buckets of different shapes need no padding).  The
 buckets are spread over a pool of streams and the whole plan is captured
 once into a CUDA graph, so a step costs one graph launch.  The autotuner
 times every bucket alone under each launch shape (per-thread radix 2^K, K = 2..5,
-balanced or tight register budget, limbs / work units per CTA, chunking of
-the bucket into launches) and keeps the fastest; the choice is baked into the
+balanced or tight register budget, limbs / work units per CTA, the
+persistent TMA-fed tensor kernel, chunking of the bucket into launches) and keeps the fastest; the choice is baked into the
 graph at capture time.
 
 The reference's batching is time multiplexing of four poly-mult instances on
@@ -118,6 +118,7 @@ class BatchExecutor:
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 0, bk.tune["k"])
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 1, bk.tune["minb"])
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 4, bk.tune.get("upc", 0))
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 5, bk.tune.get("tma", 0))
             # buckets already overlap on the executor's streams: one sub-batch per call
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 1)
             for s in range(0, bk.count, chunk):
@@ -130,6 +131,7 @@ class BatchExecutor:
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 1, 0)
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 0)
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 4, 0)
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 5, 0)
         else:
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 3, bk.tune["k"])
             for s in range(0, bk.count, chunk):
@@ -194,6 +196,8 @@ class BatchExecutor:
                 cands += [{"k": k, "minb": mb, "chunk": ch, "upc": u}
                           for k, mb, ch, u in itertools.product(RADIX_LOG2, (1, 2), (0, 128), UNITS_PER_CTA)
                           if cm_shape_built(log_n, k, mb) and not (ch and ch >= bk.count)]
+                # the persistent TMA-fed tensor kernel at the default shape
+                cands.append({"k": 0, "minb": 0, "chunk": 0, "upc": 0, "tma": 1})
             else:
                 cands += [{"k": k, "minb": 0, "chunk": 0, "upc": 0} for k in RADIX_LOG2
                           if ((1 << log_n) >> k) <= 1024]
@@ -212,7 +216,7 @@ class BatchExecutor:
                 e1.record()
                 torch.cuda.synchronize()
                 t = e0.elapsed_time(e1) / reps
-                sweep[f"K{c['k']}/b{c['minb']}/c{c['chunk']}/u{c['upc']}"] = round(t, 4)
+                sweep[f"K{c['k']}/b{c['minb']}/c{c['chunk']}/u{c['upc']}/t{c.get('tma', 0)}"] = round(t, 4)
                 if c is cands[0]:
                     default_ms = t
                 if best is None or t < best[0]:

@@ -227,6 +227,174 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   }
 }
 
+// The tensor kernel the ct-mult uses unless CKKS_TUNE_CM_TENSOR_TMA says
+// otherwise: one CTA per unit, measured faster than the TMA-fed persistent
+// variant at N = 2^12, L = 3, 256 pairs (0.050 against 0.054 ms): the kernel
+// is bound by its issue rate at 16 warps per SM more than by load latency,
+// and the staged variant adds two barriers per quarter.
+constexpr bool kTensorTmaDefault = false;
+
+// ---------------------------------------------------------------- kernel A, TMA-fed
+// Persistent variant of kernel A: each CTA walks the units blockIdx.x,
+// blockIdx.x + gridDim.x, ...  The four input limbs of a unit arrive in
+// quarters (N / 4 coefficients of a0, a1, b0, b1 per quarter) by bulk
+// asynchronous copies into two shared-memory stages, each completing on its
+// own mbarrier; one thread issues the copy of the quarter after next as soon
+// as the CTA has read a stage, so the loads of quarters 2-3 and of the next
+// unit's quarters 0-1 run under the products and the INTT of the current
+// unit.  Every wait is bounded (about 2 s): on expiry the CTA counts the event
+// in g_cm_wait_expiries (read by ckks_device_status) and stops.
+namespace {
+__device__ unsigned int g_cm_wait_expiries;
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for the phase of the given parity to complete; false after ~4e9 SM
+// cycles (about 2 s at the boost clock) without it.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+  if (mbar_test(bar, parity)) return true;
+  const long long t0 = clock64();
+  while (!mbar_test(bar, parity)) {
+    if (clock64() - t0 > 4000000000ll) return false;
+    __nanosleep(20);
+  }
+  return true;
+}
+
+// Shared memory of the TMA-fed tensor kernel: the transform workspace, two
+// stages of 4 quarter-limbs, two mbarriers.
+template <int LOGN, int K>
+constexpr int tensor_tma_smem_bytes() {
+  using Sh = NttShape<LOGN, K>;
+  return (((Sh::SMEM_WORDS + 15) & ~15) + 2 * Sh::N) * 8 + 16;
+}
+
+template <int LOGN, int K, int MINB>
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
+    k_cm_tensor_tma(const u64* __restrict__ A, const u64* __restrict__ B, CmScratch S, int level,
+                    const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct,
+                    long long n_units) {
+  extern __shared__ __align__(128) u64 sm[];
+  using Sh = NttShape<LOGN, K>;
+  constexpr int N = Sh::N;
+  constexpr int T = Sh::T;
+  constexpr int QN = N / 4;         // coefficients per quarter
+  constexpr int QE = Sh::E / 4;     // values a thread holds per quarter
+  static_assert(Sh::E >= 4, "quarters need at least 4 values a thread");
+  u64* stage[2];
+  stage[0] = sm + ((Sh::SMEM_WORDS + 15) & ~15);
+  stage[1] = stage[0] + 4 * QN;
+  unsigned long long* bars = reinterpret_cast<unsigned long long*>(stage[1] + 4 * QN);
+  const uint32_t bar[2] = {smem_u32(&bars[0]), smem_u32(&bars[1])};
+  const int tid = threadIdx.x;
+  const size_t LN = (size_t)level * N;
+  if (tid == 0) {
+    mbar_init(bar[0], 1);
+    mbar_init(bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  // quarter q (a0, a1, b0, b1) of unit u into stage s
+  auto issue = [&](long long u, int q, int s) {
+    const int j = (int)(u / n_ct);
+    const long long ct = u % n_ct;
+    const u64* a0 = A + ct * 2 * LN + (size_t)j * N + (size_t)q * QN;
+    const u64* b0 = B + ct * 2 * LN + (size_t)j * N + (size_t)q * QN;
+    mbar_expect_tx(bar[s], 4 * QN * 8);
+    bulk_g2s(smem_u32(stage[s]), a0, QN * 8, bar[s]);
+    bulk_g2s(smem_u32(stage[s] + QN), a0 + LN, QN * 8, bar[s]);
+    bulk_g2s(smem_u32(stage[s] + 2 * QN), b0, QN * 8, bar[s]);
+    bulk_g2s(smem_u32(stage[s] + 3 * QN), b0 + LN, QN * 8, bar[s]);
+  };
+  if (tid == 0 && (long long)blockIdx.x < n_units) {
+    issue(blockIdx.x, 0, 0);
+    issue(blockIdx.x, 1, 1);
+  }
+  bool expired = false;
+  for (long long u = blockIdx.x; u < n_units && !expired; u += gridDim.x) {
+    const int j = (int)(u / n_ct);
+    const long long ct = u % n_ct;
+    const PrimeInfo P = pi[j];
+    u64* d0 = S.d01 + ct * 2 * LN + (size_t)j * N;
+    u64* d2n = S.d2n + ct * LN + (size_t)j * N;
+    const long long un = u + gridDim.x;
+    double m2d[Sh::E];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int s = q & 1;
+      const bool ok = mbar_wait(bar[s], (q >> 1) & 1);
+      if (__syncthreads_or(!ok)) {
+        expired = true;
+        break;
+      }
+      const u64* st = stage[s];
+      // FP64 products as in kernel A; this thread's values of the quarter
+      // are positions q N/4 + tid + T e2 (layout C)
+#pragma unroll
+      for (int e2 = 0; e2 < QE; ++e2) {
+        const int l = tid + T * e2;
+        const int pos = q * QN + l;
+        const double a0d = u2d(st[l]), a1d = u2d(st[QN + l]);
+        const double b0d = u2d(st[2 * QN + l]), b1d = u2d(st[3 * QN + l]);
+        const double m2 = fmulmod_var(a1d, b1d, P.qd, P.qinv_d);
+        const double m0 = fmulmod_var(a0d, b0d, P.qd, P.qinv_d);
+        const double s1 = fmulmod_var(__dadd_rn(a0d, a1d), __dadd_rn(b0d, b1d), P.qd, P.qinv_d);
+        d0[pos] = d2canon(m0, P.qd, P.qinv_d);
+        d0[LN + pos] = d2canon(__dadd_rn(__dadd_rn(s1, -m0), -m2), P.qd, P.qinv_d);
+        d2n[pos] = d2canon(m2, P.qd, P.qinv_d);
+        m2d[q * QE + e2] = m2;
+      }
+      __syncthreads();  // the stage has been read by every thread
+      if (tid == 0) {
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (q < 2)
+          issue(u, q + 2, s);
+        else if (un < n_units)
+          issue(un, q - 2, s);
+      }
+    }
+    if (expired) break;
+    u64 m2[Sh::E];
+    c_to_z<LOGN, K>(m2d, sm, tid);  // |m2d| < 0.6 q: straight into the FP64 inverse
+    ntt_inv_d<LOGN, K>(m2d, m2, sm, tid, twbase<LOGN>(tw, j), P);
+    store_c<LOGN, K>(m2, S.d2c + ct * LN + (size_t)j * N, tid);
+  }
+  if (expired && tid == 0) atomicAdd(&g_cm_wait_expiries, 1u);
+}
+
+extern "C" int ckks_device_status(void) {
+  unsigned int n = 0;
+  cudaError_t e = cudaMemcpyFromSymbol(&n, g_cm_wait_expiries, sizeof(n));
+  if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "ckks_device_status: %s", cudaGetErrorString(e));
+  if (n == 0) return CKKS_OK;
+  const unsigned int zero = 0;
+  e = cudaMemcpyToSymbol(g_cm_wait_expiries, &zero, sizeof(zero));
+  if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "ckks_device_status: %s", cudaGetErrorString(e));
+  return ckks_set_error(CKKS_ETIMEOUT, "ckks_device_status: %u bounded device waits expired", n);
+}
+
 // ---------------------------------------------------------------- kernel B
 // One CTA per (ct, target prime).  Each digit is transformed (layout C in,
 // Z out) and re-distributed to layout C, so the key limbs, stored in natural
@@ -561,7 +729,26 @@ static int cm_launch_one(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_
     ensure_smem(ka, smem_a);
     ensure_smem(kb, smem_bc);
     ensure_smem(kc, smem_bc);
-    {
+    if (ctx->tune_cm_tma == 1 || (ctx->tune_cm_tma == 0 && kTensorTmaDefault)) {
+      // persistent, TMA-fed: as many CTAs as fit at once, each walking units
+      CKKS_REQUIRE(((reinterpret_cast<uintptr_t>(ct_a) | reinterpret_cast<uintptr_t>(ct_b)) & 15) == 0,
+                   "%s: the TMA-fed tensor kernel needs 16-byte aligned inputs", fn);
+      auto kt = k_cm_tensor_tma<L, K, MINB>;
+      const int smem_t = tensor_tma_smem_bytes<L, K>();
+      if (int rc = require_smem(smem_t, L, fn)) return rc;
+      ensure_smem(kt, smem_t);
+      int dev = 0, n_sm = 0, per_sm = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kt, Sh::T, smem_t);
+      const long long nu_a = (long long)n_ct * level;
+      long long grid = (long long)(n_sm > 0 ? n_sm : 1) * (per_sm > 0 ? per_sm : 1);
+      grid = grid < nu_a ? grid : nu_a;
+      ProfSpan span(CKKS_STAGE_CM_TENSOR, st);
+      kt<<<grid1d(grid), Sh::T, smem_t, st>>>(reinterpret_cast<const u64*>(ct_a),
+                                               reinterpret_cast<const u64*>(ct_b), S, level, ctx->d_pi,
+                                               ctx->d_tw, n_ct, nu_a);
+    } else {
       ProfSpan span(CKKS_STAGE_CM_TENSOR, st);
       const long long nu_a = (long long)n_ct * level;
       ka<<<grid1d((nu_a + upc - 1) / upc), Sh::T, smem_a, st>>>(

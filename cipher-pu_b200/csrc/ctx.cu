@@ -287,6 +287,11 @@ extern "C" int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value) {
                    "ckks_ctx_set_tuning: ct-mult work units per CTA must be in [0, 8]");
       ctx->tune_cm_upc = value;
       return CKKS_OK;
+    case CKKS_TUNE_CM_TENSOR_TMA:
+      CKKS_REQUIRE(value >= 0 && value <= 2,
+                   "ckks_ctx_set_tuning: ct-mult tensor variant must be 0, 1 (TMA-fed) or 2 (one CTA per unit)");
+      ctx->tune_cm_tma = value;
+      return CKKS_OK;
     case CKKS_TUNE_CM_SPLIT:
       CKKS_REQUIRE(value >= 0 && value <= 4,
                    "ckks_ctx_set_tuning: ct-mult concurrent sub-batches must be in [0, 4]");

@@ -21,6 +21,7 @@ struct ckks_ctx {
   int tune_cm_split = 0; // ct-mult: concurrent sub-batches, 1..4 (0 = default)
   int tune_ntt_k = 0;    // ckks_ntt: log2 coefficients per thread, 2..5 (0 = default)
   int tune_cm_upc = 0;   // ct-mult / rotation: work units per CTA, 1..8 (0 = default 1)
+  int tune_cm_tma = 0;   // ct-mult tensor kernel: 1 = persistent TMA-fed, 2 = one CTA per unit (0 = default)
   std::vector<u64> primes, psi, omega;
   std::vector<int> has_nega;
   std::vector<PrimeInfo> h_pi;

@@ -81,6 +81,11 @@ int ckks_ctx_destroy(ckks_ctx* ctx);
  *   polynomials) each CTA of the ct-mult and rotation kernels processes in
  *   turn, 1..8 (0 = default 1: one CTA per unit); the grid shrinks by the
  *   same factor.
+ *   CKKS_TUNE_CM_TENSOR_TMA: the ct-mult's first kernel (tensor product and
+ *   INTT of d2): 1 = persistent, one CTA per resident slot, inputs staged in
+ *   shared memory by bulk asynchronous copies (two stages of quarter limbs,
+ *   mbarrier completion, bounded waits); 2 = one CTA per (pair, limb) with
+ *   direct loads; 0 = default.
  *   CKKS_TUNE_NTT_LOG_ELEMS: K of ckks_ntt, ckks_ct_mul_plain_rescale and
  *   ckks_mul_plain_multi, in [2, 5] for log N in [6, 14] with
  *   N / 2^K <= 1024 (0 = default: min(4, log N)).
@@ -92,9 +97,19 @@ enum {
   CKKS_TUNE_CM_MIN_BLOCKS = 1,
   CKKS_TUNE_CM_SPLIT = 2,
   CKKS_TUNE_NTT_LOG_ELEMS = 3,
-  CKKS_TUNE_CM_UNITS_PER_CTA = 4
+  CKKS_TUNE_CM_UNITS_PER_CTA = 4,
+  CKKS_TUNE_CM_TENSOR_TMA = 5
 };
 int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value);
+
+/*
+ * Device-side status of the kernels that wait on asynchronous copies with a
+ * bounded spin (the TMA-fed ct-mult tensor kernel): CKKS_ETIMEOUT (and the
+ * count in ckks_last_error) when any such wait on the current device expired
+ * since the last call, which leaves those outputs incomplete; CKKS_OK
+ * otherwise.  Synchronises the device; clears the count.
+ */
+int ckks_device_status(void);
 
 /*
  * In-place forward (inverse = 0) or inverse NTT of n_polys x n_limbs

@@ -12,7 +12,7 @@ from oracle.modmath import mulmod
 pytestmark = pytest.mark.gpu
 
 # ckks_ctx_set_tuning parameters
-CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC = 0, 1, 2, 3, 4
+CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC, CM_TMA = 0, 1, 2, 3, 4, 5
 
 
 def _rand(rng, shape, basis):
@@ -31,7 +31,7 @@ def ck(cuda):
 
 
 def _reset(_lib, ctx):
-    for p in (CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC):
+    for p in (CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC, CM_TMA):
         _lib.call("ckks_ctx_set_tuning", ctx.handle, p, 0)
 
 
@@ -216,3 +216,35 @@ def test_units_per_cta_identical(ck):
             assert np.array_equal(ops.to_host(ops.rotate(ctx, da, key, 5)), rot), upc
     finally:
         _reset(_lib, ctx)
+
+
+@pytest.mark.parametrize("log_n,n_ct,level", [(12, 300, 3), (12, 7, 2), (13, 5, 4), (10, 33, 3)])
+def test_tma_tensor_kernel_identical(ck, log_n, n_ct, level):
+    """The persistent TMA-fed tensor kernel (bulk copies into shared memory,
+    mbarrier waits) gives the same ct-mult results as one CTA per unit, with
+    and without concurrent sub-batches, and no bounded wait expires."""
+    ops, _lib, Context = ck
+    from ckks_b200.params import CkksParams
+    P = CkksParams.standard(log_n, 4)
+    ctx = Context.get(log_n, P.primes, n_special=1)
+    qs = list(P.q)
+    n = 1 << log_n
+    rng = np.random.default_rng(log_n * 7 + n_ct)
+    a = _rand(rng, (n_ct, 2, level, n), qs[:level])
+    b = _rand(rng, (n_ct, 2, level, n), qs[:level])
+    ksk = _rand(rng, (4, 2, 5, n), qs + [P.special])
+    key = ops.relin_key_prepare(ctx, ops.to_device(ksk))
+    da, db = ops.to_device(a), ops.to_device(b)
+    try:
+        _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_TMA, 2)
+        base = ops.to_host(ops.ct_mul_relin_rescale(ctx, da, db, key))
+        for split in (1, 0):
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_SPLIT, split)
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_TMA, 1)
+            for _ in range(2):
+                assert np.array_equal(ops.to_host(ops.ct_mul_relin_rescale(ctx, da, db, key)), base), split
+    finally:
+        _reset(_lib, ctx)
+    assert _lib.raw("ckks_device_status")() == 0
+    sub = ksk[:level][:, :, list(range(level)) + [4]]
+    assert np.array_equal(base[:1], R.ct_mul_relin_rescale(a[:1], b[:1], sub, qs[:level], P.special))
