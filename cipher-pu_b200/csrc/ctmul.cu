@@ -35,7 +35,9 @@
 // fork / launch / join enqueue of calls from different host threads, which
 // share these events.
 namespace {
-constexpr int kMaxSplit = 4;
+constexpr int kMaxSplit = 4;     // internal streams per device
+constexpr int kMaxSub = 4;       // default sub-batches per call at most
+constexpr int kPairsPerSub = 64; // default pairs per sub-batch
 constexpr int kSplitDevices = 128;
 struct SplitStreams {
   bool ready = false;
@@ -796,8 +798,11 @@ int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
   const size_t need = ckks_ct_mul_scratch_bytes(ctx, n_ct, level);
   CKKS_REQUIRE(scratch_bytes >= need, "%s: scratch of %zu bytes < %zu needed", fn, scratch_bytes,
                need);
-  // default: one sub-batch per 64 pairs, at most 4, from 128 pairs on
-  const int split_req = ctx->tune_cm_split ? ctx->tune_cm_split : (n_ct >= 128 ? (n_ct / 64 < 4 ? n_ct / 64 : 4) : 1);
+  // default: one sub-batch per kPairsPerSub pairs, at most kMaxSub, from
+  // 2 kPairsPerSub pairs on; sub-batch h runs on internal stream h mod 4
+  const int split_req = ctx->tune_cm_split
+                            ? ctx->tune_cm_split
+                            : (n_ct >= 2 * kPairsPerSub ? (n_ct / kPairsPerSub < kMaxSub ? n_ct / kPairsPerSub : kMaxSub) : 1);
   const int split = split_req < n_ct ? split_req : n_ct;
   cudaStream_t st = as_stream(stream);
   if (split <= 1) return cm_launch_one(ctx, out, ct_a, ct_b, key, n_ct, level, cm_carve(scratch, ctx->n, n_ct, level), st, fn);
@@ -812,16 +817,18 @@ int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
   const size_t in_ct = (size_t)2 * level * ctx->n, out_ct = (size_t)2 * (level - 1) * ctx->n;
   unsigned char* sbase = reinterpret_cast<unsigned char*>(scratch);
   int rc = CKKS_OK;
+  const int n_streams = split < kMaxSplit ? split : kMaxSplit;
+  for (int h = 0; h < n_streams && e == cudaSuccess; ++h) e = cudaStreamWaitEvent(ss->s[h], ss->fork, 0);
   for (int h = 0; h < split && e == cudaSuccess && rc == CKKS_OK; ++h) {
     const int c0 = (int)((long long)n_ct * h / split), c1 = (int)((long long)n_ct * (h + 1) / split);
     const int m = c1 - c0;
-    e = cudaStreamWaitEvent(ss->s[h], ss->fork, 0);
-    if (e != cudaSuccess) break;
     rc = cm_launch_one(ctx, out + (size_t)c0 * out_ct, ct_a + (size_t)c0 * in_ct, ct_b + (size_t)c0 * in_ct, key,
-                       m, level, cm_carve(sbase, ctx->n, m, level), ss->s[h], fn);
+                       m, level, cm_carve(sbase, ctx->n, m, level), ss->s[h % n_streams], fn);
     sbase += cm_words(ctx->n, m, level) * sizeof(u64);
-    if (rc == CKKS_OK) e = cudaEventRecord(ss->join[h], ss->s[h]);
-    if (rc == CKKS_OK && e == cudaSuccess) e = cudaStreamWaitEvent(st, ss->join[h], 0);
+  }
+  for (int h = 0; h < n_streams && e == cudaSuccess && rc == CKKS_OK; ++h) {
+    e = cudaEventRecord(ss->join[h], ss->s[h]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(st, ss->join[h], 0);
   }
   if (rc != CKKS_OK) return rc;
   if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));

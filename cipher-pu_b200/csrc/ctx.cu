@@ -293,8 +293,8 @@ extern "C" int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value) {
       ctx->tune_cm_tma = value;
       return CKKS_OK;
     case CKKS_TUNE_CM_SPLIT:
-      CKKS_REQUIRE(value >= 0 && value <= 4,
-                   "ckks_ctx_set_tuning: ct-mult concurrent sub-batches must be in [0, 4]");
+      CKKS_REQUIRE(value >= 0 && value <= 16,
+                   "ckks_ctx_set_tuning: ct-mult sub-batches must be in [0, 16]");
       ctx->tune_cm_split = value;
       return CKKS_OK;
     default:

@@ -73,10 +73,12 @@ int ckks_ctx_destroy(ckks_ctx* ctx);
  *   CKKS_TUNE_CM_MIN_BLOCKS: register budget of the ct-mult kernels:
  *   1 = balanced (128 registers per thread, max(1, 512 / threads) CTAs per
  *   SM), 2 = tight (64 registers, twice the CTAs); 0 = default (balanced).
- *   CKKS_TUNE_CM_SPLIT: sub-batches of one ct-mult call run concurrently on
- *   internal streams (1..4; 0 = default: one per 64 pairs, at most 4, from
- *   128 pairs on, else 1).  The kernels of one sub-batch fill the partial
- *   last waves of the others (measured +12 % at 256 pairs, N = 2^12, L = 3).
+ *   CKKS_TUNE_CM_SPLIT: sub-batches of one ct-mult call, run on 4 internal
+ *   streams (sub-batch h on stream h mod 4; 1..16; 0 = default: one per 64
+ *   pairs, at most 4, from 128 pairs on, else 1).  The kernels of one
+ *   sub-batch fill the partial last waves of the others (measured +12 % at
+ *   256 pairs, N = 2^12, L = 3); 8 or 16 sub-batches of 32 or 16 pairs
+ *   measured 8 % and 32 % slower there.
  *   CKKS_TUNE_CM_UNITS_PER_CTA: work units (limbs, target primes, output
  *   polynomials) each CTA of the ct-mult and rotation kernels processes in
  *   turn, 1..8 (0 = default 1: one CTA per unit); the grid shrinks by the
