@@ -216,7 +216,7 @@ def test_masked_relin_equals_golden_relin(ck, n, q):
 
 
 def test_ct_mul_concurrent_sub_batches_identical(ck):
-    """A 256-pair call split into 1, 2, 3 or 4 concurrent sub-batches (internal
+    """A 256-pair call split into 1, 2, 3, 4, 8 or 16 sub-batches (4 internal
     streams joined by events) gives identical results; pairs from every
     sub-batch match the oracle."""
     ops, Context = ck
@@ -234,7 +234,7 @@ def test_ct_mul_concurrent_sub_batches_identical(ck):
     da, db = ops.to_device(a), ops.to_device(b)
     outs = []
     try:
-        for split in (1, 2, 3, 4, 0):
+        for split in (1, 2, 3, 4, 8, 16, 0):
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, split)
             outs.append(ops.to_host(ops.ct_mul_relin_rescale(ctx, da, db, key)))
     finally:
