@@ -22,9 +22,15 @@
 // Transforms per ct-mult at level L: L + (L-1)L + L + 2(L + 1) = 20 at L = 3
 // (vs 26 for the unmerged sequence).
 //
+// Arithmetic: exact FP64 on integer-valued doubles in all three kernels
+// (transforms, products, key inner product, basis conversions); residues go
+// back to canonical uint64 only where they are stored.
+//
 // Launch shape: K = log2 coefficients per thread (2..5: N/2^K threads,
-// radix-2^K register passes) and MINB = CTAs per SM the register budget is
-// cut for (__launch_bounds__).  Both are context tuning parameters.
+// radix-2^K register passes), MINB = CTAs per SM the register budget is cut
+// for (__launch_bounds__), work units per CTA, and the tensor kernel's form
+// (one CTA per unit, or persistent and TMA-fed) are context tuning
+// parameters.
 #include <mutex>
 
 #include "dispatch.cuh"
