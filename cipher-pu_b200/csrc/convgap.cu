@@ -74,6 +74,7 @@ __global__ void k_decrypt_coef0(long long* __restrict__ out, const u64* __restri
   const u64* b = ct + (size_t)c * 2 * n;
   const u64* a = b + n;
   u64 lo = 0, hi = 0;  // sum_{i >= 1} a_i s_{N-i}
+#pragma unroll 8
   for (int i = lane ? lane : 32; i < n; i += 32) {
     const u64 av = ld_stream(a + i), sv = s[n - i];
     const u64 pl = av * sv;

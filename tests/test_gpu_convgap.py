@@ -132,3 +132,26 @@ def test_general_prime_and_empty(g):
     import torch
     empty = torch.empty((0, 2, ctx.n), dtype=torch.uint64, device="cuda")
     assert G.mul_plain_multi(ctx, empty, _hat(ops, ctx, d["sc0_out"])).shape == (0, 1, 2, ctx.n)
+
+
+@pytest.mark.parametrize("log_n,q", [(4, 97), (5, 193), (13, 998244353)])
+def test_small_and_large_rings(g, log_n, q):
+    """N = 16 and 32 (fewer coefficients than a warp has lanes in the
+    decryption) and N = 8192: products and decrypted constant coefficients
+    against the oracle."""
+    G, ops, ctx0, d, m, s_res0 = g
+    from ckks_b200.context import Context
+    n = 1 << log_n
+    ctx = Context.get(log_n, [q])
+    rng = np.random.default_rng(log_n)
+    ct = rng.integers(0, q, (3, 2, n), dtype=np.uint64)
+    w = rng.integers(0, q, (2, n), dtype=np.uint64)
+    s = rng.integers(-1, 2, n)
+    out = G.mul_plain_multi(ctx, ops.to_device(ct), _hat(ops, ctx, w))
+    got = ops.to_host(out)
+    dec0 = G.decrypt_coef0(ctx, out, G.secret_residues(s, q)).cpu().numpy()
+    for c in range(3):
+        for f in range(2):
+            want = OC.mul_plain(ct[c], w[f], q)
+            assert np.array_equal(got[c, f], want), (c, f)
+            assert dec0[c, f] == OC.decrypt(want, s, q)[0]
