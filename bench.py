@@ -578,7 +578,9 @@ def run_ours(a) -> int:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "dtype_note": "exact integer arithmetic on FP64 (residues below 2^47 as doubles, FMA-based "
+                          "modular products); uint64 residues in memory",
             "data": "synthetic: uniform residues mod each prime (fresh-ciphertext distribution), random key",
             "config": config(a),
             "roofline": {"bound": "hbm", "kernel": names[dom], "achieved": achieved, "peak": hbm,
