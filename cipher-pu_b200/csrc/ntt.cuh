@@ -103,10 +103,11 @@ __device__ __forceinline__ double fmulmod(double y, double w, double wq, double 
   return __dadd_rn(__fma_rn(-qt, qd, hi), lo);
 }
 
-// a * b mod q up to a multiple of q for exact integers 0 <= a, b < 4q
+// a * b mod q up to a multiple of q for exact integers |a|, |b| < 4q
 // (q < 2^47): hi + lo is the exact product, qt = round(hi / q) is off by at
-// most 1/16 (a b / q < 2^49, two roundings of 2^-53), so hi - qt q is an
-// exact integer below 0.57 q and |result| < 0.57 q + ulp(hi) / 2 < 2^48.
+// most 1/16 (|a b| / q < 2^49, two roundings of 2^-53), so hi - qt q is an
+// exact integer below 0.57 q in magnitude and |result| < 0.57 q + ulp(hi) / 2
+// < 2^48.
 __device__ __forceinline__ double fmulmod_var(double a, double b, double qd, double qinv) {
   const double hi = __dmul_rn(a, b);
   const double lo = __fma_rn(a, b, -hi);
@@ -117,6 +118,13 @@ __device__ __forceinline__ double fmulmod_var(double a, double b, double qd, dou
 // u64 residue (< 2^52) -> exact double
 __device__ __forceinline__ double u2d(u64 x) {
   return __dadd_rn(__longlong_as_double((long long)(x | 0x4330000000000000ull)), -CKKS_FP_TWO52);
+}
+
+// exact integer double with |x| < 2^51 -> the congruent integer of
+// magnitude <= q / 2 + 1 (still a double)
+__device__ __forceinline__ double dreduce(double x, double qd, double qinv) {
+  const double qt = __dadd_rn(__fma_rn(x, qinv, CKKS_FP_MAGIC), -CKKS_FP_MAGIC);
+  return __fma_rn(-qt, qd, x);
 }
 
 // exact integer double with |x| < 2^51 -> canonical residue in [0, q)

@@ -144,8 +144,12 @@ extern "C" int ckks_vec_addsub(uint64_t* out, const uint64_t* a, const uint64_t*
 }
 
 // ------------------------------------------------------------------ poly mul
+// One CTA per polynomial limb: both operands transformed (unreduced FP64),
+// reduced to |x| <= q / 2 + 1, multiplied (fmulmod_var, |.| < 0.6 q) in the
+// evaluation order the forward leaves them in, and transformed back.  The
+// register budget targets 2 CTAs of N / 16 threads per SM.
 template <int LOGN, int K>
-__global__ void __launch_bounds__(NttShape<LOGN, K>::T)
+__global__ void __launch_bounds__(NttShape<LOGN, K>::T, (NttShape<LOGN, K>::T >= 512 ? 1 : 512 / NttShape<LOGN, K>::T))
     k_poly_mul(u64* __restrict__ out, const u64* __restrict__ a, const u64* __restrict__ b,
                int n_polys, int n_limbs, int prime_begin, const PrimeInfo* __restrict__ pi,
                const TwD* __restrict__ tw, int cyclic) {
@@ -158,20 +162,22 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
   const size_t off = ((size_t)poly * n_limbs + limb) * S::N;
   const TwD* tb = twbase<LOGN>(tw, pidx);
   const int tid = threadIdx.x;
-  u64 x[S::E], y[S::E];
+  double x[S::E], y[S::E];
 #pragma unroll
-  for (int e = 0; e < S::E; ++e) x[e] = reduce_any(a[off + posC<LOGN, K>(tid, e)], P);
-  ntt_fwd<LOGN, K>(x, sm, tid, tb, P, cyclic);
+  for (int e = 0; e < S::E; ++e) x[e] = u2d(reduce_any(ld_stream(a + off + posC<LOGN, K>(tid, e)), P));
+  ntt_fwd_d<LOGN, K>(x, sm, tid, tb, P, cyclic);
   __syncthreads();
 #pragma unroll
-  for (int e = 0; e < S::E; ++e) y[e] = reduce_any(b[off + posC<LOGN, K>(tid, e)], P);
-  ntt_fwd<LOGN, K>(y, sm, tid, tb, P, cyclic);
+  for (int e = 0; e < S::E; ++e) y[e] = u2d(reduce_any(ld_stream(b + off + posC<LOGN, K>(tid, e)), P));
+  ntt_fwd_d<LOGN, K>(y, sm, tid, tb, P, cyclic);
 #pragma unroll
-  for (int e = 0; e < S::E; ++e) x[e] = mulmod(x[e], y[e], P);
+  for (int e = 0; e < S::E; ++e)
+    x[e] = fmulmod_var(dreduce(x[e], P.qd, P.qinv_d), dreduce(y[e], P.qd, P.qinv_d), P.qd, P.qinv_d);
   __syncthreads();
-  ntt_inv<LOGN, K>(x, sm, tid, tb, P, cyclic);
+  u64 r[S::E];
+  ntt_inv_d<LOGN, K>(x, r, sm, tid, tb, P, cyclic);
 #pragma unroll
-  for (int e = 0; e < S::E; ++e) out[off + posC<LOGN, K>(tid, e)] = x[e];
+  for (int e = 0; e < S::E; ++e) out[off + posC<LOGN, K>(tid, e)] = r[e];
 }
 
 extern "C" int ckks_poly_mul(const ckks_ctx* ctx, uint64_t* out, const uint64_t* a,
