@@ -154,26 +154,37 @@ class Clocks:
             rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
         except Exception:
             rows = []
-        sm, smax, power = [], None, []
-        reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for r in rows:
-            r = [x.strip() for x in r]
-            try:
-                ts = _dt.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
-                if ts < t0 - 0.05 or ts > t1 + 0.05:
+
+        def collect(lo, hi):
+            sm, smax, power, reasons = [], None, [], set()
+            for r in rows:
+                r = [x.strip() for x in r]
+                try:
+                    ts = _dt.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    if ts < lo or ts > hi:
+                        continue
+                    sm.append(float(r[2]))
+                    smax = float(r[3])
+                    power.append(float(r[4]))
+                except Exception:
                     continue
-                sm.append(float(r[2]))
-                smax = float(r[3])
-                power.append(float(r[4]))
-            except Exception:
-                continue
-            for nm, val in zip(names, r[6:10]):
-                if val.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm),
-                "power_w_median": statistics.median(power) if power else None}
+                for nm, val in zip(names, r[6:10]):
+                    if val.lower().startswith("active"):
+                        reasons.add(nm)
+            return sm, smax, power, reasons
+
+        sm, smax, power, reasons = collect(t0 - 0.05, t1 + 0.05)
+        widened = False
+        if not sm:  # a timed region shorter than the sampling period: nearest samples, under load
+            sm, smax, power, reasons = collect(t0 - 0.3, t1 + 0.3)
+            widened = True
+        out = {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
+               "reasons": sorted(reasons), "samples": len(sm),
+               "power_w_median": statistics.median(power) if power else None}
+        if widened:
+            out["window"] = "timed region +- 0.3 s (no sample fell inside it)"
+        return out
 
 
 # ------------------------------------------------------------------ ours
