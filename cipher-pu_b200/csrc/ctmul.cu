@@ -33,6 +33,7 @@
 // parameters.
 #include <mutex>
 
+#include "ctmul.hpp"
 #include "dispatch.cuh"
 #include "profile.hpp"
 
@@ -250,8 +251,11 @@ constexpr bool kTensorTmaDefault = false;
 // own mbarrier; one thread issues the copy of the quarter after next as soon
 // as the CTA has read a stage, so the loads of quarters 2-3 and of the next
 // unit's quarters 0-1 run under the products and the INTT of the current
-// unit.  Every wait is bounded (about 2 s): on expiry the CTA counts the event
-// in g_cm_wait_expiries (read by ckks_device_status) and stops.
+// unit.  Every wait is bounded by `wait_limit` SM cycles (context tuning
+// CKKS_TUNE_WAIT_CYCLES, default about 1 s): on expiry the CTA counts the
+// event in g_cm_wait_expiries (read by ckks_device_status), thread 0 waits
+// (bounded again, kDrainCycles) for every copy it issued that has not been
+// waited for, so nothing is still landing in shared memory, and the CTA stops.
 namespace {
 __device__ unsigned int g_cm_wait_expiries;
 }
@@ -279,17 +283,20 @@ __device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
       : "memory");
   return ok != 0;
 }
-// Wait for the phase of the given parity to complete; false after ~4e9 SM
-// cycles (about 2 s at the boost clock) without it.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+// Wait for the phase of the given parity to complete; false after `limit` SM
+// cycles without it.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
   if (mbar_test(bar, parity)) return true;
   const long long t0 = clock64();
   while (!mbar_test(bar, parity)) {
-    if (clock64() - t0 > 4000000000ll) return false;
+    if (clock64() - t0 > limit) return false;
     __nanosleep(20);
   }
   return true;
 }
+// Limit of the drain that follows an expired wait: the copies still in flight
+// into the CTA's shared memory must land before the CTA may exit (about 2 s).
+constexpr long long kDrainCycles = 4000000000ll;
 
 // Shared memory of the TMA-fed tensor kernel: the transform workspace, two
 // stages of 4 quarter-limbs, two mbarriers.
@@ -303,7 +310,7 @@ template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_tensor_tma(const u64* __restrict__ A, const u64* __restrict__ B, CmScratch S, int level,
                     const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct,
-                    long long n_units) {
+                    long long n_units, long long wait_limit) {
   extern __shared__ __align__(128) u64 sm[];
   using Sh = NttShape<LOGN, K>;
   constexpr int N = Sh::N;
@@ -324,8 +331,12 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   __syncthreads();
+  // copies issued into / completions waited for on each stage; the k-th
+  // completion of a stage's barrier has parity k & 1 (issued: thread 0 only)
+  int n_issued[2] = {0, 0}, n_waited[2] = {0, 0};
   // quarter q (a0, a1, b0, b1) of unit u into stage s
   auto issue = [&](long long u, int q, int s) {
+    ++n_issued[s];
     const int j = (int)(u / n_ct);
     const long long ct = u % n_ct;
     const u64* a0 = A + ct * 2 * LN + (size_t)j * N + (size_t)q * QN;
@@ -352,11 +363,12 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
       const int s = q & 1;
-      const bool ok = mbar_wait(bar[s], (q >> 1) & 1);
+      const bool ok = mbar_wait(bar[s], n_waited[s] & 1, wait_limit);
       if (__syncthreads_or(!ok)) {
         expired = true;
         break;
       }
+      ++n_waited[s];
       const u64* st = stage[s];
       // FP64 products as in kernel A; this thread's values of the quarter
       // are positions q N/4 + tid + T e2 (layout C)
@@ -389,7 +401,16 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     ntt_inv_d<LOGN, K>(m2d, m2, sm, tid, twbase<LOGN>(tw, j), P);
     store_c<LOGN, K>(m2, S.d2c + ct * LN + (size_t)j * N, tid);
   }
-  if (expired && tid == 0) atomicAdd(&g_cm_wait_expiries, 1u);
+  if (expired && tid == 0) {
+    atomicAdd(&g_cm_wait_expiries, 1u);
+    for (int st = 0; st < 2; ++st)
+      for (; n_waited[st] < n_issued[st]; ++n_waited[st])
+        if (!mbar_wait(bar[st], n_waited[st] & 1, kDrainCycles)) {
+          atomicAdd(&g_cm_wait_expiries, 1u);  // still in flight after the drain limit
+          break;
+        }
+  }
+  __syncthreads();  // no thread leaves before the drain
 }
 
 extern "C" int ckks_device_status(void) {
@@ -755,7 +776,7 @@ static int cm_launch_one(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_
       ProfSpan span(CKKS_STAGE_CM_TENSOR, st);
       kt<<<grid1d(grid), Sh::T, smem_t, st>>>(reinterpret_cast<const u64*>(ct_a),
                                                reinterpret_cast<const u64*>(ct_b), S, level, ctx->d_pi,
-                                               ctx->d_tw, n_ct, nu_a);
+                                               ctx->d_tw, n_ct, nu_a, ckks_wait_limit(ctx));
     } else {
       ProfSpan span(CKKS_STAGE_CM_TENSOR, st);
       const long long nu_a = (long long)n_ct * level;
@@ -784,7 +805,8 @@ static int cm_launch_one(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_
 
 int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
                        const uint64_t* ct_b, const uint64_t* key, int n_ct, int level,
-                       void* scratch, size_t scratch_bytes, void* stream, const char* fn) {
+                       void* scratch, size_t scratch_bytes, void* stream, const char* fn,
+                       int max_split) {
   CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
   CKKS_REQUIRE(ctx->n_special == 1, "%s: context needs exactly one special prime", fn);
   CKKS_REQUIRE(level >= 2 && level <= ctx->n_q, "%s: level=%d outside [2, %d]", fn, level,
@@ -809,7 +831,8 @@ int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
   const int split_req = ctx->tune_cm_split
                             ? ctx->tune_cm_split
                             : (n_ct >= 2 * kPairsPerSub ? (n_ct / kPairsPerSub < kMaxSub ? n_ct / kPairsPerSub : kMaxSub) : 1);
-  const int split = split_req < n_ct ? split_req : n_ct;
+  int split = split_req < n_ct ? split_req : n_ct;
+  if (max_split > 0 && split > max_split) split = max_split;
   cudaStream_t st = as_stream(stream);
   if (split <= 1) return cm_launch_one(ctx, out, ct_a, ct_b, key, n_ct, level, cm_carve(scratch, ctx->n, n_ct, level), st, fn);
   // Concurrent sub-batches: the kernels of one sub-batch fill the partial last
@@ -846,7 +869,7 @@ extern "C" int ckks_ct_mul_relin_rescale(const ckks_ctx* ctx, uint64_t* out, con
                                          int level, void* scratch, size_t scratch_bytes,
                                          void* stream) {
   return ckks_ct_mul_launch(ctx, out, ct_a, ct_b, key, n_ct, level, scratch, scratch_bytes, stream,
-                            "ckks_ct_mul_relin_rescale");
+                            "ckks_ct_mul_relin_rescale", 0);
 }
 
 extern "C" size_t ckks_rotate_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level) {

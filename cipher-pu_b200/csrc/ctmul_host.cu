@@ -14,11 +14,8 @@
 // give the same results with serialised copies.
 #include <mutex>
 
-#include "ctx.hpp"
+#include "ctmul.hpp"
 
-int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
-                       const uint64_t* ct_b, const uint64_t* key, int n_ct, int level,
-                       void* scratch, size_t scratch_bytes, void* stream, const char* fn);
 int ckks_launch_unpack48(uint64_t* out, const void* in, long long n, cudaStream_t st);
 int ckks_launch_pack48(void* out, const uint64_t* in, long long n, cudaStream_t st);
 
@@ -142,7 +139,7 @@ static int host_pipeline(const ckks_ctx* ctx, void* out_host, const void* a_host
       if (rc == CKKS_OK) rc = ckks_launch_unpack48(db, sb, (long long)in_words, st);
       if (rc != CKKS_OK) break;
     }
-    rc = ckks_ct_mul_launch(ctx, dout, da, db, key, m, level, scratch, sl.scratch_bytes, st, fn);
+    rc = ckks_ct_mul_launch(ctx, dout, da, db, key, m, level, scratch, sl.scratch_bytes, st, fn, 0);
     if (rc != CKKS_OK) break;
     if (packed) {
       rc = ckks_launch_pack48(so, dout, (long long)out_words, st);

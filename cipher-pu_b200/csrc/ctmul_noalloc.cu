@@ -17,15 +17,10 @@
 // current) on the first call made on it, and cached.
 #include <mutex>
 
-#include "ctx.hpp"
+#include "ctmul.hpp"
 #include "profile.hpp"
 
 static __device__ __align__(256) unsigned char g_ctmul_static_scratch[CKKS_NOALLOC_SCRATCH_BYTES];
-
-// Host launcher of the three ct-mult kernels (ctmul.cu); allocates nothing.
-int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
-                       const uint64_t* ct_b, const uint64_t* key, int n_ct, int level,
-                       void* scratch, size_t scratch_bytes, void* stream, const char* fn);
 
 namespace {
 constexpr int kMaxDevices = 128;
@@ -72,7 +67,11 @@ extern "C" int ckks_ct_mul_relin_rescale_noalloc(const ckks_ctx* ctx, uint64_t* 
     base = g_noalloc_addr[dev];
   }
   // Every scratch word is written by the first two kernels before it is read,
-  // so the contents left by the previous call need no clearing.
+  // so the contents left by the previous call need no clearing.  max_split = 1:
+  // the whole batch stays on the caller's stream as one sub-batch, whatever
+  // the context's CKKS_TUNE_CM_SPLIT or the batch size, because concurrent
+  // sub-batches run on internal streams and events that the library creates
+  // on their first use.
   return ckks_ct_mul_launch(ctx, out, ct_a, ct_b, key, n_ct, level, base,
-                            (size_t)CKKS_NOALLOC_SCRATCH_BYTES, stream, fn);
+                            (size_t)CKKS_NOALLOC_SCRATCH_BYTES, stream, fn, 1);
 }

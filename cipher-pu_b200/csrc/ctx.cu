@@ -297,6 +297,10 @@ extern "C" int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value) {
                    "ckks_ctx_set_tuning: ct-mult sub-batches must be in [0, 16]");
       ctx->tune_cm_split = value;
       return CKKS_OK;
+    case CKKS_TUNE_WAIT_CYCLES:
+      CKKS_REQUIRE(value >= 0, "ckks_ctx_set_tuning: wait limit must be >= 0 SM cycles");
+      ctx->tune_wait_cycles = value;
+      return CKKS_OK;
     default:
       return ckks_set_error(CKKS_EINVAL, "ckks_ctx_set_tuning: unknown parameter %d", param);
   }

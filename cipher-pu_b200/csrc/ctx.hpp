@@ -22,6 +22,7 @@ struct ckks_ctx {
   int tune_ntt_k = 0;    // ckks_ntt: log2 coefficients per thread, 2..5 (0 = default)
   int tune_cm_upc = 0;   // ct-mult / rotation: work units per CTA, 1..8 (0 = default 1)
   int tune_cm_tma = 0;   // ct-mult tensor kernel: 1 = persistent TMA-fed, 2 = one CTA per unit (0 = default)
+  int tune_wait_cycles = 0;  // limit of every bounded device wait, SM cycles (0 = default, ~1 s)
   std::vector<u64> primes, psi, omega;
   std::vector<int> has_nega;
   std::vector<PrimeInfo> h_pi;
@@ -73,3 +74,9 @@ static inline TwPair h_twp(u64 w, u64 q) {
 }
 
 static inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+// Limit, in SM cycles, of the bounded device-side waits of this context's
+// kernels (2^31 - 1 cycles by default: about 1.1 s at the 1965 MHz boost clock).
+static inline long long ckks_wait_limit(const ckks_ctx* ctx) {
+  return ctx->tune_wait_cycles > 0 ? (long long)ctx->tune_wait_cycles : 2147483647ll;
+}

@@ -88,6 +88,11 @@ int ckks_ctx_destroy(ckks_ctx* ctx);
  *   shared memory by bulk asynchronous copies (two stages of quarter limbs,
  *   mbarrier completion, bounded waits); 2 = one CTA per (pair, limb) with
  *   direct loads; 0 = default.
+ *   CKKS_TUNE_WAIT_CYCLES: limit, in SM cycles, of every bounded device-side
+ *   wait of the context's kernels (a bulk copy landing in shared memory, a
+ *   work-queue flag); on expiry a kernel records it for ckks_device_status,
+ *   lets its own copies in flight land and returns.  0 = default
+ *   (2^31 - 1 cycles, about 1.1 s at 1965 MHz).
  *   CKKS_TUNE_NTT_LOG_ELEMS: K of ckks_ntt, ckks_ct_mul_plain_rescale and
  *   ckks_mul_plain_multi, in [2, 5] for log N in [6, 14] with
  *   N / 2^K <= 1024 (0 = default: min(4, log N)).
@@ -100,7 +105,8 @@ enum {
   CKKS_TUNE_CM_SPLIT = 2,
   CKKS_TUNE_NTT_LOG_ELEMS = 3,
   CKKS_TUNE_CM_UNITS_PER_CTA = 4,
-  CKKS_TUNE_CM_TENSOR_TMA = 5
+  CKKS_TUNE_CM_TENSOR_TMA = 5,
+  CKKS_TUNE_WAIT_CYCLES = 6
 };
 int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value);
 
@@ -599,6 +605,9 @@ int ckks_ct_mul_relin_rescale_host48(const ckks_ctx* ctx, void* out_host, const 
  *  - Nothing in the array needs clearing between calls (every word is written
  *    before it is read); it keeps the last call's intermediates.
  *  - Refused while the profiler below is enabled (it creates CUDA events).
+ *  - Always one sub-batch on the caller's stream: CKKS_TUNE_CM_SPLIT and the
+ *    default split of large batches are ignored here, since concurrent
+ *    sub-batches run on internal streams and events created on first use.
  */
 int ckks_ct_mul_relin_rescale_noalloc(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
                                       const uint64_t* ct_b, const uint64_t* key, int n_ct,

@@ -1,9 +1,9 @@
 """Generate golden vectors by running the reference's own Python functions.
 
-Run in a container that has the reference checkout (read-only) at
-REFERENCE_ROOT (default /root/reference):
+Run where a checkout of the reference project exists (read-only is fine),
+naming its root in REFERENCE_ROOT (required; there is no default):
 
-    python tests/golden/make_golden.py
+    REFERENCE_ROOT=<reference checkout> python tests/golden/make_golden.py
 
 It imports the reference's golden-model functions by path (never copying
 their source), runs them on seeded inputs and writes the inputs/outputs to
@@ -28,8 +28,20 @@ from pathlib import Path
 
 import numpy as np
 
-REF = Path(os.environ.get("REFERENCE_ROOT", "/root/reference"))
 OUT = Path(__file__).resolve().parent
+
+
+def _reference_root() -> Path:
+    root = os.environ.get("REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("make_golden.py: set REFERENCE_ROOT to the reference project's checkout")
+    path = Path(root)
+    if not (path / "scripts").is_dir():
+        raise SystemExit(f"make_golden.py: {path} has no scripts/ directory; is it the reference checkout?")
+    return path
+
+
+REF = _reference_root() if __name__ == "__main__" else Path(os.environ.get("REFERENCE_ROOT", "."))
 
 
 def load(relpath: str, name: str):

@@ -95,20 +95,27 @@ def test_encrypt_decrypt_matches_oracle(ev):
 
 
 def test_config2_ct_mult_decoded_error_and_bit_exact(ev):
-    """Config 2 semantics: slots uniform in [-1, 1], encrypt, multiply,
-    relinearise, rescale; decoded product vs the FP64 product."""
+    """The ct-mult workload with a real key (N = 2^12, L = 3 + 1 special
+    prime, scale 2^40, ternary secret, DG sigma 3.2): 256 pairs of slot
+    vectors uniform in [-1, 1] are encrypted, multiplied, relinearised and
+    rescaled; the decoded product is compared with the FP64 product x * y
+    (the structure of scripts/verify_e2e_mult.py:78-102: encrypt, e2e_mult,
+    decrypt, compare with the plaintext product).  Tolerances: max abs slot
+    error < 1e-5 and normwise relative error max|z - xy| / max|xy| < 1e-5
+    (the noise after rescale is ~2^-27 of the scale); imaginary parts < 1e-5."""
     import torch
-    from ckks_b200.evaluator import Ciphertext
     rng = np.random.default_rng(3)
-    n_pairs = 64
+    n_pairs = 256
     x = rng.uniform(-1, 1, (n_pairs, 2048))
     y = rng.uniform(-1, 1, (n_pairs, 2048))
     cx = ev.encrypt_values(x, level=3)
     cy = ev.encrypt_values(y, level=3)
     cz = ev.mul_relin_rescale(cx, cy)
+    assert cz.data.shape == (n_pairs, 2, 2, 4096)
     z = _np(ev.decrypt_values(cz, 2048))
     err = np.abs(z.real - x * y)
     assert err.max() < 1e-5, err.max()
+    assert err.max() / np.abs(x * y).max() < 1e-5
     assert np.abs(z.imag).max() < 1e-5
     # integers bit-exact against the oracle with the real key
     p = ev.params

@@ -98,3 +98,22 @@ def test_verify_e2e_mult_dropin(cuda):
     assert ve.rescale(int(ARR["e2e_rescale_in"][3]), m["q_in"], m["q_out"], m["scale_bits"]) == \
         int(ARR["e2e_rescale_out"][3])
     assert ve.main() == 0
+
+
+def test_golden_fc_layer_encrypted_forward(cuda):
+    """FCLayerGoldenModel.encrypted_forward: the reference's FC1 shape
+    (512 -> 128, Xavier-scaled N(0, 2/(in+out)) weights, seed 42;
+    scripts/golden_fc_layer.py:28-54) evaluated under CKKS on the GPU (one
+    ciphertext per input feature, the batch in the slots, weights quantised to
+    2^20 inside the encrypted linear layer) equals the plaintext float
+    forward within 1e-3 absolute (weight quantisation bounds the error by
+    512 x 2^-21 x max|x| ~ 1e-3; CKKS noise is ~1e-9)."""
+    import golden_fc_layer as fc
+
+    m = fc.FCLayerGoldenModel(in_dim=512, out_dim=128, seed=42)
+    rng = np.random.default_rng(7)
+    x = rng.uniform(-1, 1, (16, 512))
+    want = m.forward(x)
+    got = m.encrypted_forward(x, log_n=13, levels=3, seed=1)
+    assert got.shape == want.shape == (16, 128)
+    assert np.abs(got - want).max() < 1e-3, np.abs(got - want).max()

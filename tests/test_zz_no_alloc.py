@@ -63,3 +63,45 @@ def test_noalloc_entry_matches_allocating_entry(cuda):
                  too_many, level, stream)
     assert rc == 1
     assert b"static" in lib.ckks_last_error()
+
+
+def test_noalloc_entry_ignores_sub_batch_split(cuda):
+    """A batch the allocating entry would fork into concurrent sub-batches
+    (N = 2^10, L = 3, 160 pairs; and CKKS_TUNE_CM_SPLIT = 4 set on the
+    context) runs as one sub-batch on the caller's stream in the no-alloc
+    entry (which creates no stream or event) and still equals the allocating
+    entry bit for bit, on two calls in a row."""
+    import torch
+
+    import ckks_b200.ops as ops
+    from ckks_b200 import _lib
+    from ckks_b200.context import Context
+    from ckks_b200.params import CkksParams
+
+    lib = _lib.load()
+    lib.ckks_profile_enable(0)
+    P = CkksParams.standard(10, 3)
+    ctx = Context.get(10, P.primes, n_special=1)
+    qs = list(P.q)
+    rng = np.random.default_rng(78)
+    ksk = _rand(rng, (3, 2, 4, P.n), qs + [P.special])
+    key = ops.relin_key_prepare(ctx, ops.to_device(ksk))
+    n_ct, level = 160, 3
+    assert ops.ct_mul_scratch_bytes(ctx, n_ct, level) <= 32 * 1024 * 1024
+    stream = torch.cuda.current_stream().cuda_stream
+    noalloc = lib.ckks_ct_mul_relin_rescale_noalloc
+    try:
+        for split in (0, 4):
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, split)
+            for call in range(2):
+                a = ops.to_device(_rand(rng, (n_ct, 2, level, P.n), qs))
+                b = ops.to_device(_rand(rng, (n_ct, 2, level, P.n), qs))
+                ref = ops.ct_mul_relin_rescale(ctx, a, b, key)
+                out = torch.zeros_like(ref)
+                rc = noalloc(ctx.handle, out.data_ptr(), a.data_ptr(), b.data_ptr(), key.data_ptr(),
+                             n_ct, level, stream)
+                assert rc == 0, lib.ckks_last_error().decode()
+                torch.cuda.synchronize()
+                assert np.array_equal(ops.to_host(out), ops.to_host(ref)), f"split {split} call {call}"
+    finally:
+        _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 0)
