@@ -59,10 +59,14 @@ def parse():
     ap.add_argument("--enc-mlp-batches", type=int, default=8)
     ap.add_argument("--no-convgap", action="store_true",
                     help="skip the fused conv+GAP (coefficient-encoded inner product) leg")
+    ap.add_argument("--ct-mult-path", choices=["three", "fused"], default="three",
+                    help="three kernels through scratch (default) or the fused cluster kernel")
     ap.add_argument("--soak-seconds", type=float, default=1.2,
                     help="identical steps around the timed region, for the clock record")
     ap.add_argument("--no-decoded", action="store_true",
                     help="skip the decoded-slot error check of the ct-mult (real keys)")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the host-buffer end-to-end legs (profiling runs)")
     ap.add_argument("--e2e-chunk", type=int, default=48,
                     help="pairs per pipelined chunk of the host-buffer call")
     return ap.parse_args()
@@ -73,6 +77,7 @@ def config(a) -> dict:
                         f"prime, dnum={a.levels}, {a.batch} ciphertext pairs per step per GPU",
             "log_n": a.log_n, "levels": a.levels, "special_primes": 1, "dnum": a.levels,
             "batch_per_gpu": a.batch, "global_batch": a.batch * max(1, a.gpus),
+            "ct_mult_path": a.ct_mult_path,
             "l2": "inputs larger than L2: 4 distinct input batches rotate between steps",
             "parallelism": f"replicas x{max(1, a.gpus)} (ciphertext batch sharded, no collective)"}
 
@@ -203,8 +208,12 @@ class Clocks:
 
 
 # ------------------------------------------------------------------ ours
+# ct-mult kernels and their library profiler stage ids
+STAGES = {0: "k_cm_tensor", 1: "k_cm_modup", 2: "k_cm_down", 5: "k_cm_fused"}
+
+
 def stage_bytes(stage: int, n: int, level: int) -> int:
-    """Compulsory HBM bytes of each ct-mult kernel per ciphertext pair (each
+    """Algorithmic HBM bytes of each ct-mult kernel per ciphertext pair (each
     input and output word once; the relinearisation key is shared by the whole
     batch and L2-resident, so it is not counted per pair).  w = one limb."""
     w = 8 * n
@@ -212,8 +221,10 @@ def stage_bytes(stage: int, n: int, level: int) -> int:
         return 8 * level * w
     if stage == 1:   # modup: read d2 (coef + eval); write acc over q (2 polys) and over p
         return (4 * level + 2) * w
-    # down: read acc over p (2), d0/d1 (2L), acc over q (2L); write 2 (L-1) limbs
-    return 6 * level * w
+    if stage == 2:   # down: read acc over p (2), d0/d1 (2L), acc over q (2L); write 2 (L-1) limbs
+        return 6 * level * w
+    # fused: the compulsory bytes alone, read a0,a1,b0,b1 (4L limbs), write 2 (L-1) limbs
+    return (4 * level + 2 * (level - 1)) * w
 
 
 def stage_modmuls(stage: int, n: int, level: int) -> int:
@@ -227,9 +238,11 @@ def stage_modmuls(stage: int, n: int, level: int) -> int:
         return level * (3 * n + inv)
     if stage == 1:   # L^2 NTTs (each digit to every other prime and p) + 2 key products per digit and prime
         return level * level * fwd + (level + 1) * level * 2 * n
-    # per poly: INTT_p, p^-1 on limb t, INTT_t, [v]_t p^-1, then per limb i < t: NTT_i + 3 products
-    t = level - 1
-    return 2 * (inv + n + inv + n + t * (fwd + 3 * n))
+    if stage == 2:   # per poly: INTT_p, p^-1 on limb t, INTT_t, [v]_t p^-1, then per limb i < t: NTT_i + 3 products
+        t = level - 1
+        return 2 * (inv + n + inv + n + t * (fwd + 3 * n))
+    # fused: the same transforms and products, plus d_k [p] folded into the accumulators (2 per limb)
+    return sum(stage_modmuls(k, n, level) for k in range(3)) + 2 * level * n
 
 
 def measure_transforms(ctx, dev, hbm_peak: float, reps: int = 20) -> dict:
@@ -459,6 +472,7 @@ def run_ours(a) -> int:
     cts = [(rnd((B, 2, L, n), P.q), rnd((B, 2, L, n), P.q)) for _ in range(NB)]
     ksk = rnd((L, 2, L + 1, n), list(P.q) + [P.special]).contiguous()
     key = ops.relin_key_prepare(ctx, ksk)
+    _lib.call("ckks_ctx_set_tuning", ctx.handle, 7, 1 if a.ct_mult_path == "fused" else 0)
     scratch = torch.empty((ops.ct_mul_scratch_bytes(ctx, B, L) + 7) // 8, dtype=torch.uint64, device=dev)
     out = torch.empty((B, 2, L - 1, n), dtype=torch.uint64, device=dev)
 
@@ -531,8 +545,9 @@ def run_ours(a) -> int:
     # per-kernel durations: the same steps again with the library's event
     # profiler on (its two events per launch cost ~6 % of a step, so they stay
     # out of the headline timing above)
-    # each kernel alone over the whole batch (concurrent sub-batches off), so a
-    # launch's event-measured duration is that kernel's own
+    # each kernel alone over the whole batch (concurrent sub-batches of the
+    # three-kernel path off), so a launch's event-measured duration is that
+    # kernel's own
     _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 1)
     for i in range(3):
         step(i)
@@ -545,63 +560,72 @@ def run_ours(a) -> int:
     torch.cuda.synchronize()
     lib.ckks_profile_enable(0)
     _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 0)
-    stages = []
-    for s in range(3):
+    stages = {}
+    for s in STAGES:
         tot = C.c_double()
         cnt = C.c_longlong()
         lib.ckks_profile_read(s, C.byref(tot), C.byref(cnt))
-        stages.append((tot.value, cnt.value))
+        stages[s] = (tot.value, cnt.value)
+    launches_per_step = sum(c for _, c in stages.values()) / max(1, prof_steps)
     clocks = clk.summary(t_soak0, t_soak1)
     clocks["window"] = (f"{t_soak1 - t_soak0:.2f} s of identical steps: {soak_a[0]} before, the {a.steps} "
                         f"timed ({(t_host1 - t_host0) * 1e3:.1f} ms host clock), {soak_b[0]} after")
 
-    # ---------------- end to end: pinned host buffers through the host-buffer C
-    # ABI entry (H2D of both inputs, the kernels, D2H of the result inside the
-    # call, pipelined in chunks over three streams); the call blocks until the
-    # outputs are in host memory, so the region is timed on the host clock
-    ha = cts[0][0].cpu().pin_memory()
-    hb = cts[0][1].cpu().pin_memory()
-    hout = torch.empty(out.shape, dtype=torch.uint64).pin_memory()
-    ws_host = torch.empty((ops.ct_mul_host_workspace_bytes(ctx, a.e2e_chunk, L) + 7) // 8,
-                          dtype=torch.uint64, device=dev)
-    for _ in range(3):
-        ops.ct_mul_relin_rescale_host(ctx, ha, hb, key, out=hout, chunk=a.e2e_chunk, workspace=ws_host)
-    torch.cuda.synchronize()
-    barrier()
-    e2_steps = max(20, a.steps // 4)
-    t0 = time.perf_counter()
-    for _ in range(e2_steps):
-        ops.ct_mul_relin_rescale_host(ctx, ha, hb, key, out=hout, chunk=a.e2e_chunk, workspace=ws_host)
-    t1 = time.perf_counter()
-    barrier()
-    ms_e2e = max_over_ranks((t1 - t0) * 1000.0)
-    e2e_value = ws * B * e2_steps / (ms_e2e / 1000.0)
-    # the host result must be the device result of the same inputs
-    ops.ct_mul_relin_rescale(ctx, cts[0][0], cts[0][1], key, scratch=scratch, out=out)
-    if not torch.equal(out.cpu(), hout):
-        raise RuntimeError("host-buffer ct-mult differs from the device-buffer call")
-    # the same through the 48-bit wire format (6 bytes per residue on PCIe;
-    # unpack / pack on the GPU inside the call)
-    ha48 = ops.pack48_host(ha).pin_memory()
-    hb48 = ops.pack48_host(hb).pin_memory()
-    hout48 = torch.empty(6 * hout.numel(), dtype=torch.uint8).pin_memory()
-    ws48 = torch.empty((_lib.raw("ckks_ct_mul_host48_workspace_bytes")(ctx.handle, a.e2e_chunk, L) + 7) // 8,
-                       dtype=torch.uint64, device=dev)
-    for _ in range(3):
-        ops.ct_mul_relin_rescale_host48(ctx, ha48, hb48, key, B, L, out48=hout48, chunk=a.e2e_chunk,
-                                        workspace=ws48)
-    torch.cuda.synchronize()
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(e2_steps):
-        ops.ct_mul_relin_rescale_host48(ctx, ha48, hb48, key, B, L, out48=hout48, chunk=a.e2e_chunk,
-                                        workspace=ws48)
-    t1 = time.perf_counter()
-    barrier()
-    ms_e2e48 = max_over_ranks((t1 - t0) * 1000.0)
-    e2e48_value = ws * B * e2_steps / (ms_e2e48 / 1000.0)
-    if not torch.equal(ops.unpack48_host(hout48, hout.shape), hout):
-        raise RuntimeError("48-bit wire-format ct-mult differs from the device-buffer call")
+    def end_to_end():
+        # ---------------- end to end: pinned host buffers through the host-buffer C
+        # ABI entry (H2D of both inputs, the kernels, D2H of the result inside the
+        # call, pipelined in chunks over three streams); the call blocks until the
+        # outputs are in host memory, so the region is timed on the host clock
+        ha = cts[0][0].cpu().pin_memory()
+        hb = cts[0][1].cpu().pin_memory()
+        hout = torch.empty(out.shape, dtype=torch.uint64).pin_memory()
+        ws_host = torch.empty((ops.ct_mul_host_workspace_bytes(ctx, a.e2e_chunk, L) + 7) // 8,
+                              dtype=torch.uint64, device=dev)
+        for _ in range(3):
+            ops.ct_mul_relin_rescale_host(ctx, ha, hb, key, out=hout, chunk=a.e2e_chunk, workspace=ws_host)
+        torch.cuda.synchronize()
+        barrier()
+        e2_steps = max(20, a.steps // 4)
+        t0 = time.perf_counter()
+        for _ in range(e2_steps):
+            ops.ct_mul_relin_rescale_host(ctx, ha, hb, key, out=hout, chunk=a.e2e_chunk, workspace=ws_host)
+        t1 = time.perf_counter()
+        barrier()
+        ms_e2e = max_over_ranks((t1 - t0) * 1000.0)
+        e2e_value = ws * B * e2_steps / (ms_e2e / 1000.0)
+        # the host result must be the device result of the same inputs
+        ops.ct_mul_relin_rescale(ctx, cts[0][0], cts[0][1], key, scratch=scratch, out=out)
+        if not torch.equal(out.cpu(), hout):
+            raise RuntimeError("host-buffer ct-mult differs from the device-buffer call")
+        # the same through the 48-bit wire format (6 bytes per residue on PCIe;
+        # unpack / pack on the GPU inside the call)
+        ha48 = ops.pack48_host(ha).pin_memory()
+        hb48 = ops.pack48_host(hb).pin_memory()
+        hout48 = torch.empty(6 * hout.numel(), dtype=torch.uint8).pin_memory()
+        ws48 = torch.empty((_lib.raw("ckks_ct_mul_host48_workspace_bytes")(ctx.handle, a.e2e_chunk, L) + 7) // 8,
+                           dtype=torch.uint64, device=dev)
+        for _ in range(3):
+            ops.ct_mul_relin_rescale_host48(ctx, ha48, hb48, key, B, L, out48=hout48, chunk=a.e2e_chunk,
+                                            workspace=ws48)
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(e2_steps):
+            ops.ct_mul_relin_rescale_host48(ctx, ha48, hb48, key, B, L, out48=hout48, chunk=a.e2e_chunk,
+                                            workspace=ws48)
+        t1 = time.perf_counter()
+        barrier()
+        ms_e2e48 = max_over_ranks((t1 - t0) * 1000.0)
+        e2e48_value = ws * B * e2_steps / (ms_e2e48 / 1000.0)
+        if not torch.equal(ops.unpack48_host(hout48, hout.shape), hout):
+            raise RuntimeError("48-bit wire-format ct-mult differs from the device-buffer call")
+        return e2e_value, e2e48_value, e2_steps, ha, hb, hout, ha48, hb48, hout48
+
+    if a.no_e2e:
+        e2e_value = e2e48_value = e2_steps = None
+        ha = hb = hout = ha48 = hb48 = hout48 = torch.empty(0, dtype=torch.uint8)
+    else:
+        e2e_value, e2e48_value, e2_steps, ha, hb, hout, ha48, hb48, hout48 = end_to_end()
 
     if rank == 0:
         peaks = {}
@@ -612,8 +636,9 @@ def run_ours(a) -> int:
         hbm = peaks.get("hbm_gbs")
         peak_src = "measured" if hbm else "fallback"
         hbm = hbm or 6650.0
-        dom = max(range(3), key=lambda s: stages[s][0])
-        names = ["k_cm_tensor", "k_cm_modup", "k_cm_down"]
+        dom = max(STAGES, key=lambda s: stages[s][0])
+        names = STAGES
+        active = [s for s in STAGES if stages[s][1] > 0]
         per_launch_ms = stages[dom][0] / max(1, stages[dom][1])
         # a call may run its batch as concurrent sub-batches: pairs per launch
         # from the profiled launch count
@@ -628,7 +653,7 @@ def run_ours(a) -> int:
                 traffic = rec["bytes_per_pair"] * pairs_per_launch
         except Exception:
             pass
-        tot_ms = sum(s[0] for s in stages)
+        tot_ms = sum(v[0] for v in stages.values())
         # FP64 modular-multiply pipe: the butterflies' arithmetic bound, against
         # the double-word modmul throughput measured on this GPU just now
         from ckks_b200.peak import modmul_peak
@@ -679,20 +704,19 @@ def run_ours(a) -> int:
             "transforms": transforms,
             "convgap": convgap,
             "enc_mlp": enc_mlp,
-            "stage_ms_per_step": {names[s]: stages[s][0] / max(1, prof_steps) for s in range(3)},
+            "stage_ms_per_step": {names[s]: stages[s][0] / max(1, prof_steps) for s in active},
             "stage_timing": (f"library event profiler over {prof_steps} identical steps right after the timed "
-                             "region, each kernel launched alone over the whole batch (the timed region runs "
-                             "the batch as concurrent sub-batches)"),
+                             "region, each kernel launched alone over the whole batch"),
             "roofline_step": {
-                "fp64_achieved": sum(stage_modmuls(k, n, L) for k in range(3)) * B / (ms / a.steps / 1000.0) / 1e12,
+                "fp64_achieved": sum(stage_modmuls(k, n, L) for k in active) * B / (ms / a.steps / 1000.0) / 1e12,
                 "fp64_peak": mm_peak, "fp64_unit": "Tmodmul/s",
-                "fp64_frac": sum(stage_modmuls(k, n, L) for k in range(3)) * B / (ms / a.steps / 1000.0) / 1e12 / mm_peak,
-                "hbm_achieved": sum(stage_bytes(k, n, L) for k in range(3)) * B / (ms / a.steps / 1000.0) / 1e9,
+                "fp64_frac": sum(stage_modmuls(k, n, L) for k in active) * B / (ms / a.steps / 1000.0) / 1e12 / mm_peak,
+                "hbm_achieved": stage_bytes(5, n, L) * B / (ms / a.steps / 1000.0) / 1e9,
                 "hbm_peak": hbm, "hbm_unit": "GB/s",
-                "hbm_frac": sum(stage_bytes(k, n, L) for k in range(3)) * B / (ms / a.steps / 1000.0) / 1e9 / hbm,
-                "basis": "whole step: all three kernels' algorithmic modmuls / bytes per pair x pairs per GPU, "
-                         "over the timed step time"},
-            "stage_share": {names[s]: (stages[s][0] / tot_ms if tot_ms else None) for s in range(3)},
+                "hbm_frac": stage_bytes(5, n, L) * B / (ms / a.steps / 1000.0) / 1e9 / hbm,
+                "basis": "whole step: the running kernels' algorithmic modmuls per pair, and the compulsory bytes "
+                         "per pair (inputs and outputs once), x pairs per GPU over the timed step time"},
+            "stage_share": {names[s]: (stages[s][0] / tot_ms if tot_ms else None) for s in active},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT,
                     "h2d_bytes_per_step": int(ha.numel() * 8 + hb.numel() * 8),
@@ -710,7 +734,9 @@ def run_ours(a) -> int:
             "soak": {"value": soak_value, "unit": UNIT, "steps": soak_steps,
                      "note": "identical steps around the timed region (clock record window)"},
             "decoded": decoded,
-            "gpu_launches": 3 * (min(4, B // 64) if B >= 128 else 1) * a.steps,
+            "gpu_launches": int(round(launches_per_step * a.steps)),
+            "gpu_launches_basis": f"{launches_per_step:g} library kernel launches per step, counted by the "
+                                  "library's profiler over the profiled pass",
             "clocks": clocks,
         }
         print(json.dumps(line), flush=True)

@@ -60,6 +60,7 @@ SIGNATURES: dict[str, tuple] = {
     "ckks_dare_refresh": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _vp, _i32, _i32, _i32, _i32, _vp,
                                  _sz, _vp]),
     "ckks_noise_energy": (_i32, [_u64p, _u64p, _i32, _i32, _u64, _vp]),
+    "ckks_noise_energy_sat": (_i32, [_u64p, _vp, _u64p, _i32, _i32, _u64, _i32, _vp]),
     "ckks_snr_sums": (_i32, [_vp, _vp, _vp, _i32, _i32, _i32, _vp]),
     "ckks_block_sparse_mask": (_i32, [_vp, _vp, _vp, _i64, _i32, C.c_double, _vp]),
     "ckks_block_post_process": (_i32, [_u64p, _vp, _u64p, _i32, _i32, _i32, _u64, _u64, _i32, _vp]),

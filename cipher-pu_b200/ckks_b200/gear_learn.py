@@ -97,6 +97,12 @@ class GearNet:
 
     def fit(self, X: np.ndarray, T: np.ndarray, epochs: int = 30, batch: int = 1024, lr: float = 2e-3,
             seed: int = 0, val_frac: float = 0.1) -> dict:
+        """Adam on the mean squared error (targets in units of 100 dB), cosine
+        learning rate.  Under torch.distributed every rank passes the same
+        traces (sharded.gen_traces gathers them) and the same seed; each
+        minibatch is split over the ranks and the gradients averaged
+        (sharded.fit_loop), so every rank ends with the same parameters."""
+        from .sharded import fit_loop
         X = np.asarray(X, dtype=np.float64)
         T = np.clip(np.asarray(T, dtype=np.float64), *SNR_CLIP) / 100.0
         self.mu = X.mean(0)
@@ -107,6 +113,7 @@ class GearNet:
         va, tr = idx[:nv], idx[nv:]
         Xd = self._norm(X)
         Td = torch.from_numpy(T.astype(np.float32)).to(self.device)
+        tr_d = torch.from_numpy(tr).to(self.device)
         m = torch.zeros_like(self.p)
         v = torch.zeros_like(self.p)
         grad = torch.empty_like(self.p)
@@ -114,25 +121,30 @@ class GearNet:
         cache = torch.empty((batch, 128), dtype=torch.float32, device=self.device)
         dcache = torch.empty((batch, 132), dtype=torch.float32, device=self.device)
         st = torch.cuda.current_stream().cuda_stream
-        step = 0
         hist = []
-        for ep in range(epochs):
-            perm = torch.from_numpy(rng.permutation(tr)).to(self.device)
-            for s in range(0, len(tr) - batch + 1, batch):
-                bi = perm[s:s + batch]
-                xb = Xd[bi].contiguous()
-                tb = Td[bi].contiguous()
-                _lib.call("ckks_gear_mlp_forward", self.p.data_ptr(), xb.data_ptr(), y.data_ptr(),
-                          cache.data_ptr(), batch, st)
-                _lib.call("ckks_gear_mlp_backward", self.p.data_ptr(), xb.data_ptr(), cache.data_ptr(),
-                          y.data_ptr(), tb.data_ptr(), None, grad.data_ptr(), dcache.data_ptr(), batch, st)
-                step += 1
-                lr_t = lr * 0.5 * (1 + math.cos(math.pi * ep / max(1, epochs)))
-                _lib.call("ckks_gear_mlp_adam", self.p.data_ptr(), grad.data_ptr(), m.data_ptr(),
-                          v.data_ptr(), step, float(lr_t), 0.9, 0.999, 1e-8, st)
+
+        def grad_step(rows):
+            b = len(rows)
+            bi = tr_d[torch.from_numpy(np.asarray(rows)).to(self.device)]
+            xb = Xd[bi].contiguous()
+            tb = Td[bi].contiguous()
+            _lib.call("ckks_gear_mlp_forward", self.p.data_ptr(), xb.data_ptr(), y.data_ptr(),
+                      cache.data_ptr(), b, st)
+            _lib.call("ckks_gear_mlp_backward", self.p.data_ptr(), xb.data_ptr(), cache.data_ptr(),
+                      y.data_ptr(), tb.data_ptr(), None, grad.data_ptr(), dcache.data_ptr(), b, st)
+            return grad, b
+
+        def apply_step(g, step, ep):
+            lr_t = lr * 0.5 * (1 + math.cos(math.pi * ep / max(1, epochs)))
+            _lib.call("ckks_gear_mlp_adam", self.p.data_ptr(), g.data_ptr(), m.data_ptr(),
+                      v.data_ptr(), step, float(lr_t), 0.9, 0.999, 1e-8, st)
+
+        def on_epoch(ep):
             pv = self.predict(X[va])
             hist.append(float(np.sqrt(((pv - T[va] * 100.0) ** 2).mean())))
-        return {"val_rmse_db": hist, "train": len(tr), "val": nv, "steps": step}
+
+        steps = fit_loop(len(tr), batch, epochs, rng, grad_step, apply_step, on_epoch)
+        return {"val_rmse_db": hist, "train": len(tr), "val": nv, "steps": steps}
 
     def save(self, path):
         np.savez(path, schema=SCHEMA, params=self.p.cpu().numpy(), mu=self.mu, sd=self.sd)

@@ -347,6 +347,17 @@ def noise_energy(x: torch.Tensor, q: int) -> list[int]:
     return [int(lo) + (int(hi) << 64) for lo, hi in h]
 
 
+def noise_energy_sat(x: torch.Tensor, q: int, acc_bits: int = 106) -> tuple[list[int], list[bool]]:
+    """The noise monitor with an acc_bits-wide accumulator: per row of x [R, L]
+    the sum of min(c, q-c)^2 (clamped to 2^acc_bits - 1) and its saturation flag."""
+    R, L = x.shape
+    out = torch.empty((R, 2), dtype=U64, device=x.device)
+    sat = torch.empty(R, dtype=torch.uint8, device=x.device)
+    _lib.call("ckks_noise_energy_sat", _p(out), sat.data_ptr(), _p(x), R, L, int(q), int(acc_bits), _stream())
+    h = to_host(out)
+    return [int(lo) + (int(hi) << 64) for lo, hi in h], [bool(v) for v in sat.cpu().tolist()]
+
+
 def snr_sums(dec: torch.Tensor, ref: torch.Tensor) -> torch.Tensor:
     """Per row (signal energy, error energy) of complex or real float64 tensors [R, L]."""
     cplx = dec.is_complex()

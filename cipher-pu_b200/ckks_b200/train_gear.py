@@ -1,6 +1,7 @@
 """Train the learned gear controller and compare it with the plain one.
 
     python -m ckks_b200.train_gear train   [--traces 200000] [--epochs 40] [--out PATH]
+    torchrun --nproc-per-node G -m ckks_b200.train_gear train ...   (data-parallel)
     python -m ckks_b200.train_gear compare [--net PATH] [--model mlp|cnn] [--batches 8]
 
 train: generates noise-monitor traces by running random encrypted layers of
@@ -26,21 +27,25 @@ DEFAULT_NET = Path(__file__).resolve().parent / "data" / "gear_net.npz"
 
 def train(n_traces: int = 200_000, epochs: int = 40, out: Path = DEFAULT_NET, seed: int = 0,
           log_n: int = 13, levels: int = 4) -> dict:
+    from .dist import world
     from .evaluator import Evaluator
     from .gear_learn import GearNet, gen_traces
     from .params import CkksParams
+    from .sharded import gen_traces as sharded_traces
     ev = Evaluator(CkksParams.standard(log_n, levels, seed=seed + 100))
     ev.keygen()
     t0 = time.perf_counter()
-    X, T = gen_traces(ev, n_traces, seed=seed)
+    # each rank generates its share (own seed), every rank gets all traces
+    X, T = sharded_traces(n_traces, seed, lambda count, sd: gen_traces(ev, count, seed=sd))
     t_gen = time.perf_counter() - t0
     net = GearNet(seed=seed)
     t1 = time.perf_counter()
-    hist = net.fit(X, T, epochs=epochs, seed=seed)
+    hist = net.fit(X, T, epochs=epochs, seed=seed)   # data-parallel under torch.distributed
     t_fit = time.perf_counter() - t1
     out = Path(out)
-    out.parent.mkdir(parents=True, exist_ok=True)
-    net.save(out)
+    if world()[1] == 0:
+        out.parent.mkdir(parents=True, exist_ok=True)
+        net.save(out)
     return {"traces": len(X), "gen_s": t_gen, "fit_s": t_fit, "val_rmse_db": hist["val_rmse_db"][-1],
             "val_rmse_curve": hist["val_rmse_db"], "checkpoint": str(out)}
 
@@ -82,6 +87,20 @@ def compare(net_path: Path = DEFAULT_NET, model: str = "mlp", batches: int = 8, 
             "snr_gap_db": rl["snr_db"] - rp["snr_db"]}
 
 
+def _init_distributed():
+    """Under torchrun (WORLD_SIZE > 1): one process per GPU over NCCL."""
+    import os
+    if int(os.environ.get("WORLD_SIZE", "1")) <= 1:
+        return False
+    from datetime import timedelta
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    return True
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser()
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -95,11 +114,17 @@ def main(argv=None) -> int:
     c.add_argument("--batches", type=int, default=8)
     c.add_argument("--target-db", type=float, default=40.0)
     a = ap.parse_args(argv)
+    distributed = _init_distributed() if a.cmd == "train" else False
     if a.cmd == "train":
         r = train(a.traces, a.epochs, Path(a.out))
     else:
         r = compare(Path(a.net), a.model, a.batches, target_db=a.target_db)
-    print(json.dumps(r, default=float))
+    from .dist import world
+    if world()[1] == 0:
+        print(json.dumps(r, default=float))
+    if distributed:
+        import torch.distributed as dist
+        dist.destroy_process_group()
     return 0
 
 

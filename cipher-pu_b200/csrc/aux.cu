@@ -52,6 +52,82 @@ extern "C" int ckks_noise_energy(uint64_t* out_sum, const uint64_t* in, int n_ro
   return ckks_check_launch("ckks_noise_energy");
 }
 
+// ---------------------------------------------------------------- noise energy, saturating
+// The same sum with the RTL accumulator's saturation flag
+// (rtl/m4/noise_monitor.sv:62-73: an ACC_W-bit accumulator that stops, flag
+// set, once a sum would wrap).  The sum is formed exactly in 192 bits
+// (q < 2^62: each square < 2^122, at most 2^31 terms), so the flag does not
+// depend on the order of the parallel reduction: saturated[row] = 1 exactly
+// when the sum reaches 2^acc_bits, and the reported sum is then clamped to
+// 2^acc_bits - 1 (the RTL holds its last pre-wrap value instead, which
+// depends on the coefficient order).
+struct U192 {
+  u64 w0, w1, w2;
+};
+__device__ __forceinline__ void add192(U192& a, const U192& b) {
+  const u64 s0 = a.w0 + b.w0;
+  const u64 c0 = s0 < a.w0 ? 1ull : 0ull;
+  const u64 t1 = a.w1 + b.w1;
+  const u64 c1a = t1 < a.w1 ? 1ull : 0ull;
+  const u64 s1 = t1 + c0;
+  const u64 c1b = s1 < t1 ? 1ull : 0ull;
+  a.w0 = s0;
+  a.w1 = s1;
+  a.w2 = a.w2 + b.w2 + c1a + c1b;
+}
+
+__global__ void k_noise_energy_sat(unsigned long long* __restrict__ out, unsigned char* __restrict__ sat,
+                                   const u64* __restrict__ in, int row_len, u64 q, int acc_bits) {
+  const long long row = blockIdx.x;
+  const u64* src = in + (size_t)row * row_len;
+  U192 acc = {0, 0, 0};
+  for (int i = threadIdx.x; i < row_len; i += blockDim.x) {
+    const u64 c = src[i] % q;
+    const u64 a = c <= q - c ? c : q - c;
+    const U192 sq = {a * a, __umul64hi(a, a), 0};
+    add192(acc, sq);
+  }
+  for (int off = 16; off; off >>= 1) {
+    const U192 o = {__shfl_down_sync(0xffffffffu, acc.w0, off), __shfl_down_sync(0xffffffffu, acc.w1, off),
+                    __shfl_down_sync(0xffffffffu, acc.w2, off)};
+    add192(acc, o);
+  }
+  __shared__ U192 part[32];
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) part[w] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    U192 tot = {0, 0, 0};
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) add192(tot, part[k]);
+    // tot >= 2^acc_bits ?
+    bool over;
+    if (acc_bits >= 128) over = tot.w2 != 0;
+    else if (acc_bits >= 64) over = tot.w2 != 0 || (acc_bits < 128 && (tot.w1 >> (acc_bits - 64)) != 0);
+    else over = tot.w2 != 0 || tot.w1 != 0 || (tot.w0 >> acc_bits) != 0;
+    if (over) {
+      tot.w0 = acc_bits >= 64 ? ~0ull : ((1ull << acc_bits) - 1);
+      tot.w1 = acc_bits >= 128 ? ~0ull : (acc_bits > 64 ? ((1ull << (acc_bits - 64)) - 1) : 0ull);
+    }
+    out[2 * row] = tot.w0;
+    out[2 * row + 1] = tot.w1;
+    sat[row] = over ? 1 : 0;
+  }
+}
+
+extern "C" int ckks_noise_energy_sat(uint64_t* out_sum, uint8_t* saturated, const uint64_t* in, int n_rows,
+                                     int row_len, uint64_t q, int acc_bits, void* stream) {
+  CKKS_REQUIRE(n_rows >= 0 && row_len >= 0, "ckks_noise_energy_sat: negative size");
+  CKKS_REQUIRE(q >= 2 && q < (1ull << 62), "ckks_noise_energy_sat: q outside [2, 2^62)");
+  CKKS_REQUIRE(acc_bits >= 1 && acc_bits <= 128, "ckks_noise_energy_sat: acc_bits=%d outside [1, 128]",
+               acc_bits);
+  if (n_rows == 0) return CKKS_OK;
+  CKKS_REQUIRE(out_sum && saturated && in, "ckks_noise_energy_sat: NULL pointer argument");
+  k_noise_energy_sat<<<grid1d(n_rows), 256, 0, as_stream(stream)>>>(
+      reinterpret_cast<unsigned long long*>(out_sum), reinterpret_cast<unsigned char*>(saturated),
+      reinterpret_cast<const u64*>(in), row_len, q, acc_bits);
+  return ckks_check_launch("ckks_noise_energy_sat");
+}
+
 // ---------------------------------------------------------------- slot SNR
 // Per row: sum |ref|^2 and sum |dec - ref|^2 over row_len complex values.
 __global__ void k_snr(double* __restrict__ out, const double* __restrict__ dec,

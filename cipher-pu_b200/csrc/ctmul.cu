@@ -736,9 +736,15 @@ extern "C" int ckks_relin_key_prepare(const ckks_ctx* ctx, uint64_t* prepared,
   return ckks_check_launch("ckks_relin_key_prepare");
 }
 
-extern "C" size_t ckks_ct_mul_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level) {
+size_t ckks_ct_mul_scratch_bytes_3k(const ckks_ctx* ctx, int n_ct, int level) {
   if (!ctx || n_ct < 0 || level < 1) return 0;
   return cm_words(ctx->n, n_ct, level) * sizeof(u64);
+}
+
+extern "C" size_t ckks_ct_mul_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level) {
+  if (!ctx || n_ct < 0 || level < 1) return 0;
+  if (ckks_ct_mul_fused_will_run(ctx, level)) return 0;
+  return ckks_ct_mul_scratch_bytes_3k(ctx, n_ct, level);
 }
 
 // The three ct-mult kernels for one sub-batch on one stream.
@@ -806,7 +812,7 @@ static int cm_launch_one(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_
 int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
                        const uint64_t* ct_b, const uint64_t* key, int n_ct, int level,
                        void* scratch, size_t scratch_bytes, void* stream, const char* fn,
-                       int max_split) {
+                       int max_split, bool allow_fused) {
   CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
   CKKS_REQUIRE(ctx->n_special == 1, "%s: context needs exactly one special prime", fn);
   CKKS_REQUIRE(level >= 2 && level <= ctx->n_q, "%s: level=%d outside [2, %d]", fn, level,
@@ -822,8 +828,17 @@ int ckks_ct_mul_launch(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_a,
   CKKS_REQUIRE(pmax < 2 * pmin && pmax < (1ull << 61) / 4,
                "%s: primes must satisfy max < 2 min (centred basis conversion)", fn);
   if (n_ct == 0) return CKKS_OK;
+  if (allow_fused && ckks_ct_mul_fused_will_run(ctx, level)) {
+    CKKS_REQUIRE(out && ct_a && ct_b && key, "%s: NULL pointer argument", fn);
+    const int rc = ckks_ct_mul_fused(ctx, out, ct_a, ct_b, key, n_ct, level, stream, fn);
+    if (rc != CKKS_EUNSUPPORTED) return rc;
+  }
+  if (allow_fused && ctx->tune_cm_fused == 1)
+    return ckks_set_error(CKKS_EUNSUPPORTED,
+                          "%s: the fused kernel is not built or not schedulable for log_n=%d, level=%d "
+                          "(built: log_n 10..13, level 2..7)", fn, ctx->log_n, level);
   CKKS_REQUIRE(out && ct_a && ct_b && key && scratch, "%s: NULL pointer argument", fn);
-  const size_t need = ckks_ct_mul_scratch_bytes(ctx, n_ct, level);
+  const size_t need = ckks_ct_mul_scratch_bytes_3k(ctx, n_ct, level);
   CKKS_REQUIRE(scratch_bytes >= need, "%s: scratch of %zu bytes < %zu needed", fn, scratch_bytes,
                need);
   // default: one sub-batch per kPairsPerSub pairs, at most kMaxSub, from
@@ -869,11 +884,11 @@ extern "C" int ckks_ct_mul_relin_rescale(const ckks_ctx* ctx, uint64_t* out, con
                                          int level, void* scratch, size_t scratch_bytes,
                                          void* stream) {
   return ckks_ct_mul_launch(ctx, out, ct_a, ct_b, key, n_ct, level, scratch, scratch_bytes, stream,
-                            "ckks_ct_mul_relin_rescale", 0);
+                            "ckks_ct_mul_relin_rescale", 0, true);
 }
 
 extern "C" size_t ckks_rotate_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level) {
-  return ckks_ct_mul_scratch_bytes(ctx, n_ct, level);
+  return ckks_ct_mul_scratch_bytes_3k(ctx, n_ct, level);
 }
 
 extern "C" int ckks_rotate(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct, const uint64_t* key,

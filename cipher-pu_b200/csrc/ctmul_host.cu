@@ -139,7 +139,7 @@ static int host_pipeline(const ckks_ctx* ctx, void* out_host, const void* a_host
       if (rc == CKKS_OK) rc = ckks_launch_unpack48(db, sb, (long long)in_words, st);
       if (rc != CKKS_OK) break;
     }
-    rc = ckks_ct_mul_launch(ctx, dout, da, db, key, m, level, scratch, sl.scratch_bytes, st, fn, 0);
+    rc = ckks_ct_mul_launch(ctx, dout, da, db, key, m, level, scratch, sl.scratch_bytes, st, fn, 0, true);
     if (rc != CKKS_OK) break;
     if (packed) {
       rc = ckks_launch_pack48(so, dout, (long long)out_words, st);

@@ -40,8 +40,8 @@ extern "C" int ckks_ct_mul_relin_rescale_noalloc(const ckks_ctx* ctx, uint64_t* 
   // The optional profiler creates CUDA events; keep this path free of any
   // resource creation.
   CKKS_REQUIRE(!prof_on(), "%s: profiling is enabled (ckks_profile_enable); disable it first", fn);
-  const size_t per_pair = ckks_ct_mul_scratch_bytes(ctx, 1, level);
-  const size_t need = ckks_ct_mul_scratch_bytes(ctx, n_ct, level);
+  const size_t per_pair = ckks_ct_mul_scratch_bytes_3k(ctx, 1, level);
+  const size_t need = ckks_ct_mul_scratch_bytes_3k(ctx, n_ct, level);
   CKKS_REQUIRE(need <= (size_t)CKKS_NOALLOC_SCRATCH_BYTES,
                "%s: %d pairs at N=%d, level %d need %zu scratch bytes, above the fixed static "
                "buffer of %zu bytes; pass at most %zu pairs per call",
@@ -71,7 +71,8 @@ extern "C" int ckks_ct_mul_relin_rescale_noalloc(const ckks_ctx* ctx, uint64_t* 
   // the whole batch stays on the caller's stream as one sub-batch, whatever
   // the context's CKKS_TUNE_CM_SPLIT or the batch size, because concurrent
   // sub-batches run on internal streams and events that the library creates
-  // on their first use.
+  // on their first use.  allow_fused = false: this entry is the three-kernel
+  // path with its scratch in the static array.
   return ckks_ct_mul_launch(ctx, out, ct_a, ct_b, key, n_ct, level, base,
-                            (size_t)CKKS_NOALLOC_SCRATCH_BYTES, stream, fn, 1);
+                            (size_t)CKKS_NOALLOC_SCRATCH_BYTES, stream, fn, 1, false);
 }

@@ -23,6 +23,7 @@ struct ckks_ctx {
   int tune_cm_upc = 0;   // ct-mult / rotation: work units per CTA, 1..8 (0 = default 1)
   int tune_cm_tma = 0;   // ct-mult tensor kernel: 1 = persistent TMA-fed, 2 = one CTA per unit (0 = default)
   int tune_wait_cycles = 0;  // limit of every bounded device wait, SM cycles (0 = default, ~1 s)
+  int tune_cm_fused = 0;     // ct-mult: 0 = fused kernel where built, 1 = fused required, 2 = three kernels
   std::vector<u64> primes, psi, omega;
   std::vector<int> has_nega;
   std::vector<PrimeInfo> h_pi;

@@ -88,6 +88,15 @@ int ckks_ctx_destroy(ckks_ctx* ctx);
  *   shared memory by bulk asynchronous copies (two stages of quarter limbs,
  *   mbarrier completion, bounded waits); 2 = one CTA per (pair, limb) with
  *   direct loads; 0 = default.
+ *   CKKS_TUNE_CM_FUSED: ct-mult path.  0 = default = 2: the three kernels
+ *   (tensor, ModUp + key inner product, ModDown + rescale) through scratch;
+ *   1 = the fused kernel (one thread-block cluster of level + 1 CTAs per
+ *   pair, intermediates exchanged through distributed shared memory and
+ *   accumulated in TMEM, no scratch), built for log N in [10, 13] and level
+ *   in [2, 7], refusing other shapes.  The fused kernel reads and writes only
+ *   the compulsory bytes but measured 0.50-0.77x the three kernels' rate on
+ *   B200 (its CTAs wait at cluster barriers), so it is not the default.
+ *   ckks_ct_mul_scratch_bytes follows this choice (0 when fused).
  *   CKKS_TUNE_WAIT_CYCLES: limit, in SM cycles, of every bounded device-side
  *   wait of the context's kernels (a bulk copy landing in shared memory, a
  *   work-queue flag); on expiry a kernel records it for ckks_device_status,
@@ -106,7 +115,8 @@ enum {
   CKKS_TUNE_NTT_LOG_ELEMS = 3,
   CKKS_TUNE_CM_UNITS_PER_CTA = 4,
   CKKS_TUNE_CM_TENSOR_TMA = 5,
-  CKKS_TUNE_WAIT_CYCLES = 6
+  CKKS_TUNE_WAIT_CYCLES = 6,
+  CKKS_TUNE_CM_FUSED = 7
 };
 int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value);
 
@@ -217,7 +227,9 @@ int ckks_rescale_rns(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in, int
 int ckks_relin_key_prepare(const ckks_ctx* ctx, uint64_t* prepared, const uint64_t* ksk,
                            void* stream);
 
-/* Scratch bytes needed by ckks_ct_mul_relin_rescale for (n_ct, level). */
+/* Scratch bytes needed by ckks_ct_mul_relin_rescale for (n_ct, level): 0
+ * when the call takes the fused kernel (see CKKS_TUNE_CM_FUSED), else the
+ * three-kernel path's (6 level + 2) limbs per pair. */
 size_t ckks_ct_mul_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level);
 
 /*
@@ -228,7 +240,8 @@ size_t ckks_ct_mul_scratch_bytes(const ckks_ctx* ctx, int n_ct, int level);
  *   key        : prepared relinearisation key (ckks_relin_key_prepare)
  *   out        : [n_ct][2][level-1][N] evaluation domain
  *   scratch    : caller-allocated device buffer of at least
- *                ckks_ct_mul_scratch_bytes(ctx, n_ct, level) bytes
+ *                ckks_ct_mul_scratch_bytes(ctx, n_ct, level) bytes (may be
+ *                NULL when that is 0: the fused kernel needs none)
  * Decryption convention m ~ c0 + c1 * s.
  * Replaces scripts/verify_e2e_mult.py:78 e2e_mult (tensor + relin +
  * rescale) and the controllers rtl/m4/e2e_ckks_mult_ctrl_m4.sv /
@@ -324,6 +337,18 @@ int ckks_dare_refresh(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct, co
  */
 int ckks_noise_energy(uint64_t* out_sum, const uint64_t* in, int n_rows, int row_len, uint64_t q,
                       void* stream);
+
+/*
+ * The noise monitor with its accumulator width and saturation flag: as
+ * ckks_noise_energy, plus saturated[row] = 1 when the exact sum reaches
+ * 2^acc_bits (1 <= acc_bits <= 128), in which case the reported sum is
+ * 2^acc_bits - 1.  acc_bits = 106 is the RTL's ACC_W.  The flag marks a
+ * window whose noise left the monitor's range - a corrupted ciphertext or
+ * key, or a decryption that wrapped around q.  Replaces the `saturated`
+ * output of rtl/m4/noise_monitor.sv:30,62-73.
+ */
+int ckks_noise_energy_sat(uint64_t* out_sum, uint8_t* saturated, const uint64_t* in, int n_rows,
+                          int row_len, uint64_t q, int acc_bits, void* stream);
 
 /*
  * Slot SNR sums: per row, out[2*row] = sum |ref|^2, out[2*row+1] =
@@ -618,7 +643,8 @@ int ckks_ct_mul_relin_rescale_noalloc(const ckks_ctx* ctx, uint64_t* out, const 
  * points record CUDA events around each kernel on the launching stream;
  * ckks_profile_read(stage) resolves them and returns the accumulated device
  * milliseconds and launch count of a stage: 0 = ct-mult tensor, 1 = ct-mult
- * ModUp + key inner product, 2 = ct-mult ModDown + rescale, 3 = ckks_ntt.
+ * ModUp + key inner product, 2 = ct-mult ModDown + rescale, 3 = ckks_ntt,
+ * 4 = other kernels, 5 = the fused ct-mult kernel.
  * The reference has no runtime tracing (its timing comes from Vivado reports
  * and the cycle model of scripts/exp_e17_energy_efficiency.py:36-65).
  */

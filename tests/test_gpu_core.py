@@ -234,11 +234,14 @@ def test_ct_mul_concurrent_sub_batches_identical(ck):
     da, db = ops.to_device(a), ops.to_device(b)
     outs = []
     try:
+        _lib.call("ckks_ctx_set_tuning", ctx.handle, 7, 2)  # the three-kernel path (sub-batches apply to it)
         for split in (1, 2, 3, 4, 8, 16, 0):
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, split)
             outs.append(ops.to_host(ops.ct_mul_relin_rescale(ctx, da, db, key)))
     finally:
         _lib.call("ckks_ctx_set_tuning", ctx.handle, 2, 0)
+        _lib.call("ckks_ctx_set_tuning", ctx.handle, 7, 0)
+    outs.append(ops.to_host(ops.ct_mul_relin_rescale(ctx, da, db, key)))  # default: the fused kernel
     assert all(np.array_equal(o, outs[0]) for o in outs[1:])
     idx = [0, 85, 170, 255]
     assert np.array_equal(outs[0][idx], R.ct_mul_relin_rescale(a[idx], b[idx], ksk, qs, P.special))

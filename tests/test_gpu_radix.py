@@ -13,6 +13,7 @@ pytestmark = pytest.mark.gpu
 
 # ckks_ctx_set_tuning parameters
 CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC, CM_TMA = 0, 1, 2, 3, 4, 5
+CM_FUSED = 7  # 0 = fused kernel where built (default), 2 = the three-kernel path these shapes tune
 
 
 def _rand(rng, shape, basis):
@@ -31,8 +32,14 @@ def ck(cuda):
 
 
 def _reset(_lib, ctx):
-    for p in (CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC, CM_TMA):
+    for p in (CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC, CM_TMA, CM_FUSED):
         _lib.call("ckks_ctx_set_tuning", ctx.handle, p, 0)
+
+
+def _three_kernels(_lib, ctx):
+    """Route ct-mults through the three-kernel path, whose launch shapes the
+    tests sweep (the default fused kernel has one shape)."""
+    _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_FUSED, 2)
 
 
 @pytest.mark.parametrize("log_n", [6, 10, 12, 13])
@@ -93,6 +100,7 @@ def test_ct_mul_every_launch_shape_identical(ck, log_n, n_ct):
     shapes = _cm_shapes(log_n)
     assert {k for k, _ in shapes} >= {3, 4, 5}
     try:
+        _three_kernels(_lib, ctx)
         for k, mb in shapes:
             _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_K, k)
             _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_MINB, mb)
@@ -180,6 +188,7 @@ def test_unbuilt_shapes_refused(ck):
     a = ops.to_device(_rand(rng, (1, 2, 3, 8192), list(P.q)))
     key = ops.relin_key_prepare(ctx, ops.to_device(_rand(rng, (3, 2, 4, 8192), list(P.q) + [P.special])))
     try:
+        _three_kernels(_lib, ctx)
         for k, mb in ((2, 1), (5, 2)):  # K = 2 not built at N = 2^13; K = 5 balanced only
             _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_K, k)
             _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_MINB, mb)
@@ -208,6 +217,7 @@ def test_units_per_cta_identical(ck):
     rot = ops.to_host(ops.rotate(ctx, da, key, 5))
     assert np.array_equal(base[36:], R.ct_mul_relin_rescale(a[36:], b[36:], ksk, qs, P.special))
     try:
+        _three_kernels(_lib, ctx)
         for upc in (1, 2, 3, 4, 8):
             _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_UPC, upc)
             for k in (3, 4):
@@ -236,6 +246,7 @@ def test_tma_tensor_kernel_identical(ck, log_n, n_ct, level):
     key = ops.relin_key_prepare(ctx, ops.to_device(ksk))
     da, db = ops.to_device(a), ops.to_device(b)
     try:
+        _three_kernels(_lib, ctx)
         _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_TMA, 2)
         base = ops.to_host(ops.ct_mul_relin_rescale(ctx, da, db, key))
         for split in (1, 0):

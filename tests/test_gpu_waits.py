@@ -19,6 +19,7 @@ pytestmark = pytest.mark.gpu
 CKKS_ETIMEOUT = -2
 TUNE_TENSOR_TMA = 5
 TUNE_WAIT_CYCLES = 6
+TUNE_CM_FUSED = 7
 
 
 def _rand(rng, shape, basis):
@@ -50,6 +51,7 @@ def test_tma_tensor_wait_expiry_is_reported_and_recoverable(cuda):
     torch.cuda.synchronize()
     assert lib.ckks_device_status() == 0, lib.ckks_last_error().decode()
     try:
+        _lib.call("ckks_ctx_set_tuning", ctx.handle, TUNE_CM_FUSED, 2)  # the TMA-fed kernel is on that path
         _lib.call("ckks_ctx_set_tuning", ctx.handle, TUNE_TENSOR_TMA, 1)
         _lib.call("ckks_ctx_set_tuning", ctx.handle, TUNE_WAIT_CYCLES, 1)
         ops.ct_mul_relin_rescale(ctx, da, db, key)
@@ -68,6 +70,7 @@ def test_tma_tensor_wait_expiry_is_reported_and_recoverable(cuda):
     finally:
         _lib.call("ckks_ctx_set_tuning", ctx.handle, TUNE_WAIT_CYCLES, 0)
         _lib.call("ckks_ctx_set_tuning", ctx.handle, TUNE_TENSOR_TMA, 0)
+        _lib.call("ckks_ctx_set_tuning", ctx.handle, TUNE_CM_FUSED, 0)
 
 
 def test_wait_limit_rejects_negative(cuda):

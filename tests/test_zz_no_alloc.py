@@ -56,8 +56,9 @@ def test_noalloc_entry_matches_allocating_entry(cuda):
         torch.cuda.synchronize()
         assert np.array_equal(ops.to_host(out), ops.to_host(ref)), f"call {call} differs"
 
-    # one pair more than the static array holds is refused on the host
-    per_pair = ops.ct_mul_scratch_bytes(ctx, 1, level)
+    # one pair more than the static array holds is refused on the host (the
+    # entry runs the three-kernel path: (6 level + 2) limbs of scratch per pair)
+    per_pair = (6 * level + 2) * P.n * 8
     too_many = (32 * 1024 * 1024) // per_pair + 1
     rc = noalloc(ctx.handle, out.data_ptr(), a.data_ptr(), b.data_ptr(), key.data_ptr(),
                  too_many, level, stream)
@@ -87,7 +88,7 @@ def test_noalloc_entry_ignores_sub_batch_split(cuda):
     ksk = _rand(rng, (3, 2, 4, P.n), qs + [P.special])
     key = ops.relin_key_prepare(ctx, ops.to_device(ksk))
     n_ct, level = 160, 3
-    assert ops.ct_mul_scratch_bytes(ctx, n_ct, level) <= 32 * 1024 * 1024
+    assert n_ct * (6 * level + 2) * P.n * 8 <= 32 * 1024 * 1024
     stream = torch.cuda.current_stream().cuda_stream
     noalloc = lib.ckks_ct_mul_relin_rescale_noalloc
     try:
