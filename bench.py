@@ -59,6 +59,8 @@ def parse():
     ap.add_argument("--enc-mlp-batches", type=int, default=8)
     ap.add_argument("--no-convgap", action="store_true",
                     help="skip the fused conv+GAP (coefficient-encoded inner product) leg")
+    ap.add_argument("--linear-only", action="store_true",
+                    help="time only the encrypted linear layer (integer pipe and tensor cores), print it, exit")
     ap.add_argument("--ct-mult-path", choices=["three", "fused"], default="three",
                     help="three kernels through scratch (default) or the fused cluster kernel")
     ap.add_argument("--soak-seconds", type=float, default=1.2,
@@ -288,7 +290,7 @@ def measure_transforms(ctx, dev, hbm_peak: float, reps: int = 20) -> dict:
     res["poly_mul"] = {"products_per_s": npoly // 2 * nl / s, "GBps": byts / s / 1e9,
                        "frac_hbm": byts / s / 1e9 / hbm_peak}
     res["shape"] = f"N=2^{logn}, 45-bit primes, {npoly} polys x {nl} limbs per launch, 4 rotating buffers"
-    res["linear_mlp"] = measure_linear(dev, reps=reps)
+    res["linear_mlp"] = measure_linear(dev, reps=reps, hbm_peak=hbm_peak)
     return res
 
 
@@ -358,14 +360,20 @@ def measure_convgap(dev, hbm_peak: float, with_cpu: bool, reps: int = 20) -> dic
     return res
 
 
-def measure_linear(dev, reps: int = 10) -> dict:
+def measure_linear(dev, reps: int = 10, hbm_peak: float = 6550.0, bf16_peak: float = 1657.7) -> dict:
     """Encrypted FC layer of the MLP workload (784 -> 128 at N = 2^13, L = 4,
     50 % 4x4 block sparsity, weights at 2^20): inputs are 784 ciphertexts
-    (411 MB), one launch of ckks_linear_plain_weights per rep."""
+    (411 MB), one launch per rep, on the integer pipe (ckks_linear_plain_weights,
+    skips zero blocks) and on the tensor cores (ckks_linear_plain_weights_tc,
+    int8 byte-limb GEMM, dense).  The tensor-core roofline counts the 18 int8
+    limb GEMMs (2 x 18 x 128 x 896 x positions ops: features padded to the
+    128-feature chunk) against 2x the measured dense bf16 rate (the nominal
+    int8 : bf16 ratio of B200), and its algorithmic bytes (inputs read once,
+    outputs written once) against the measured HBM copy rate."""
     import math
     import numpy as np
     import torch
-    from ckks_b200 import _lib
+    from ckks_b200 import _lib, ops
     from ckks_b200.context import Context
     from ckks_b200.mlp import gear_keep, make_block_sparse
     from ckks_b200.params import CkksParams
@@ -373,61 +381,53 @@ def measure_linear(dev, reps: int = 10) -> dict:
     ctx = Context.get(13, P.primes, n_special=1)
     rng = np.random.default_rng(5)
     W = make_block_sparse(rng.standard_normal((128, 784)) / math.sqrt(784), 0.5, 6)
-    w = torch.from_numpy(np.round(W * 2 ** 20).astype(np.int32)).to(dev)
+    w_np = np.round(W * 2 ** 20).astype(np.int32)
+    w = torch.from_numpy(w_np).to(dev)
     keep_np = gear_keep(W, 0.0)
     keep = torch.from_numpy(keep_np).to(dev)
+    packed = ops.linear_tc_pack(w_np, keep_np, device=dev)
     npos = 2 * 4 * P.n
     x = torch.randint(0, 1 << 44, (784, npos), dtype=torch.int64, device=dev).view(torch.uint64)
     out = torch.empty((128, npos), dtype=torch.uint64, device=dev)
     bias = torch.zeros(128, dtype=torch.int64, device=dev)
     st = torch.cuda.current_stream().cuda_stream
 
-    def call():
+    def call_int():
         _lib.call("ckks_linear_plain_weights", ctx.handle, out.data_ptr(), x.data_ptr(), w.data_ptr(),
                   bias.data_ptr(), keep.data_ptr(), 128, 784, 4, st)
-    for _ in range(3):
-        call()
-    torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(reps):
-        call()
-    e1.record()
-    torch.cuda.synchronize()
-    s = e0.elapsed_time(e1) / reps / 1000.0
+
+    def call_tc():
+        _lib.call("ckks_linear_plain_weights_tc", ctx.handle, out.data_ptr(), x.data_ptr(), packed.data_ptr(),
+                  bias.data_ptr(), 128, 784, 4, st)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps / 1000.0
+    s_int = timed(call_int)
+    ref = out.clone()
+    s_tc = timed(call_tc)
+    if not torch.equal(out, ref):
+        raise RuntimeError("tensor-core linear layer differs from the integer-pipe layer")
     macs = 128 * 784 * npos * float(keep_np.mean())
-    return {"ms": s * 1e3, "TMAC_s": macs / s / 1e12, "kept_blocks": float(keep_np.mean()),
-            "shape": "784 -> 128, N=2^13, L=4, 784 input ciphertexts (411 MB)"}
-
-
-def measure_decoded(dev, log_n: int, levels: int, batch: int) -> dict:
-    """Decoded error of the ct-mult with a real key (the workload's parameters:
-    scale 2^40, ternary secret, discrete-Gaussian sigma 3.2 errors): `batch`
-    pairs of slot vectors uniform in [-1, 1] are encoded, encrypted,
-    multiplied, relinearised and rescaled, decrypted and decoded, and compared
-    with the FP64 product x * y.  max_rel_err is normwise: max |z - x y| over
-    max |x y| (elementwise ratios are unbounded where x y is near 0)."""
-    import numpy as np
-    import torch
-    from ckks_b200.evaluator import Evaluator
-    from ckks_b200.params import CkksParams
-    ev = Evaluator(CkksParams.standard(log_n, levels, seed=11), device=dev)
-    ev.keygen()
-    rng = np.random.default_rng(12)
-    slots = (1 << log_n) // 2
-    x = rng.uniform(-1, 1, (batch, slots))
-    y = rng.uniform(-1, 1, (batch, slots))
-    z = ev.decrypt_values(ev.mul_relin_rescale(ev.encrypt_values(x, level=levels),
-                                               ev.encrypt_values(y, level=levels)), slots)
-    z = z.cpu().numpy() if isinstance(z, torch.Tensor) else np.asarray(z)
-    ref = x * y
-    err = np.abs(z.real - ref)
-    return {"pairs": batch, "slots_per_ct": slots, "max_abs_err": float(err.max()),
-            "mean_abs_err": float(err.mean()), "max_rel_err": float(err.max() / np.abs(ref).max()),
-            "max_abs_imag": float(np.abs(z.imag).max()),
-            "rel_err_definition": "max |z - x y| / max |x y| (normwise)",
-            "params": f"N=2^{log_n}, L={levels}, scale 2^40, ternary secret, DG sigma 3.2, real key"}
+    tc_ops = 2 * 18 * 128 * 896 * npos
+    byts = 784 * npos * 8 + 128 * npos * 8
+    return {"shape": "784 -> 128, N=2^13, L=4, 784 input ciphertexts (411 MB)", "kept_blocks": float(keep_np.mean()),
+            "int_pipe": {"ms": s_int * 1e3, "TMAC_s": macs / s_int / 1e12},
+            "tensor_core": {"ms": s_tc * 1e3, "int8_TOPS": tc_ops / s_tc / 1e12,
+                            "frac_of_2x_bf16_peak": tc_ops / s_tc / 1e12 / (2 * bf16_peak),
+                            "GBps": byts / s_tc / 1e9, "frac_hbm": byts / s_tc / 1e9 / hbm_peak},
+            "speedup_tc_over_int": s_int / s_tc, "bit_identical": True,
+            # the previous keys, kept for readers of earlier lines
+            "ms": s_tc * 1e3, "TMAC_s": macs / s_tc / 1e12}
 
 
 def _lib_call_poly_mul(ctx, out, a, b, nl):
@@ -748,6 +748,11 @@ def run_ours(a) -> int:
 
 def main() -> int:
     a = parse()
+    if a.linear_only:
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"linear_mlp": measure_linear(torch.device("cuda", 0), reps=max(3, a.steps))}), flush=True)
+        return 0
     ws, _, _ = dist_env()
     if ws > 1:
         a.gpus = ws

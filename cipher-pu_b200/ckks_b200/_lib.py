@@ -67,6 +67,9 @@ SIGNATURES: dict[str, tuple] = {
     "ckks_rns_split": (_i32, [C.POINTER(_u64), _i32, _u64p, _u64p, _i64, _i32, _i32, _vp]),
     "ckks_rns_merge": (_i32, [C.POINTER(_u64), _i32, _u64p, _u64p, _i64, _i32, _i32, _vp]),
     "ckks_linear_plain_weights": (_i32, [_vp, _u64p, _u64p, _vp, _vp, _vp, _i32, _i32, _i32, _vp]),
+    "ckks_linear_tc_packed_bytes": (_sz, [_i32, _i32]),
+    "ckks_linear_tc_pack": (_i32, [_vp, _sz, _vp, _vp, _i32, _i32]),
+    "ckks_linear_plain_weights_tc": (_i32, [_vp, _u64p, _u64p, _vp, _vp, _i32, _i32, _i32, _vp]),
     "ckks_ct_mul_plain_rescale": (_i32, [_vp, _u64p, _u64p, _u64p, _i32, _i32, _i32, _vp]),
     "ckks_relin_single_masked": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _u64p, _u64p, _u64p, _u64p,
                                         _u64p, _i32, _i32, _vp]),

@@ -85,6 +85,7 @@ class Layer:
     w_int: torch.Tensor = None       # int32 [O, F] on device (round(W 2^wbits))
     keeps: list = field(default_factory=list)   # per gear: uint8 device masks
     keeps_np: list = field(default_factory=list)
+    packed: list = None              # per gear: tensor-core weight images (None: integer pipe)
 
 
 @dataclass
@@ -95,11 +96,23 @@ class ProbeResult:
     nsr: float
 
 
+# largest |w| that three balanced signed byte limbs hold (tensor-core layer)
+TC_W_MAX = 127 * (1 + 256 + 65536)
+
+
 class EncryptedMLP:
-    def __init__(self, ev: Evaluator, layers: list, wbits: int = 20, dare_shift: int | None = None):
+    """tensor_cores: run the linear layers on the tensor cores
+    (ckks_linear_plain_weights_tc, bit-identical to the integer-pipe layer and
+    5x faster on the MLP shape, but dense: a gear's dropped blocks are
+    multiplied as zeros); False keeps the integer pipe, whose time shrinks
+    with each gear's kept fraction."""
+
+    def __init__(self, ev: Evaluator, layers: list, wbits: int = 20, dare_shift: int | None = None,
+                 tensor_cores: bool = True):
         self.ev = ev
         self.wbits = wbits
         self.layers = [l if isinstance(l, Layer) else Layer(*l) for l in layers]
+        self.tensor_cores = tensor_cores
         dev = ev.device
         for L in self.layers:
             wq = np.round(L.W * (1 << wbits))
@@ -108,6 +121,8 @@ class EncryptedMLP:
             L.w_int = torch.from_numpy(wq.astype(np.int32)).to(dev).contiguous()
             L.keeps_np = [gear_keep(L.W, s) for s in GEAR_SPARSITY]
             L.keeps = [torch.from_numpy(k).to(dev).contiguous() for k in L.keeps_np]
+            if tensor_cores and np.abs(wq).max() <= TC_W_MAX and L.W.shape[1] <= 2048:
+                L.packed = [ops.linear_tc_pack(wq.astype(np.int64), k, device=dev) for k in L.keeps_np]
         self.dare_shift = dare_shift
         self.timers = {}
 
@@ -134,9 +149,12 @@ class EncryptedMLP:
         out = torch.empty((O, 2, level, self.ev.n), dtype=torch.uint64, device=self.ev.device)
         bias = torch.from_numpy(np.round(L.b * X.scale * (1 << self.wbits)).astype(np.int64)).to(
             self.ev.device).contiguous()
-        _lib.call("ckks_linear_plain_weights", self.ev.ctx.handle, out.data_ptr(), X.data.data_ptr(),
-                  L.w_int.data_ptr(), bias.data_ptr(), L.keeps[gear].data_ptr(), O, F, level,
-                  torch.cuda.current_stream().cuda_stream)
+        if L.packed is not None:
+            ops.linear_plain_weights_tc(self.ev.ctx, X.data, L.packed[gear], O, bias=bias, out=out)
+        else:
+            _lib.call("ckks_linear_plain_weights", self.ev.ctx.handle, out.data_ptr(), X.data.data_ptr(),
+                      L.w_int.data_ptr(), bias.data_ptr(), L.keeps[gear].data_ptr(), O, F, level,
+                      torch.cuda.current_stream().cuda_stream)
         return Ciphertext(out, X.scale * (1 << self.wbits))
 
     def square(self, Y: Ciphertext) -> Ciphertext:

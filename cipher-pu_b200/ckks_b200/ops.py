@@ -430,3 +430,29 @@ def sample_dgauss(shape, sigma: float, seed: int, stream_id: int, device=None) -
     _lib.call("ckks_sample_dgauss", out.data_ptr(), out.numel(), float(sigma), int(seed) & (2 ** 64 - 1),
               int(stream_id) & (2 ** 64 - 1), _stream())
     return out
+
+
+# ---------------------------------------------------------------- tensor-core linear layer
+def linear_tc_pack(w: np.ndarray, keep: np.ndarray | None = None, device=None) -> torch.Tensor:
+    """int weights [O, F] (|w| <= 8355711) and an optional 4x4 block-keep mask
+    -> the packed byte-limb image on the device (ckks_linear_tc_pack)."""
+    import ctypes as C
+    w = np.ascontiguousarray(np.asarray(w, dtype=np.int32))
+    O, F = w.shape
+    nbytes = int(_lib.raw("ckks_linear_tc_packed_bytes")(O, F))
+    host = np.zeros(nbytes, dtype=np.uint8)
+    k = None if keep is None else np.ascontiguousarray(np.asarray(keep, dtype=np.uint8))
+    _lib.call("ckks_linear_tc_pack", host.ctypes.data, nbytes, w.ctypes.data,
+              None if k is None else k.ctypes.data, O, F)
+    return torch.from_numpy(host).to(device or torch.device("cuda", torch.cuda.current_device()))
+
+
+def linear_plain_weights_tc(ctx: Context, x: torch.Tensor, packed: torch.Tensor, n_out: int,
+                            bias: torch.Tensor | None = None, out: torch.Tensor | None = None) -> torch.Tensor:
+    """x [F, 2, level, N] ciphertexts -> [n_out, 2, level, N] on the tensor cores."""
+    F, two, level, n = x.shape
+    if out is None:
+        out = torch.empty((n_out, 2, level, n), dtype=U64, device=x.device)
+    _lib.call("ckks_linear_plain_weights_tc", ctx.handle, _p(out), _p(x), packed.data_ptr(),
+              None if bias is None else bias.data_ptr(), n_out, F, level, _stream())
+    return out

@@ -413,15 +413,21 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
   __syncthreads();  // no thread leaves before the drain
 }
 
+// expiries of the tensor-core linear layer's waits (linear_tc.cu), read and cleared
+int ckks_linear_tc_status_take(unsigned int* n);
+
 extern "C" int ckks_device_status(void) {
-  unsigned int n = 0;
+  unsigned int n = 0, n_tc = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&n, g_cm_wait_expiries, sizeof(n));
   if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "ckks_device_status: %s", cudaGetErrorString(e));
-  if (n == 0) return CKKS_OK;
-  const unsigned int zero = 0;
-  e = cudaMemcpyToSymbol(g_cm_wait_expiries, &zero, sizeof(zero));
-  if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "ckks_device_status: %s", cudaGetErrorString(e));
-  return ckks_set_error(CKKS_ETIMEOUT, "ckks_device_status: %u bounded device waits expired", n);
+  if (n) {
+    const unsigned int zero = 0;
+    e = cudaMemcpyToSymbol(g_cm_wait_expiries, &zero, sizeof(zero));
+    if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "ckks_device_status: %s", cudaGetErrorString(e));
+  }
+  if (int rc = ckks_linear_tc_status_take(&n_tc)) return rc;
+  if (n + n_tc == 0) return CKKS_OK;
+  return ckks_set_error(CKKS_ETIMEOUT, "ckks_device_status: %u bounded device waits expired", n + n_tc);
 }
 
 // ---------------------------------------------------------------- kernel B

@@ -122,7 +122,8 @@ int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value);
 
 /*
  * Device-side status of the kernels that wait on asynchronous copies with a
- * bounded spin (the TMA-fed ct-mult tensor kernel): CKKS_ETIMEOUT (and the
+ * bounded spin (the TMA-fed ct-mult tensor kernel, the tensor-core linear
+ * layer's MMA completions): CKKS_ETIMEOUT (and the
  * count in ckks_last_error) when any such wait on the current device expired
  * since the last call, which leaves those outputs incomplete; CKKS_OK
  * otherwise.  Synchronises the device; clears the count.
@@ -443,6 +444,27 @@ int ckks_sample_dgauss(int64_t* out, int64_t n, double sigma, uint64_t seed, uin
 int ckks_linear_plain_weights(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in,
                               const int32_t* w, const int64_t* bias, const uint8_t* block_keep,
                               int n_out, int n_in, int level, void* stream);
+
+/*
+ * The same encrypted linear layer on the tensor cores (tcgen05.mma kind::i8,
+ * accumulators in TMEM): residues split into 6 unsigned bytes, weights into 3
+ * balanced signed bytes, the 18 byte GEMMs accumulated exactly in int32 per
+ * limb sum and recombined mod q in the epilogue.  Bit-identical to
+ * ckks_linear_plain_weights.  Weights first go through ckks_linear_tc_pack
+ * (host memory in and out, once per weight matrix and block mask; |w| <=
+ * 8355711 = 127 (1 + 256 + 256^2), else CKKS_EINVAL), and the packed buffer
+ * (ckks_linear_tc_packed_bytes, copied to the device, 16-byte aligned) is
+ * passed here.  The 4x4 block mask is applied by the pack; dropped blocks are
+ * multiplied as zeros (the tensor-core work does not shrink with sparsity).
+ * n_in <= 2048, N >= 32.  Replaces the same reference layer as
+ * ckks_linear_plain_weights (scripts/exp_e11_ckks_e2e_real.py:142).
+ */
+size_t ckks_linear_tc_packed_bytes(int n_out, int n_in);
+int ckks_linear_tc_pack(void* packed_host, size_t packed_bytes, const int32_t* w_host,
+                        const uint8_t* block_keep_host, int n_out, int n_in);
+int ckks_linear_plain_weights_tc(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in,
+                                 const void* packed, const int64_t* bias, int n_out, int n_in,
+                                 int level, void* stream);
 
 /*
  * Learned gear controller network (no counterpart in the reference, whose
