@@ -56,7 +56,7 @@ def parse():
                     help="skip the standalone NTT / poly-mult measurement")
     ap.add_argument("--no-enc-mlp", action="store_true",
                     help="skip the encrypted-MLP learned-vs-plain gear leg")
-    ap.add_argument("--enc-mlp-batches", type=int, default=8)
+    ap.add_argument("--enc-mlp-batches", type=int, default=16)
     ap.add_argument("--no-convgap", action="store_true",
                     help="skip the fused conv+GAP (coefficient-encoded inner product) leg")
     ap.add_argument("--linear-only", action="store_true",
@@ -430,6 +430,35 @@ def measure_linear(dev, reps: int = 10, hbm_peak: float = 6550.0, bf16_peak: flo
             "ms": s_tc * 1e3, "TMAC_s": macs / s_tc / 1e12}
 
 
+def measure_decoded(dev, log_n: int, levels: int, batch: int) -> dict:
+    """Decoded error of the ct-mult with a real key (the workload's parameters:
+    scale 2^40, ternary secret, discrete-Gaussian sigma 3.2 errors): `batch`
+    pairs of slot vectors uniform in [-1, 1] are encoded, encrypted,
+    multiplied, relinearised and rescaled, decrypted and decoded, and compared
+    with the FP64 product x * y.  max_rel_err is normwise: max |z - x y| over
+    max |x y| (elementwise ratios are unbounded where x y is near 0)."""
+    import numpy as np
+    import torch
+    from ckks_b200.evaluator import Evaluator
+    from ckks_b200.params import CkksParams
+    ev = Evaluator(CkksParams.standard(log_n, levels, seed=11), device=dev)
+    ev.keygen()
+    rng = np.random.default_rng(12)
+    slots = (1 << log_n) // 2
+    x = rng.uniform(-1, 1, (batch, slots))
+    y = rng.uniform(-1, 1, (batch, slots))
+    z = ev.decrypt_values(ev.mul_relin_rescale(ev.encrypt_values(x, level=levels),
+                                               ev.encrypt_values(y, level=levels)), slots)
+    z = z.cpu().numpy() if isinstance(z, torch.Tensor) else np.asarray(z)
+    ref = x * y
+    err = np.abs(z.real - ref)
+    return {"pairs": batch, "slots_per_ct": slots, "max_abs_err": float(err.max()),
+            "mean_abs_err": float(err.mean()), "max_rel_err": float(err.max() / np.abs(ref).max()),
+            "max_abs_imag": float(np.abs(z.imag).max()),
+            "rel_err_definition": "max |z - x y| / max |x y| (normwise)",
+            "params": f"N=2^{log_n}, L={levels}, scale 2^40, ternary secret, DG sigma 3.2, real key"}
+
+
 def _lib_call_poly_mul(ctx, out, a, b, nl):
     import torch
     from ckks_b200 import _lib
@@ -662,21 +691,39 @@ def run_ours(a) -> int:
         transforms = measure_transforms(ctx, dev, hbm) if not a.no_transforms else None
         convgap = (measure_convgap(dev, hbm, with_cpu=not a.no_cpu_baseline)
                    if not a.no_convgap and ws == 1 else None)
-        enc_mlp = None
+        enc_mlp = enc_cnn = None
         if not a.no_enc_mlp and ws == 1:
             # second half of the metric: encrypted MLP 784-128-10 (N=2^13, L=4,
             # batch 1024, DARE between layers) under the plain SNR-monitor
             # gear controller and the learned one, same inputs
             from ckks_b200.train_gear import compare
-            r = compare(model="mlp", batches=a.enc_mlp_batches)
-            enc_mlp = {"metric": "enc-MLP samples/s learned vs plain gear", "unit": "samples/s",
-                       "plain": r["plain"]["samples_per_s"], "learned": r["learned"]["samples_per_s"],
-                       "speedup": r["speedup"], "snr_db_plain": r["plain"]["snr_db"],
-                       "snr_db_learned": r["learned"]["snr_db"],
-                       "top1_plain": r["plain"]["top1_agreement"], "top1_learned": r["learned"]["top1_agreement"],
-                       "probes_plain": r["plain"]["probes"], "probes_learned": r["learned"]["probes"],
-                       "workload": f"784-128-10, N=2^13, L=4, {r['batches']} batches of {r['batch']} samples, "
-                                   f"target {r['target_db']} dB, synthetic uniform [0,1] inputs, random weights"}
+            def gear_leg(model: str, batches: int, workload: str) -> dict:
+                r = compare(model=model, batches=batches)
+                return {"metric": f"enc-{model.upper()} samples/s learned vs plain gear", "unit": "samples/s",
+                        "plain": r["plain"]["samples_per_s"], "learned": r["learned"]["samples_per_s"],
+                        "speedup": r["speedup"], "snr_db_plain": r["plain"]["snr_db"],
+                        "snr_db_learned": r["learned"]["snr_db"], "snr_gap_db": r["snr_gap_db"],
+                        "top1_plain": r["plain"]["top1_agreement"], "top1_learned": r["learned"]["top1_agreement"],
+                        "probes_plain": r["plain"]["probes"], "probes_learned": r["learned"]["probes"],
+                        "recomputed_layers_plain": r["plain"]["recomputed_layers"],
+                        "recomputed_layers_learned": r["learned"]["recomputed_layers"],
+                        "gear_histogram_plain": r["plain_gear_histogram"],
+                        "gear_histogram_learned": r["learned_gear_histogram"],
+                        "attempted_gear_histogram_plain": r["plain_attempted_histogram"],
+                        "attempted_gear_histogram_learned": r["learned_attempted_histogram"],
+                        "gear_histogram_layout": "[layer][gear 0..3] = batch-layers whose result used that gear "
+                                                 "(attempted: chosen before a failed probe forced a gear-0 recompute); "
+                                                 "two alternating runs per arm",
+                        "samples_per_s_runs_plain": r["plain"]["samples_per_s_runs"],
+                        "samples_per_s_runs_learned": r["learned"]["samples_per_s_runs"],
+                        "workload": f"{workload}, {r['batches']} batches of {r['batch']} samples, target "
+                                    f"{r['target_db']} dB, synthetic uniform [0,1] inputs, random weights",
+                        "controllers": "plain: the RTL gear state machine (adaptive_gear_ctrl) fed by the decrypt-"
+                                       "based monitor after every layer; learned: the trained 16-64-64-4 predictor, "
+                                       "calibrated on the first batch inside the timed region, probing on audits"}
+            enc_mlp = gear_leg("mlp", a.enc_mlp_batches, "784-128-10, N=2^13, L=4")
+            enc_cnn = gear_leg("cnn", max(4, a.enc_mlp_batches // 2),
+                               "conv 5x5x8 s2 + x^2 + 2x2 avg-pool + FC 288->10, N=2^13, L=5")
         decoded = measure_decoded(dev, a.log_n, a.levels, a.batch) if not a.no_decoded else None
         cpu = None
         if ws == 1 and not a.no_cpu_baseline:
@@ -704,6 +751,7 @@ def run_ours(a) -> int:
             "transforms": transforms,
             "convgap": convgap,
             "enc_mlp": enc_mlp,
+            "enc_cnn": enc_cnn,
             "stage_ms_per_step": {names[s]: stages[s][0] / max(1, prof_steps) for s in active},
             "stage_timing": (f"library event profiler over {prof_steps} identical steps right after the timed "
                              "region, each kernel launched alone over the whole batch"),

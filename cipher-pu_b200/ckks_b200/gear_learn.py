@@ -175,16 +175,41 @@ def random_layer(rng, F: int, O: int, act: str, base_sparsity: float) -> Layer:
     return Layer(W, b, act)
 
 
+def random_conv_layer(rng, act: str) -> Layer:
+    """A random convolution over a 28 x 28 image as a sparse matrix (channels
+    in {4, 8}, kernel 3 or 5, stride 2; the C channels of an output pixel on
+    adjacent rows), the structure of the encrypted CNN's first layer."""
+    C = int(rng.choice([4, 8]))
+    K = int(rng.choice([3, 5]))
+    S, IN = 2, 28
+    OUT = (IN - K) // S + 1
+    kern = rng.standard_normal((C, K, K)) / math.sqrt(K * K)
+    W = np.zeros((C * OUT * OUT, IN * IN))
+    for c in range(C):
+        for i in range(OUT):
+            for j in range(OUT):
+                r = (i * OUT + j) * C + c
+                for di in range(K):
+                    W[r, (S * i + di) * IN + S * j:(S * i + di) * IN + S * j + K] = kern[c, di]
+    return Layer(W, np.tile(rng.standard_normal(C) * 0.1, OUT * OUT), act)
+
+
 def gen_traces(ev, n_traces: int, seed: int = 0, batch: int = 256, progress=None) -> tuple:
-    """Run random encrypted layers at all four gears; one trace per neuron."""
+    """Run random encrypted layers at all four gears; one trace per neuron.
+    Three in ten are convolution-structured (random_conv_layer), the rest
+    dense block-sparse layers of the MLP family."""
     rng = np.random.default_rng(seed)
     Xs, Ts = [], []
     total = 0
     while total < n_traces:
-        F = int(rng.choice([128, 256, 512, 784]))
-        O = int(rng.choice([16, 32, 64, 128]))
         act = "square" if rng.random() < 0.7 else "none"
-        L = random_layer(rng, F, O, act, float(rng.choice([0.25, 0.5, 0.75])))
+        if rng.random() < 0.3:
+            L = random_conv_layer(rng, act)
+        else:
+            F = int(rng.choice([128, 256, 512, 784]))
+            O = int(rng.choice([16, 32, 64, 128]))
+            L = random_layer(rng, F, O, act, float(rng.choice([0.25, 0.5, 0.75])))
+        O, F = L.W.shape
         m = EncryptedMLP(ev, [L])
         lo, hi = sorted(rng.uniform(0.0, 1.5, 2))
         x = rng.uniform(lo, hi + 0.05, (batch, F))
@@ -201,9 +226,13 @@ def gen_traces(ev, n_traces: int, seed: int = 0, batch: int = 256, progress=None
             err = ((d - ref.T) ** 2).sum(1)
             sig = (ref.T ** 2).sum(1) + 1e-300
             T[:, g] = 10 * np.log10(sig / np.maximum(err, 1e-300))
-        Xs.append(layer_features(m, 0, x, None, X.level, X.scale))
+        feats = layer_features(m, 0, x, None, X.level, X.scale)
+        if O > 128:   # a convolution's many neurons: a random 128 of them, so no layer kind dominates
+            rows = rng.choice(O, 128, replace=False)
+            feats, T = feats[rows], T[rows]
+        Xs.append(feats)
         Ts.append(T)
-        total += O
+        total += len(T)
         if progress:
             progress(total)
     return np.concatenate(Xs)[:n_traces], np.concatenate(Ts)[:n_traces]
@@ -217,37 +246,38 @@ def layer_snr_from_neurons(snr_db: np.ndarray, sig_weight: np.ndarray | None = N
     return -10 * np.log10((w[:, None] * nsr).sum(0) / w.sum())
 
 
-class PlainController:
-    """Probe after every layer; downgrade at once when the SNR misses the
-    target, upgrade one gear after `hyst` consecutive measurements at least
-    `margin` dB above target; reset gear 3."""
+def nsr_energy(nsr: float) -> int:
+    """A probe's noise-to-signal energy ratio as the integer energy the RTL
+    controller compares (fixed point, 2^48 = an NSR of 1)."""
+    return int(min(max(nsr, 0.0), 2.0 ** 60) * float(1 << 48))
 
-    def __init__(self, n_layers: int, target_db: float, margin_db: float = 10.0, hyst: int = 3,
-                 reset_gear: int = 3):
-        self.target, self.margin, self.hyst = target_db, margin_db, hyst
-        self.gear = [reset_gear] * n_layers
-        self.count = [0] * n_layers
+
+class PlainController:
+    """The reference's gear controller, rtl/m4/adaptive_gear_ctrl.sv:43-99,
+    run by the library's C state machine (gear.GearCtrl) with one instance per
+    layer, fed by the decrypt-based monitor after every layer of every batch
+    (the RTL's monitor runs on every flush).  The monitor's noise energy (NSR)
+    maps to a raw gear through three thresholds: NSR >= the target's -> gear 0,
+    >= target's / 10^(step/10) -> 1, >= target's / 10^(2 step/10) -> 2,
+    cleaner -> 3; a lower raw gear takes effect at once, a higher one after
+    HYST_CNT agreeing readings; reset gear 3."""
+
+    def __init__(self, n_layers: int, target_db: float, step_db: float = 10.0, hyst: int = 3):
+        from .gear import GearCtrl
+        self.target = target_db
+        th = [nsr_energy(10.0 ** (-(target_db + k * step_db) / 10.0)) for k in range(3)]
+        self.ctl = [GearCtrl(thresholds=tuple(th), hyst_cnt=hyst) for _ in range(n_layers)]
         self.probes = 0
 
     def choose(self, li, info):
-        return self.gear[li]
+        return self.ctl[li].gear
 
     def probe_policy(self, li, g, info):
         self.probes += 1
         return True
 
     def on_probe(self, pr):
-        li = pr.layer
-        if pr.snr_db < self.target:
-            self.gear[li] = max(0, self.gear[li] - 1)
-            self.count[li] = 0
-        elif pr.snr_db >= self.target + self.margin and self.gear[li] < N_GEAR - 1:
-            self.count[li] += 1
-            if self.count[li] > self.hyst:
-                self.gear[li] += 1
-                self.count[li] = 0
-        else:
-            self.count[li] = 0
+        self.ctl[pr.layer].flush(nsr_energy(pr.nsr))
 
 
 class LearnedController:
@@ -269,6 +299,13 @@ class LearnedController:
         self.stats = {}
         self.calls = [0] * len(m.layers)
 
+    # Calibration: until a layer's input statistics are known (the first
+    # batch), the controller runs gear 0 and probes every layer; the probes'
+    # decrypted layer inputs give the statistics (ProbeResult.input_stats), so
+    # the features come from monitor quantities measured inside the stream.
+    def calibrated(self, li: int) -> bool:
+        return li in self.stats
+
     def set_input_stats(self, li: int, stats: dict):
         self.stats[li] = stats
         self.pred.pop(li, None)
@@ -277,19 +314,24 @@ class LearnedController:
         key = (info["level"], round(math.log2(info["scale"]), 3))
         hit = self.pred.get(li)
         if hit is None or hit[0] != key:
-            st = self.stats.get(li) or self.stats.get(0)
+            st = self.stats[li]
             feats = layer_features(self.m, li, None, st, info["level"], info["scale"])
             hit = (key, layer_snr_from_neurons(self.net.predict(feats)))
             self.pred[li] = hit
         return hit[1]
 
     def choose(self, li, info):
+        if not self.calibrated(li):
+            return 0
         p = self.predicted(li, info)
         ok = [g for g in range(N_GEAR) if p[g] >= self.target + self.margin and g <= self.cap[li]]
         return max(ok) if ok else 0
 
     def probe_policy(self, li, g, info):
         self.calls[li] += 1
+        if not self.calibrated(li):
+            self.probes += 1
+            return True
         p = self.predicted(li, info)
         need = ((li, g) not in self.verified or abs(p[g] - self.target) < self.band
                 or (self.audit and self.calls[li] % self.audit == 0))
@@ -298,6 +340,8 @@ class LearnedController:
         return need
 
     def on_probe(self, pr):
+        if pr.input_stats is not None and not self.calibrated(pr.layer):
+            self.set_input_stats(pr.layer, pr.input_stats)
         if pr.snr_db < self.target:
             self.cap[pr.layer] = max(0, pr.gear - 1)
             self.verified.discard((pr.layer, pr.gear))

@@ -65,7 +65,7 @@ def run_stream(m: EncryptedMLP, ctrl, batches: list, ref_layers: list | None = N
     ref_layers = ref_layers or m.layers
     sig = err = 0.0
     agree = total = 0
-    gears = []
+    gears, attempted = [], []
     recomputed = 0
     t_total = 0.0
     per_batch_snr = []
@@ -85,10 +85,12 @@ def run_stream(m: EncryptedMLP, ctrl, batches: list, ref_layers: list | None = N
         agree += int((d.argmax(1) == ref.argmax(1)).sum())
         total += len(x)
         gears.append(r["gears"])
+        attempted.append(r["attempted_gears"])
         recomputed += r["recomputed"]
         if calibrate:
             calibrate(r)
     return {"samples": total, "seconds": t_total, "samples_per_s": total / t_total,
             "snr_db": 10 * math.log10(sig / max(err, 1e-300)), "top1_agreement": agree / total,
             "probes": getattr(ctrl, "probes", None), "recomputed_layers": recomputed, "gears": gears,
+            "attempted_gears": attempted,
             "min_batch_snr_db": min(per_batch_snr)}

@@ -64,25 +64,41 @@ def compare(net_path: Path = DEFAULT_NET, model: str = "mlp", batches: int = 8, 
     m = EncryptedMLP(ev, layers)
     rng = np.random.default_rng(seed + 1)
     data = [rng.uniform(0, 1, (batch, 784)) for _ in range(batches)]
-    # warm-up (kernels, contexts)
-    m.forward(data[0][:64], lambda li, info: 0)
-    plain = PlainController(len(layers), target_db)
-    rp = run_stream(m, plain, data, fallback_db=target_db)
+    # warm-up: a full batch at every gear with every probe (kernels, weight
+    # images, cached biases, allocator), so neither arm pays first-use costs
+    for g in range(4):
+        m.forward(data[0], lambda li, info, g=g: g)
     net = GearNet.load(net_path)
-    learned = LearnedController(m, net, target_db)
-    # input statistics per layer from one calibration pass (probed, counted)
-    cal = m.forward(data[0][:256], lambda li, info: 0)
-    x_in = data[0][:256]
-    for li, L in enumerate(layers):
-        learned.set_input_stats(li, {"mean": float(x_in.mean()), "std": float(x_in.std()),
-                                     "ms": float((x_in ** 2).mean())})
-        h = x_in @ L.W.T + L.b
-        x_in = h * h if L.act == "square" else h
-    learned.probes += len(layers)
-    rl = run_stream(m, learned, data, fallback_db=target_db)
+    # the arms alternate, twice each, with fresh controllers (so a warm or
+    # cold GPU favours neither); the learned controller calibrates itself on
+    # each stream's first batch (probes of every layer, timed, counted)
+    runs = {"plain": [], "learned": []}
+    for _ in range(2):
+        runs["plain"].append(run_stream(m, PlainController(len(layers), target_db), data, fallback_db=target_db))
+        runs["learned"].append(run_stream(m, LearnedController(m, net, target_db), data, fallback_db=target_db))
+
+    def merged(rs):
+        r = dict(rs[-1])
+        r["seconds"] = sum(x["seconds"] for x in rs)
+        r["samples"] = sum(x["samples"] for x in rs)
+        r["samples_per_s"] = r["samples"] / r["seconds"]
+        r["samples_per_s_runs"] = [x["samples_per_s"] for x in rs]
+        return r
+    rp, rl = merged(runs["plain"]), merged(runs["learned"])
+
+    def hist(gears):
+        h = np.zeros((len(layers), 4), dtype=int)
+        for per_batch in gears:
+            for li, g in enumerate(per_batch):
+                h[li, g] += 1
+        return h.tolist()
+    drop = ("gears", "attempted_gears")
     return {"model": model, "target_db": target_db, "batch": batch, "batches": batches,
-            "plain": {k: v for k, v in rp.items() if k != "gears"}, "plain_gears": rp["gears"],
-            "learned": {k: v for k, v in rl.items() if k != "gears"}, "learned_gears": rl["gears"],
+            "plain": {k: v for k, v in rp.items() if k not in drop}, "plain_gears": rp["gears"],
+            "learned": {k: v for k, v in rl.items() if k not in drop}, "learned_gears": rl["gears"],
+            "plain_gear_histogram": hist(rp["gears"]), "learned_gear_histogram": hist(rl["gears"]),
+            "plain_attempted_histogram": hist(rp["attempted_gears"]),
+            "learned_attempted_histogram": hist(rl["attempted_gears"]),
             "speedup": rl["samples_per_s"] / rp["samples_per_s"],
             "snr_gap_db": rl["snr_db"] - rp["snr_db"]}
 

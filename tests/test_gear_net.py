@@ -73,14 +73,71 @@ def test_gpu_training_reduces_loss(cuda):
 
 @pytest.mark.gpu
 def test_learned_controller_gains_over_plain(cuda):
-    """The trained predictor lets the controller skip most SNR probes: at least
-    1.15x the plain controller's samples/s, SNR no worse than 0.5 dB below, the
-    same top-1 agreement, on the encrypted MLP (N = 2^13, L = 4)."""
+    """Encrypted MLP 784-128-10 (N = 2^13, L = 4), 16 batches, target 40 dB.
+    Plain: the RTL gear state machine fed by the decrypt-based monitor after
+    every layer; with random weights every sparse gear misses the target, and
+    the RTL rule keeps re-attempting gear 3 after each HYST_CNT + 1 clean
+    readings (a failed probe, then a gear-0 recompute).  Learned: calibrated on
+    the first batch inside the timed region, then audits only; it never
+    attempts a gear its predictor puts below the target.  Equal SNR (within
+    0.5 dB), equal top-1 agreement, fewer probes, and at least 1.3x the plain
+    arm's samples/s (the driver's bench reports the measured ratio)."""
     if not NET.exists():
         pytest.fail(f"trained gear network missing: {NET}")
     from ckks_b200.train_gear import compare
-    r = compare(NET, "mlp", batches=8, batch=1024)
+    r = compare(NET, "mlp", batches=16, batch=1024)
     assert r["learned"]["probes"] < r["plain"]["probes"]
-    assert r["learned"]["snr_db"] >= r["plain"]["snr_db"] - 0.5
-    assert r["learned"]["top1_agreement"] >= r["plain"]["top1_agreement"]
-    assert r["speedup"] >= 1.15, r
+    assert abs(r["snr_gap_db"]) <= 0.5
+    assert r["learned"]["top1_agreement"] == r["plain"]["top1_agreement"]
+    assert r["learned"]["recomputed_layers"] == 0
+    assert sum(r["plain_attempted_histogram"][0][1:]) > 0          # the RTL rule's upgrade attempts
+    assert sum(r["learned_attempted_histogram"][0][1:]) == 0
+    assert r["speedup"] >= 1.3, r
+
+
+@pytest.mark.gpu
+def test_learned_vs_plain_encrypted_cnn(cuda):
+    """Config 5: the encrypted CNN (conv 5x5x8 s2, x^2, 2x2 average pool, FC
+    288 -> 10) at N = 2^13, L = 5, 8 batches: both arms at the same SNR (above
+    60 dB against the FP64 model) and top-1; the learned arm needs fewer probes,
+    no recomputes, and is not slower."""
+    from ckks_b200.train_gear import compare
+    r = compare(NET, "cnn", batches=8, batch=1024)
+    assert r["plain"]["snr_db"] > 60 and r["learned"]["snr_db"] > 60
+    assert abs(r["snr_gap_db"]) <= 0.5
+    assert r["learned"]["top1_agreement"] == r["plain"]["top1_agreement"]
+    assert r["learned"]["probes"] < r["plain"]["probes"]
+    assert r["learned"]["recomputed_layers"] == 0
+    assert r["speedup"] >= 1.0, r
+
+
+@pytest.mark.gpu
+def test_learned_controller_selects_sparse_gears_when_admissible(cuda):
+    """A compressible layer (4x4 block scales log-normal, so the smallest
+    quarter of the blocks holds a tiny share of the energy) on the integer
+    pipe, where a sparse gear skips its dropped blocks: the learned controller
+    runs layer 0 at a sparse gear after calibration, every audit passes, and
+    the final SNR meets the target."""
+    import math
+    from ckks_b200.evaluator import Evaluator
+    from ckks_b200.gear_learn import GearNet, LearnedController
+    from ckks_b200.mlp import EncryptedMLP, Layer, apply_keep, make_block_sparse
+    from ckks_b200.models import run_stream
+    from ckks_b200.params import CkksParams
+    rng = np.random.default_rng(21)
+    W = rng.standard_normal((128, 784)) / math.sqrt(784)
+    scales = np.exp(rng.normal(0.0, 2.0, (32, 196)))
+    W = apply_keep(W, np.ones((32, 196), dtype=np.uint8)) * np.repeat(np.repeat(scales, 4, 0), 4, 1)
+    W = make_block_sparse(W / np.sqrt((W ** 2).sum(1, keepdims=True)), 0.5, 5)
+    W2 = make_block_sparse(rng.standard_normal((10, 128)) / math.sqrt(128), 0.5, 6)
+    layers = [Layer(W, rng.standard_normal(128) * 0.1, "square"), Layer(W2, rng.standard_normal(10) * 0.1, "none")]
+    ev = Evaluator(CkksParams.standard(13, 4, seed=9))
+    ev.keygen()
+    m = EncryptedMLP(ev, layers, tensor_cores=False)
+    data = [rng.uniform(0, 1, (1024, 784)) for _ in range(6)]
+    ctl = LearnedController(m, GearNet.load(NET), 40.0)
+    r = run_stream(m, ctl, data, fallback_db=40.0)
+    layer0 = [g[0] for g in r["gears"]]
+    assert max(layer0[1:]) >= 1, layer0
+    assert r["recomputed_layers"] == 0
+    assert r["snr_db"] >= 40.0
