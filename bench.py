@@ -65,6 +65,9 @@ def parse():
                     help="three kernels through scratch (default) or the fused cluster kernel")
     ap.add_argument("--soak-seconds", type=float, default=1.2,
                     help="identical steps around the timed region, for the clock record")
+    ap.add_argument("--no-batch", action="store_true",
+                    help="skip the batched uneven workload leg (persistent kernel)")
+    ap.add_argument("--batch-items", type=int, default=4096)
     ap.add_argument("--no-decoded", action="store_true",
                     help="skip the decoded-slot error check of the ct-mult (real keys)")
     ap.add_argument("--no-e2e", action="store_true",
@@ -459,6 +462,60 @@ def measure_decoded(dev, log_n: int, levels: int, batch: int) -> dict:
             "params": f"N=2^{log_n}, L={levels}, scale 2^40, ternary secret, DG sigma 3.2, real key"}
 
 
+def measure_batch(dev, n_items: int = 4096, steps: int = 10, warmup: int = 3) -> dict:
+    """The batched uneven workload: `n_items` operations, 60 % ct x ct +
+    relin + rescale and 40 % ct x pt + rescale, N uniform in {2^12, 2^13},
+    level uniform in 2..8 (45-bit primes).  Reference outputs come from the
+    eager per-bucket path (one batched launch sequence per same-shape
+    bucket); the persistent plan (one kernel launch per graph replay) is
+    checked bit-exact against them, its lag and CTAs per SM tuned, then
+    timed as graph replays; the per-bucket graph (default launch shapes) is
+    timed beside it."""
+    import numpy as np
+    import torch
+    from ckks_b200.batch import BatchExecutor, synthetic_workload
+    from ckks_b200 import _lib
+    items = synthetic_workload(n_items, seed=0)
+    ex = BatchExecutor(items, device=dev)
+    ex.run_eager()
+    torch.cuda.synchronize()
+    ref = [b.out.clone() for b in ex.buckets]
+    streams = ex.time_steps(steps, warmup, use_graph=True)
+    ex.mode = "persistent"
+    tune = ex.autotune_persistent()
+    for b in ex.buckets:
+        b.out.zero_()
+    torch.cuda.synchronize()
+    ex.plan.run()
+    torch.cuda.synchronize()
+    exact = all(torch.equal(b.out, r) for b, r in zip(ex.buckets, ref))
+    n_bad, _ = ex.plan.incomplete()
+    persistent = ex.time_steps(steps, warmup, use_graph=True)
+    exact_graph = all(torch.equal(b.out, r) for b, r in zip(ex.buckets, ref))
+    status = _lib.load().ckks_device_status()
+    ctct = sum(b.count for b in ex.buckets if b.shape.op == "ctct")
+    info = ex.plan.info()
+    out = {"metric": "batched uneven operations/s", "unit": "items/s",
+           "value": persistent["items_per_s"], "ms_per_step": persistent["ms_per_step"],
+           "workload": f"{n_items} items ({ctct} ct x ct + relin + rescale, {n_items - ctct} ct x pt + rescale), "
+                       "N uniform in {2^12, 2^13}, level uniform in 2..8, 45-bit primes, seed 0",
+           "buckets": len(ex.buckets), "units_per_step": info["units"], "grid": info["grid"],
+           "lag_percent": info["lag_percent"], "ctas_per_sm": info["ctas_per_sm"],
+           "persistent_sweep_ms": tune["sweep"],
+           "launches_per_step": {"kernels": 1, "memsets": 1},
+           "bit_exact_vs_eager_per_bucket": bool(exact and exact_graph), "incomplete_items": n_bad,
+           "device_status": status,
+           "per_bucket_graph": {"items_per_s": streams["items_per_s"], "ms_per_step": streams["ms_per_step"],
+                                "note": "one batched launch sequence per bucket on 4 streams, one graph, "
+                                        "default launch shapes"},
+           "speedup_vs_per_bucket_graph": persistent["items_per_s"] / streams["items_per_s"],
+           "l2": "inputs larger than L2 (several GB of ciphertexts per step)"}
+    ex.plan.close()
+    del ex
+    torch.cuda.empty_cache()
+    return out
+
+
 def _lib_call_poly_mul(ctx, out, a, b, nl):
     import torch
     from ckks_b200 import _lib
@@ -725,6 +782,7 @@ def run_ours(a) -> int:
             enc_cnn = gear_leg("cnn", max(4, a.enc_mlp_batches // 2),
                                "conv 5x5x8 s2 + x^2 + 2x2 avg-pool + FC 288->10, N=2^13, L=5")
         decoded = measure_decoded(dev, a.log_n, a.levels, a.batch) if not a.no_decoded else None
+        batch = measure_batch(dev, a.batch_items) if not a.no_batch and ws == 1 else None
         cpu = None
         if ws == 1 and not a.no_cpu_baseline:
             from oracle import cpu_baseline
@@ -782,6 +840,7 @@ def run_ours(a) -> int:
             "soak": {"value": soak_value, "unit": UNIT, "steps": soak_steps,
                      "note": "identical steps around the timed region (clock record window)"},
             "decoded": decoded,
+            "batch": batch,
             "gpu_launches": int(round(launches_per_step * a.steps)),
             "gpu_launches_basis": f"{launches_per_step:g} library kernel launches per step, counted by the "
                                   "library's profiler over the profiled pass",

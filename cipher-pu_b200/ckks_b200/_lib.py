@@ -19,6 +19,17 @@ _i64 = C.c_int64
 _u64 = C.c_uint64
 _sz = C.c_size_t
 
+
+
+class BatchBucket(C.Structure):
+    """ckks_batch_bucket: n_ct same-shape operations of the persistent batch."""
+    _fields_ = [("ctx", _vp), ("op", C.c_int32), ("n_ct", C.c_int32), ("level", C.c_int32),
+                ("pt_per_ct", C.c_int32), ("a", _vp), ("b", _vp), ("out", _vp), ("key", _vp)]
+
+
+BATCH_CT_CT, BATCH_CT_PT = 0, 1
+BATCH_RUN_UNMET_WAIT = 1
+
 # name -> (restype, argtypes); must mirror include/ckks_b200.h
 SIGNATURES: dict[str, tuple] = {
     "ckks_abi_version": (_i32, []),
@@ -94,6 +105,13 @@ SIGNATURES: dict[str, tuple] = {
     "ckks_gear_ctrl_init": (_i32, [_vp, C.POINTER(_u64), C.POINTER(_u64), _i32]),
     "ckks_gear_ctrl_raw": (_i32, [_vp, _u64, _u64]),
     "ckks_gear_ctrl_flush": (_i32, [_vp, _u64, _u64, _i32, _i32, _i32]),
+    "ckks_batch_plan_create": (_i32, [C.POINTER(BatchBucket), _i32, _i32, _i32, C.POINTER(_vp)]),
+    "ckks_batch_plan_run": (_i32, [_vp, C.c_longlong, _i32, _vp]),
+    "ckks_batch_plan_incomplete": (_i32, [_vp, C.POINTER(_i32), _vp]),
+    "ckks_batch_plan_info": (_i32, [_vp, C.POINTER(C.c_longlong), C.POINTER(_i32), C.POINTER(_i32),
+                                     C.POINTER(_sz)]),
+    "ckks_batch_plan_destroy": (None, [_vp]),
+    "ckks_batch_schedule": (_i32, [_i32, _vp, _vp, _vp, _vp, C.c_longlong, _vp, C.POINTER(C.c_longlong)]),
     "ckks_profile_enable": (_i32, [_i32]),
     "ckks_profile_reset": (_i32, []),
     "ckks_profile_read": (_i32, [_i32, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),

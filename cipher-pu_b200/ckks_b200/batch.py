@@ -2,14 +2,25 @@
 dimension (N = 2^12, 2^13), level (2..8 limbs) and kind (ct x ct + relin +
 rescale, ct x pt + rescale) in one CUDA-graph replay per step.
 
-Items are grouped into same-shape buckets (kind, log N, level); each bucket
-is one batched launch sequence of the library's kernels (one CTA per
-polynomial limb, so the buckets of different shapes need no padding).  The
-buckets are spread over a pool of streams and the whole plan is captured
-once into a CUDA graph, so a step costs one graph launch.  The autotuner
-times every bucket alone under each launch shape (per-thread radix 2^K, K = 2..5,
-balanced or tight register budget, limbs / work units per CTA, the
-persistent TMA-fed tensor kernel, chunking of the bucket into launches) and keeps the fastest; the choice is baked into the
+Items are grouped into same-shape buckets (kind, log N, level).  Two
+executions of the same buckets, bit-identical to each other:
+
+* ``persistent`` (PersistentPlan, ckks_batch_plan_*): ONE launch of the
+  persistent batch kernel drains a device work list of every bucket's work
+  units (a ct x ct pair's tensor limbs, ModUp target primes and ModDown
+  polynomials, a ct x pt item's two polynomials) with per-item dependency
+  counters and bounded waits; a graph replay is one memset node and one
+  kernel node.
+* ``streams``: each bucket is one batched launch sequence of the library's
+  kernels (one CTA per polynomial limb, so buckets of different shapes need
+  no padding), spread over a pool of streams and captured into one graph.
+
+The autotuner times every bucket alone under each launch shape (per-thread
+radix 2^K, K = 2..5, balanced or tight register budget, limbs / work units
+per CTA, the persistent TMA-fed tensor kernel, chunking of the bucket into
+launches) and keeps the fastest, then times the persistent plan under each
+lag (how far a dependent stage is listed after its producers) and CTAs per
+SM, and keeps whichever execution is faster; the choice is baked into the
 graph at capture time.
 
 The reference's batching is time multiplexing of four poly-mult instances on
@@ -18,6 +29,7 @@ scripts/exp_e17_energy_efficiency.py:32).
 """
 from __future__ import annotations
 
+import ctypes
 import itertools
 import time
 from dataclasses import dataclass, field
@@ -79,8 +91,59 @@ def cm_shape_built(log_n: int, k: int, minb: int) -> bool:
     return k in (3, 4)
 
 
+class PersistentPlan:
+    """ckks_batch_plan over a list of Buckets: created once (validates, sizes
+    and allocates its device memory, lists the work units), then run any
+    number of times; ``run`` is capturable into a CUDA graph."""
+
+    def __init__(self, evs: dict, buckets: list, lag_percent: int = 200, ctas_per_sm: int = 1):
+        arr = (_lib.BatchBucket * max(1, len(buckets)))()
+        for i, bk in enumerate(buckets):
+            ev = evs[bk.shape.log_n]
+            ctct = bk.shape.op == "ctct"
+            arr[i] = _lib.BatchBucket(ev.ctx.handle, _lib.BATCH_CT_CT if ctct else _lib.BATCH_CT_PT, bk.count,
+                                      bk.shape.level, 0 if ctct else 1, bk.a.data_ptr(), bk.b.data_ptr(),
+                                      bk.out.data_ptr(), ev.rlk.data_ptr() if ctct else None)
+        h = ctypes.c_void_p()
+        _lib.call("ckks_batch_plan_create", arr, len(buckets), int(lag_percent), int(ctas_per_sm), ctypes.byref(h))
+        self.handle = h
+        self.buckets = buckets
+        self.lag_percent = lag_percent
+        self.ctas_per_sm = ctas_per_sm
+
+    def run(self, wait_cycles: int = 0, flags: int = 0, stream=None):
+        st = (stream or torch.cuda.current_stream()).cuda_stream
+        _lib.call("ckks_batch_plan_run", self.handle, int(wait_cycles), int(flags), st)
+
+    def incomplete(self) -> tuple[int, list]:
+        """(items of the last run whose output is incomplete, per-bucket complete flags)."""
+        n = ctypes.c_int()
+        flags = (ctypes.c_uint8 * max(1, len(self.buckets)))()
+        _lib.call("ckks_batch_plan_incomplete", self.handle, ctypes.byref(n), flags)
+        return n.value, [bool(flags[i]) for i in range(len(self.buckets))]
+
+    def info(self) -> dict:
+        nu, grid, smem, nb = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
+        _lib.call("ckks_batch_plan_info", self.handle, ctypes.byref(nu), ctypes.byref(grid), ctypes.byref(smem),
+                  ctypes.byref(nb))
+        return {"units": nu.value, "grid": grid.value, "smem_bytes": smem.value, "device_bytes": nb.value,
+                "lag_percent": self.lag_percent, "ctas_per_sm": self.ctas_per_sm}
+
+    def close(self):
+        if self.handle:
+            _lib.raw("ckks_batch_plan_destroy")(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class BatchExecutor:
-    def __init__(self, items: list, max_level: int = 8, seed: int = 0, n_streams: int = 4, device=None):
+    def __init__(self, items: list, max_level: int = 8, seed: int = 0, n_streams: int = 4, device=None,
+                 mode: str = "streams"):
         self.device = device or torch.device("cuda", torch.cuda.current_device())
         counts = {}
         for it in items:
@@ -106,6 +169,28 @@ class BatchExecutor:
             self.buckets.append(bk)
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(n_streams)]
         self.graph = None
+        self.plan = None
+        self.mode = mode
+
+    @property
+    def mode(self) -> str:
+        return self._mode
+
+    @mode.setter
+    def mode(self, m: str):
+        if m not in ("streams", "persistent"):
+            raise ValueError(f"mode={m!r}: 'streams' or 'persistent'")
+        self._mode = m
+        self.graph = None               # a captured step belongs to one mode
+
+    def persistent_plan(self, lag_percent: int = 200, ctas_per_sm: int = 1) -> PersistentPlan:
+        if self.plan is not None and (self.plan.lag_percent, self.plan.ctas_per_sm) == (lag_percent, ctas_per_sm):
+            return self.plan
+        if self.plan is not None:
+            self.plan.close()
+        self.plan = PersistentPlan(self.evs, self.buckets, lag_percent, ctas_per_sm)
+        self.graph = None
+        return self.plan
 
     # ---------------------------------------------------------------- launches
     def launch(self, bk: Bucket):
@@ -140,6 +225,13 @@ class BatchExecutor:
                           bk.b[s:e].data_ptr(), 1, e - s, lvl, st)
             _lib.call("ckks_ctx_set_tuning", ctx.handle, 3, 0)
 
+    def run(self):
+        """One step in the selected mode, without a graph."""
+        if self.mode == "persistent":
+            (self.plan or self.persistent_plan()).run()
+        else:
+            self.run_eager()
+
     def run_eager(self):
         cur = torch.cuda.current_stream()
         fork = torch.cuda.Event()
@@ -156,11 +248,11 @@ class BatchExecutor:
             cur.wait_event(j)
 
     def capture(self):
-        self.run_eager()                      # kernel attributes, lazy module loading
+        self.run()                            # kernel attributes, lazy module loading
         torch.cuda.synchronize()
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
-            self.run_eager()
+            self.run()
         self.graph = g
         return g
 
@@ -170,7 +262,7 @@ class BatchExecutor:
         self.graph.replay()
 
     def time_steps(self, steps: int = 10, warmup: int = 3, use_graph: bool = True) -> dict:
-        fn = self.step if use_graph else self.run_eager
+        fn = self.step if use_graph else self.run
         for _ in range(warmup):
             fn()
         torch.cuda.synchronize()
@@ -182,7 +274,8 @@ class BatchExecutor:
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / steps
-        return {"ms_per_step": ms, "items_per_s": self.n_items / (ms / 1000.0), "graph": use_graph}
+        return {"ms_per_step": ms, "items_per_s": self.n_items / (ms / 1000.0), "graph": use_graph,
+                "mode": self.mode}
 
     # ---------------------------------------------------------------- autotuner
     def autotune(self, reps: int = 3) -> dict:
@@ -233,6 +326,40 @@ class BatchExecutor:
         self.graph = None
         return choices
 
+    def autotune_persistent(self, reps: int = 3, lags=(100, 200, 400), ctas=(1, 2)) -> dict:
+        """Time the persistent plan under each lag and CTAs-per-SM choice
+        (2 only where every bucket is N = 2^12); keep the fastest plan."""
+        sweep = {}
+        best = None
+        only12 = all(b.shape.log_n == 12 for b in self.buckets)
+        for lag in lags:
+            for c in ctas:
+                if c == 2 and not only12:
+                    continue
+                plan = PersistentPlan(self.evs, self.buckets, lag, c)
+                plan.run()
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(reps):
+                    plan.run()
+                e1.record()
+                torch.cuda.synchronize()
+                t = e0.elapsed_time(e1) / reps
+                sweep[f"lag{lag}/c{c}"] = round(t, 4)
+                if best is None or t < best[0]:
+                    if best is not None:
+                        best[1].close()
+                    best = (t, plan)
+                else:
+                    plan.close()
+        if self.plan is not None:
+            self.plan.close()
+        self.plan = best[1]
+        self.graph = None
+        return {"ms": best[0], **self.plan.info(), "sweep": sweep}
+
 
 def main(argv=None) -> int:
     """Time the batched uneven workload: eager launches, one graph replay per
@@ -248,15 +375,23 @@ def main(argv=None) -> int:
     a = ap.parse_args(argv)
     items = synthetic_workload(a.items, seed=a.seed)
     ex = BatchExecutor(items)
+    ex.mode = "persistent"
+    ex.persistent_plan()
+    persistent = ex.time_steps(a.steps, a.warmup, use_graph=True)
+    ex.mode = "streams"
     res = {"workload": f"{a.items} items, 60% ct x ct + relin + rescale / 40% ct x pt + rescale, "
                        "N in {2^12, 2^13}, level uniform in 2..8",
            "buckets": len(ex.buckets),
            "ctct_items": sum(b.count for b in ex.buckets if b.shape.op == "ctct"),
            "eager": ex.time_steps(a.steps, a.warmup, use_graph=False),
-           "graph_default": ex.time_steps(a.steps, a.warmup, use_graph=True)}
+           "graph_default": ex.time_steps(a.steps, a.warmup, use_graph=True),
+           "persistent_default": {**persistent, **ex.plan.info()}}
     if not a.no_autotune:
         res["autotune"] = ex.autotune()
         res["graph_tuned"] = ex.time_steps(a.steps, a.warmup, use_graph=True)
+        res["autotune_persistent"] = ex.autotune_persistent()
+        ex.mode = "persistent"
+        res["persistent_tuned"] = ex.time_steps(a.steps, a.warmup, use_graph=True)
     print(json.dumps(res, indent=1))
     return 0
 

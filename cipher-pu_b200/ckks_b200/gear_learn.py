@@ -168,8 +168,17 @@ def _default_init(seed: int) -> np.ndarray:
 
 
 # ------------------------------------------------------------------ traces
-def random_layer(rng, F: int, O: int, act: str, base_sparsity: float) -> Layer:
+def random_layer(rng, F: int, O: int, act: str, base_sparsity: float, block_spread: float = 0.0) -> Layer:
+    """Dense N(0, 1/F) weights with a random base block sparsity; block_spread
+    > 0 scales each 4x4 block by exp(N(0, block_spread)) (rows renormalised):
+    a compressible layer, whose smallest blocks hold a small share of the
+    energy."""
     W = rng.standard_normal((O, F)) / math.sqrt(F)
+    if block_spread > 0:
+        nb = (-(-O // 4), -(-F // 4))
+        s = np.exp(rng.normal(0.0, block_spread, nb))
+        W = W * np.repeat(np.repeat(s, 4, 0), 4, 1)[:O, :F]
+        W = W / np.sqrt((W ** 2).sum(1, keepdims=True) + 1e-300)   # unit rows, as N(0, 1/F) rows
     W = make_block_sparse(W, base_sparsity, int(rng.integers(1 << 30)))
     b = rng.standard_normal(O) * 0.1
     return Layer(W, b, act)
@@ -197,7 +206,9 @@ def random_conv_layer(rng, act: str) -> Layer:
 def gen_traces(ev, n_traces: int, seed: int = 0, batch: int = 256, progress=None) -> tuple:
     """Run random encrypted layers at all four gears; one trace per neuron.
     Three in ten are convolution-structured (random_conv_layer), the rest
-    dense block-sparse layers of the MLP family."""
+    dense block-sparse layers of the MLP family, about a third of those
+    compressible (random_layer's block_spread), so the traces cover sparse
+    gears that lose almost nothing as well as ones that lose most."""
     rng = np.random.default_rng(seed)
     Xs, Ts = [], []
     total = 0
@@ -208,7 +219,8 @@ def gen_traces(ev, n_traces: int, seed: int = 0, batch: int = 256, progress=None
         else:
             F = int(rng.choice([128, 256, 512, 784]))
             O = int(rng.choice([16, 32, 64, 128]))
-            L = random_layer(rng, F, O, act, float(rng.choice([0.25, 0.5, 0.75])))
+            spread = float(rng.uniform(0.5, 3.0)) if rng.random() < 0.35 else 0.0
+            L = random_layer(rng, F, O, act, float(rng.choice([0.25, 0.5, 0.75])), spread)
         O, F = L.W.shape
         m = EncryptedMLP(ev, [L])
         lo, hi = sorted(rng.uniform(0.0, 1.5, 2))

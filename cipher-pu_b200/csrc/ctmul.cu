@@ -34,6 +34,7 @@
 #include <mutex>
 
 #include "ctmul.hpp"
+#include "ctmul_units.cuh"
 #include "dispatch.cuh"
 #include "profile.hpp"
 
@@ -76,13 +77,6 @@ int split_streams_for_device(SplitStreams** out, const char* fn) {
 }
 }  // namespace
 
-struct CmScratch {
-  u64* d01;   // [n_ct][2][level][N]  tensor d0, d1 (evaluation)
-  u64* d2n;   // [n_ct][level][N]     tensor d2 (evaluation)
-  u64* d2c;   // [n_ct][level][N]     d2 digits (coefficient)
-  u64* acc;   // [n_ct][2][level][N]  key inner product over q_i (evaluation)
-  u64* accp;  // [n_ct][2][N]         key inner product over p (evaluation)
-};
 
 static size_t cm_words(int n, int n_ct, int level) {
   return (size_t)n_ct * n * (size_t)(6 * level + 2);
@@ -181,58 +175,19 @@ static int dispatch_cm(int log_n, int kreq, int mreq, F&& f, const char* fn) {
 }
 
 // ---------------------------------------------------------------- kernel A
-// One CTA per (ct, limb j).  All global traffic is lane-contiguous (layout C);
-// d2 is re-distributed to layout Z through shared memory for its INTT.
+// One CTA per (ct, limb j) (body: cm_tensor_unit, ctmul_units.cuh).
 template <int LOGN, int K, int MINB>
 __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
     k_cm_tensor(const u64* __restrict__ A, const u64* __restrict__ B, CmScratch S, int level,
                 const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct,
                 long long n_units, int upc) {
   extern __shared__ u64 sm[];
-  using Sh = NttShape<LOGN, K>;
-  constexpr int N = Sh::N;
   // `upc` work units per CTA, consecutive in the unit order
   for (int r = 0; r < upc; ++r) {
     const long long unit = (long long)blockIdx.x * upc + r;
     if (unit >= n_units) return;  // uniform across the CTA
     if (r) __syncthreads();       // the previous unit is done with shared memory
-    const int j = unit / n_ct;  // limb-major: resident CTAs share q_j's tables
-    const long long ct = unit % n_ct;
-    const int tid = threadIdx.x;
-    const PrimeInfo P = pi[j];
-    const size_t LN = (size_t)level * N;
-    const u64* a0 = A + ct * 2 * LN + (size_t)j * N;
-    const u64* b0 = B + ct * 2 * LN + (size_t)j * N;
-    u64* d0 = S.d01 + ct * 2 * LN + (size_t)j * N;
-    // Products in FP64 (exact two-product + rounded quotient, fmulmod_var):
-    // d2 = a1 b1, d0 = a0 b0, d1 = (a0 + a1)(b0 + b1) - d0 - d2, each partial
-    // result below 2^48 in magnitude, reduced to [0, q) once at the end.
-    u64 x[Sh::E], y[Sh::E];
-    load_c<LOGN, K>(x, a0 + LN, tid);
-    load_c<LOGN, K>(y, b0 + LN, tid);
-    double m2d[Sh::E];
-  #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) m2d[e] = fmulmod_var(u2d(x[e]), u2d(y[e]), P.qd, P.qinv_d);
-    u64 a0v[Sh::E], b0v[Sh::E];
-    load_c<LOGN, K>(a0v, a0, tid);
-    load_c<LOGN, K>(b0v, b0, tid);
-  #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) {
-      const double a0d = u2d(a0v[e]), b0d = u2d(b0v[e]);
-      const double m0 = fmulmod_var(a0d, b0d, P.qd, P.qinv_d);
-      const double s1 = fmulmod_var(__dadd_rn(a0d, u2d(x[e])), __dadd_rn(b0d, u2d(y[e])), P.qd, P.qinv_d);
-      a0v[e] = d2canon(m0, P.qd, P.qinv_d);
-      b0v[e] = d2canon(__dadd_rn(__dadd_rn(s1, -m0), -m2d[e]), P.qd, P.qinv_d);  // |.| < 3 2^48
-    }
-    store_c<LOGN, K>(a0v, d0, tid);
-    store_c<LOGN, K>(b0v, d0 + LN, tid);
-    u64 m2[Sh::E];
-  #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) m2[e] = d2canon(m2d[e], P.qd, P.qinv_d);
-    store_c<LOGN, K>(m2, S.d2n + ct * LN + (size_t)j * N, tid);
-    c_to_z<LOGN, K>(m2d, sm, tid);  // |m2d| < 0.6 q: straight into the FP64 inverse
-    ntt_inv_d<LOGN, K>(m2d, m2, sm, tid, twbase<LOGN>(tw, j), P);
-    store_c<LOGN, K>(m2, S.d2c + ct * LN + (size_t)j * N, tid);
+    cm_tensor_unit<LOGN, K>(A, B, S, level, pi, tw, n_ct, unit, sm, threadIdx.x);
   }
 }
 
@@ -415,9 +370,10 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 
 // expiries of the tensor-core linear layer's waits (linear_tc.cu), read and cleared
 int ckks_linear_tc_status_take(unsigned int* n);
+int ckks_batch_status_take(unsigned int* n);
 
 extern "C" int ckks_device_status(void) {
-  unsigned int n = 0, n_tc = 0;
+  unsigned int n = 0, n_tc = 0, n_pb = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&n, g_cm_wait_expiries, sizeof(n));
   if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "ckks_device_status: %s", cudaGetErrorString(e));
   if (n) {
@@ -426,8 +382,9 @@ extern "C" int ckks_device_status(void) {
     if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "ckks_device_status: %s", cudaGetErrorString(e));
   }
   if (int rc = ckks_linear_tc_status_take(&n_tc)) return rc;
-  if (n + n_tc == 0) return CKKS_OK;
-  return ckks_set_error(CKKS_ETIMEOUT, "ckks_device_status: %u bounded device waits expired", n + n_tc);
+  if (int rc = ckks_batch_status_take(&n_pb)) return rc;
+  if (n + n_tc + n_pb == 0) return CKKS_OK;
+  return ckks_set_error(CKKS_ETIMEOUT, "ckks_device_status: %u bounded device waits expired", n + n_tc + n_pb);
 }
 
 // ---------------------------------------------------------------- kernel B
@@ -441,85 +398,12 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
                const PrimeInfo* __restrict__ pi, const TwD* __restrict__ tw, int n_ct,
                 long long n_units, int upc) {
   extern __shared__ u64 sm[];
-  using Sh = NttShape<LOGN, K>;
-  constexpr int N = Sh::N;
-  constexpr int T = Sh::T;
-  u64* acc0s = sm + Sh::SMEM_WORDS;
-  u64* acc1s = acc0s + N;
-  // target-major (resident CTAs share one prime), special prime first: its
-  // CTAs transform every digit, one more than the others, so they go first
-  // and the shorter ones fill the last wave
-  // `upc` work units per CTA, consecutive in the unit order
+  // `upc` work units per CTA, consecutive in the unit order (body: cm_modup_unit)
   for (int r = 0; r < upc; ++r) {
     const long long unit = (long long)blockIdx.x * upc + r;
     if (unit >= n_units) return;  // uniform across the CTA
     if (r) __syncthreads();       // the previous unit is done with shared memory
-    const int ti = level - (int)(unit / n_ct);
-    const long long ct = unit % n_ct;
-    const bool special = ti == level;
-    const int pidx = special ? nq : ti;
-    const int tid = threadIdx.x;
-    const PrimeInfo P = pi[pidx];
-    const size_t LN = (size_t)level * N;
-    const TwD* tb = twbase<LOGN>(tw, pidx);
-    double* acc0s_d = reinterpret_cast<double*>(acc0s);
-    double* acc1s_d = reinterpret_cast<double*>(acc1s);
-  #pragma unroll 1
-    for (int j = 0; j < level; ++j) {
-      // digit j as exact doubles in layout C: its evaluation-domain residues at
-      // its own prime, else its coefficient residues (< q_j < 2 q_i) transformed
-      // unreduced (|x| < 2^51 on return, fine for fmulmod)
-      double x[Sh::E];
-      u64 xu[Sh::E];
-      if (!special && j == ti) {
-        load_c<LOGN, K>(xu, S.d2n + ct * LN + (size_t)j * N, tid);
-  #pragma unroll
-        for (int e = 0; e < Sh::E; ++e) x[e] = u2d(xu[e]);
-      } else {
-        load_c<LOGN, K>(xu, S.d2c + ct * LN + (size_t)j * N, tid);
-  #pragma unroll
-        for (int e = 0; e < Sh::E; ++e) x[e] = u2d(xu[e]);
-        ntt_fwd_d<LOGN, K>(x, sm, tid, tb, P);
-        z_to_c<LOGN, K>(x, sm, tid);
-      }
-      // key inner product in exact FP64 on the key values alone (8 bytes per
-      // word): w / q is formed as w * (1/q), two roundings off, so the quotient
-      // estimate may miss by one and each product lands within 1.5 q (still
-      // exact: every intermediate is an integer below 2^53); the running sum is
-      // folded back below q / 2 + 1 every 16 digits so it stays exact
-  #pragma unroll 1
-      for (int kk = 0; kk < 2; ++kk) {
-        const double* kp = reinterpret_cast<const double*>(key) + (((size_t)j * 2 + kk) * (nq + 1) + pidx) * (2 * N);
-        double* acc = kk ? acc1s_d : acc0s_d;
-        const bool fold = (j & 15) == 15;
-  #pragma unroll
-        for (int e = 0; e < Sh::E; ++e) {
-          const double w = ld_stream_d(kp + posC<LOGN, K>(tid, e));
-          const int s = e * T + tid;
-          const double t = fmulmod(x[e], w, __dmul_rn(w, P.qinv_d), P.qd);
-          double a = j == 0 ? t : __dadd_rn(acc[s], t);
-          if (fold) {
-            const double qt = __dadd_rn(__fma_rn(a, P.qinv_d, CKKS_FP_MAGIC), -CKKS_FP_MAGIC);
-            a = __fma_rn(-qt, P.qd, a);
-          }
-          acc[s] = a;
-        }
-      }
-    }
-    // Special-prime accumulators stay in the evaluation domain here; kernel C
-    // (one CTA per output polynomial) brings each back with one INTT, which
-    // keeps the per-CTA work of this kernel within one transform of each other.
-    u64 x[Sh::E];
-    u64* o = special ? S.accp + ct * 2 * N : S.acc + ct * 2 * LN + (size_t)ti * N;
-    const size_t kstride = special ? (size_t)N : LN;
-  #pragma unroll 1
-    for (int k = 0; k < 2; ++k) {
-      const u64* a = k ? acc1s : acc0s;
-  #pragma unroll
-      for (int e = 0; e < Sh::E; ++e)
-        x[e] = d2canon(reinterpret_cast<const double*>(a)[e * T + tid], P.qd, P.qinv_d);
-      store_c<LOGN, K>(x, o + (size_t)k * kstride, tid);
-    }
+    cm_modup_unit<LOGN, K, false>(S, key, level, nq, pi, tw, n_ct, unit, sm, threadIdx.x);
   }
 }
 
@@ -538,80 +422,12 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
               const TwPair* __restrict__ pinv, const TwPair* __restrict__ qtinv, long long n_units,
               int upc) {
   extern __shared__ u64 sm[];
-  using Sh = NttShape<LOGN, K>;
-  constexpr int N = Sh::N;
-  constexpr int T = Sh::T;
-  double* vs = reinterpret_cast<double*>(sm + Sh::SMEM_WORDS);
-  double* ws = vs + N;
-  // `upc` work units per CTA, consecutive in the unit order
+  // `upc` work units per CTA, consecutive in the unit order (body: cm_down_unit)
   for (int r = 0; r < (MULTI ? upc : 1); ++r) {
     const long long unit = (long long)blockIdx.x * upc + r;
     if (MULTI && unit >= n_units) return;  // uniform across the CTA
     if (r) __syncthreads();       // the previous unit is done with shared memory
-    const long long ct = unit >> 1;
-    const int k = unit & 1;
-    const int t = level - 1;
-    const int tid = threadIdx.x;
-    const size_t LN = (size_t)level * N;
-    const PrimeInfo PP = pi[nq];
-    const PrimeInfo PT = pi[t];
-    const u64* dk = S.d01 + ct * 2 * LN + (size_t)k * LN;
-    const u64* ak = S.acc + ct * 2 * LN + (size_t)k * LN;
-    u64* ok = out + ((size_t)ct * 2 + k) * (size_t)t * N;
-
-    double d[Sh::E];
-    u64 x[Sh::E];
-    load_c<LOGN, K>(x, S.accp + (ct * 2 + k) * N, tid);
-  #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) d[e] = u2d(x[e]);
-    c_to_z<LOGN, K>(d, sm, tid);
-    ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, nq), PP);
-  #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) vs[e * T + tid] = x[e] > PP.half ? u2d(x[e]) - PP.qd : u2d(x[e]);
-    // Rescale limb t in the coefficient domain without a transform of v:
-    // w = INTT_t(d_t + acc_t p^-1) - v p^-1, equal mod q_t to
-    // INTT_t(d_t + (acc_t - NTT_t([v]_t)) p^-1) by linearity of the NTT.
-    const double ptw = (double)pinv[t].w;
-    const double ptq = __ddiv_rn(ptw, PT.qd);
-    {
-      u64 dv[Sh::E];
-      load_c<LOGN, K>(dv, dk + (size_t)t * N, tid);
-      load_c<LOGN, K>(x, ak + (size_t)t * N, tid);
-  #pragma unroll
-      for (int e = 0; e < Sh::E; ++e) {
-        const double dc = dv[e] > PT.half ? u2d(dv[e]) - PT.qd : u2d(dv[e]);
-        d[e] = __dadd_rn(fmulmod(u2d(x[e]), ptw, ptq, PT.qd), dc);
-      }
-    }
-    c_to_z<LOGN, K>(d, sm, tid);
-    ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, t), PT);
-  #pragma unroll
-    for (int e = 0; e < Sh::E; ++e) {
-      const u64 w = d2canon(__dadd_rn(u2d(x[e]), -fmulmod(vs[e * T + tid], ptw, ptq, PT.qd)), PT.qd, PT.qinv_d);
-      ws[e * T + tid] = w > PT.half ? u2d(w) - PT.qd : u2d(w);
-    }
-  #pragma unroll 1
-    for (int i = 0; i < t; ++i) {
-      const PrimeInfo P = pi[i];
-      const double pvw = (double)pinv[i].w;
-      const double pvq = __ddiv_rn(pvw, P.qd);
-      const double ciw = (double)qtinv[(size_t)t * nq + i].w;
-      const double ciq = __ddiv_rn(ciw, P.qd);
-  #pragma unroll
-      for (int e = 0; e < Sh::E; ++e)
-        d[e] = __dadd_rn(fmulmod(vs[e * T + tid], pvw, pvq, P.qd), ws[e * T + tid]);  // |.| < 2 q_i
-      ntt_fwd_d<LOGN, K>(d, sm, tid, twbase<LOGN>(tw, i), P);
-      z_to_c<LOGN, K>(d, sm, tid);
-      u64 dv[Sh::E], av[Sh::E];
-      load_c<LOGN, K>(dv, dk + (size_t)i * N, tid);
-      load_c<LOGN, K>(av, ak + (size_t)i * N, tid);
-  #pragma unroll
-      for (int e = 0; e < Sh::E; ++e) {
-        const double sd = __dadd_rn(__dadd_rn(u2d(dv[e]), fmulmod(u2d(av[e]), pvw, pvq, P.qd)), -d[e]);
-        x[e] = d2canon(fmulmod(sd, ciw, ciq, P.qd), P.qd, P.qinv_d);
-      }
-      store_c<LOGN, K>(x, ok + (size_t)i * N, tid);
-    }
+    cm_down_unit<LOGN, K, false>(S, out, level, nq, pi, tw, pinv, qtinv, unit, sm, threadIdx.x);
   }
 }
 

@@ -1,10 +1,9 @@
 // ctpt.cu - ciphertext x plaintext multiply fused with the RNS rescale.
 //
-// One CTA per (ct, poly k): x_i = a_k,i * p_i per limb (evaluation domain);
-// the last limb is brought to the coefficient domain (INTT), centred, and for
-// every remaining limb out_i = (x_i - NTT_i([w]_{q_i})) * q_t^-1.  The
+// One CTA per (ct, poly k) (body: ctpt_unit, ctmul_units.cuh).  The
 // plaintext may be shared by all ciphertexts (pt_stride = 0) or given per
 // ciphertext (pt_stride = 1).
+#include "ctmul_units.cuh"
 #include "dispatch.cuh"
 #include "profile.hpp"
 
@@ -23,49 +22,8 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, (CtptBlocks<LOGN, K>::va
                    int pt_stride, int level, const PrimeInfo* __restrict__ pi,
                    const TwD* __restrict__ tw, const TwPair* __restrict__ qtinv, int nq) {
   extern __shared__ u64 sm[];
-  using Sh = NttShape<LOGN, K>;
-  constexpr int N = Sh::N;
-  constexpr int T = Sh::T;
-  double* ws = reinterpret_cast<double*>(sm + Sh::SMEM_WORDS);
-  const long long c = blockIdx.x >> 1;
-  const int k = blockIdx.x & 1;
-  const int t = level - 1;
-  const int tid = threadIdx.x;
-  const size_t LN = (size_t)level * N;
-  const u64* a = ct + (c * 2 + k) * LN;
-  const u64* p = pt + (size_t)c * pt_stride * LN;
-  u64* o = out + (c * 2 + k) * (size_t)t * N;
-  const PrimeInfo PT = pi[t];
-  // FP64 throughout: products by fmulmod_var (|.| < 0.6 q), the rescale limb
-  // w kept centred and signed (|w| <= q_t / 2 < q_i), q_t^-1 by fmulmod.
-  double d[Sh::E];
-  u64 x[Sh::E], y[Sh::E];
-  load_c<LOGN, K>(x, a + (size_t)t * N, tid);
-  load_c<LOGN, K>(y, p + (size_t)t * N, tid);
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) d[e] = fmulmod_var(u2d(x[e]), u2d(y[e]), PT.qd, PT.qinv_d);
-  c_to_z<LOGN, K>(d, sm, tid);
-  ntt_inv_d<LOGN, K>(d, x, sm, tid, twbase<LOGN>(tw, t), PT);
-#pragma unroll
-  for (int e = 0; e < Sh::E; ++e) ws[e * T + tid] = x[e] > PT.half ? u2d(x[e]) - PT.qd : u2d(x[e]);
-#pragma unroll 1
-  for (int i = 0; i < t; ++i) {
-    const PrimeInfo P = pi[i];
-    const double ciw = (double)qtinv[(size_t)t * nq + i].w;
-    const double ciq = __ddiv_rn(ciw, P.qd);
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e) d[e] = ws[e * T + tid];
-    ntt_fwd_d<LOGN, K>(d, sm, tid, twbase<LOGN>(tw, i), P);  // |d| < 13.75 q
-    z_to_c<LOGN, K>(d, sm, tid);
-    load_c<LOGN, K>(x, a + (size_t)i * N, tid);
-    load_c<LOGN, K>(y, p + (size_t)i * N, tid);
-#pragma unroll
-    for (int e = 0; e < Sh::E; ++e) {
-      const double sd = __dadd_rn(fmulmod_var(u2d(x[e]), u2d(y[e]), P.qd, P.qinv_d), -d[e]);
-      x[e] = d2canon(fmulmod(sd, ciw, ciq, P.qd), P.qd, P.qinv_d);
-    }
-    store_c<LOGN, K>(x, o + (size_t)i * N, tid);
-  }
+  ctpt_unit<LOGN, K>(out, ct, pt, pt_stride, level, pi, tw, qtinv, nq, blockIdx.x >> 1, blockIdx.x & 1, sm,
+                     threadIdx.x);
 }
 
 extern "C" int ckks_ct_mul_plain_rescale(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct,

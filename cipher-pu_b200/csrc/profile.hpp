@@ -11,6 +11,7 @@ enum {
   CKKS_STAGE_NTT = 3,        // standalone batched NTT
   CKKS_STAGE_OTHER = 4,
   CKKS_STAGE_CM_FUSED = 5,   // ct-mult: the one-cluster-per-pair kernel
+  CKKS_STAGE_BATCH = 6,      // the persistent batch kernel
   CKKS_PROFILE_STAGES = 8
 };
 

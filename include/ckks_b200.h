@@ -121,9 +121,10 @@ enum {
 int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value);
 
 /*
- * Device-side status of the kernels that wait on asynchronous copies with a
- * bounded spin (the TMA-fed ct-mult tensor kernel, the tensor-core linear
- * layer's MMA completions): CKKS_ETIMEOUT (and the
+ * Device-side status of the kernels that wait with a bounded spin (the
+ * TMA-fed ct-mult tensor kernel on its copies, the tensor-core linear
+ * layer on its MMA completions, the persistent batch kernel on its work
+ * queue's dependency counters): CKKS_ETIMEOUT (and the
  * count in ckks_last_error) when any such wait on the current device expired
  * since the last call, which leaves those outputs incomplete; CKKS_OK
  * otherwise.  Synchronises the device; clears the count.
@@ -661,12 +662,86 @@ int ckks_ct_mul_relin_rescale_noalloc(const ckks_ctx* ctx, uint64_t* out, const 
                                       int level, void* stream);
 
 /*
+ * Batched uneven workload in ONE persistent launch.  A bucket is n_ct
+ * same-shape operations on one context (N = 2^12 or 2^13): op
+ * CKKS_BATCH_CT_CT = ct_a x ct_b + relinearisation + rescale
+ * (ckks_ct_mul_relin_rescale's operands: a, b ciphertexts [n_ct][2][level][N],
+ * key prepared by ckks_relin_key_prepare, out [n_ct][2][level - 1][N]) or
+ * CKKS_BATCH_CT_PT = ciphertext x plaintext + rescale
+ * (ckks_ct_mul_plain_rescale's: b = plaintexts, one per ciphertext when
+ * pt_per_ct, else one shared).  Results are bit-identical to those entry
+ * points.
+ *
+ * ckks_batch_plan_create validates the buckets, allocates the plan's device
+ * memory once (scratch for every ct x ct pair, the work list, dependency
+ * counters) and lists every work unit (a pair's tensor limbs, ModUp target
+ * primes, ModDown polynomials; a ct x pt item's two polynomials) in a
+ * dependency-respecting order, each dependent stage lag_percent % of one
+ * wave of CTAs after its producers (0..10000; 200 is a good default).
+ * ctas_per_sm: 0 or 1 = one 512-thread CTA per SM (128 registers a thread),
+ * 2 = two (64 registers; for plans of N = 2^12 only).  The buckets' device
+ * pointers are baked into the plan: they must stay valid while it is used.
+ *
+ * ckks_batch_plan_run zeroes the plan's counters (one memset) and launches
+ * the persistent kernel on `stream`: CTAs take units from one atomic ticket;
+ * a unit whose inputs are not finished waits on its item's counter with a
+ * bounded spin of at most wait_cycles SM cycles (<= 0: 2^31 - 1).  On expiry
+ * the kernel records it for ckks_device_status (CKKS_ETIMEOUT), stops every
+ * CTA, and leaves the unfinished items incomplete.  Both calls of a run may
+ * be captured into a CUDA graph (one memset node, one kernel node).  flags:
+ * 0, or CKKS_BATCH_RUN_UNMET_WAIT (a test hook: the ModUp units of the first
+ * ct x ct item wait for one tensor unit more than exist, so that wait ends
+ * only by its limit).
+ *
+ * ckks_batch_plan_incomplete synchronises the device and counts the items
+ * of the last run whose output is not complete (bucket_complete, if not
+ * NULL, gets one 0/1 byte per bucket).
+ *
+ * The reference batches by time-multiplexing four poly-mult instances on one
+ * datapath (rtl/m4/e2e_ckks_mult_ctrl_m4.sv:368-482); it has no equivalent
+ * of the uneven-shape work list.
+ */
+enum { CKKS_BATCH_CT_CT = 0, CKKS_BATCH_CT_PT = 1 };
+enum { CKKS_BATCH_RUN_UNMET_WAIT = 1 };
+typedef struct ckks_batch_bucket {
+  const ckks_ctx* ctx;
+  int32_t op;
+  int32_t n_ct;
+  int32_t level;
+  int32_t pt_per_ct;
+  const uint64_t* a;
+  const uint64_t* b;
+  uint64_t* out;
+  const uint64_t* key;
+} ckks_batch_bucket;
+typedef struct ckks_batch_plan ckks_batch_plan;
+int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_buckets, int lag_percent, int ctas_per_sm,
+                           ckks_batch_plan** plan);
+int ckks_batch_plan_run(ckks_batch_plan* plan, long long wait_cycles, int flags, void* stream);
+int ckks_batch_plan_incomplete(ckks_batch_plan* plan, int* n_incomplete, uint8_t* bucket_complete);
+int ckks_batch_plan_info(const ckks_batch_plan* plan, long long* n_units, int* grid, int* smem_bytes,
+                         size_t* device_bytes);
+void ckks_batch_plan_destroy(ckks_batch_plan* plan);
+/*
+ * The plan's work list computed on the host alone (no device): for buckets
+ * described by op, n_ct, level and a cost that ranks them (costliest first),
+ * with dependent stages `lag` units after their producers, writes two
+ * uint32 per unit, (bucket << 8 | stage << 6 | sub, item): stage 0 tensor
+ * (sub = limb), 1 ModUp (sub = target prime, level = the special prime),
+ * 2 ModDown (sub = output polynomial), 3 ct x pt (sub = output polynomial).
+ * *n_units: capacity in, units written out.
+ */
+int ckks_batch_schedule(int n_buckets, const int* op, const int* n_ct, const int* level, const double* cost,
+                        long long lag, uint32_t* jobs, long long* n_units);
+
+/*
  * Per-kernel device timing (tracing).  When enabled, the multi-kernel entry
  * points record CUDA events around each kernel on the launching stream;
  * ckks_profile_read(stage) resolves them and returns the accumulated device
  * milliseconds and launch count of a stage: 0 = ct-mult tensor, 1 = ct-mult
  * ModUp + key inner product, 2 = ct-mult ModDown + rescale, 3 = ckks_ntt,
- * 4 = other kernels, 5 = the fused ct-mult kernel.
+ * 4 = other kernels, 5 = the fused ct-mult kernel, 6 = the persistent
+ * batch kernel (ckks_batch_plan_run).
  * The reference has no runtime tracing (its timing comes from Vivado reports
  * and the cycle model of scripts/exp_e17_energy_efficiency.py:36-65).
  */

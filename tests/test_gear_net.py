@@ -138,6 +138,16 @@ def test_learned_controller_selects_sparse_gears_when_admissible(cuda):
     ctl = LearnedController(m, GearNet.load(NET), 40.0)
     r = run_stream(m, ctl, data, fallback_db=40.0)
     layer0 = [g[0] for g in r["gears"]]
-    assert max(layer0[1:]) >= 1, layer0
+    # measured layer-0 SNR per gear, for the failure message
+    x = data[0]
+    X = m.encrypt_inputs(x)
+    ref = (x @ layers[0].W.T + layers[0].b) ** 2
+    measured = []
+    for g in range(4):
+        d = np.asarray(m.decrypt(m.square(m.linear(X, 0, g)), len(x)), dtype=np.float64)
+        d = d.reshape(ref.T.shape) if d.size == ref.size else d[:ref.shape[1], :ref.shape[0]]
+        measured.append(float(10 * np.log10((ref ** 2).sum() / ((d - ref.T) ** 2).sum())))
+    predicted = ctl.predicted(0, {"level": X.level, "scale": X.scale}).tolist() if ctl.calibrated(0) else None
+    assert max(layer0[1:]) >= 1, (layer0, "measured", measured, "predicted", predicted)
     assert r["recomputed_layers"] == 0
     assert r["snr_db"] >= 40.0
