@@ -748,7 +748,7 @@ def run_ours(a) -> int:
         transforms = measure_transforms(ctx, dev, hbm) if not a.no_transforms else None
         convgap = (measure_convgap(dev, hbm, with_cpu=not a.no_cpu_baseline)
                    if not a.no_convgap and ws == 1 else None)
-        enc_mlp = enc_cnn = None
+        enc_mlp = enc_cnn = enc_mlp_c = None
         if not a.no_enc_mlp and ws == 1:
             # second half of the metric: encrypted MLP 784-128-10 (N=2^13, L=4,
             # batch 1024, DARE between layers) under the plain SNR-monitor
@@ -757,6 +757,7 @@ def run_ours(a) -> int:
             def gear_leg(model: str, batches: int, workload: str) -> dict:
                 r = compare(model=model, batches=batches)
                 return {"metric": f"enc-{model.upper()} samples/s learned vs plain gear", "unit": "samples/s",
+                        "engine": r["engine"],
                         "plain": r["plain"]["samples_per_s"], "learned": r["learned"]["samples_per_s"],
                         "speedup": r["speedup"], "snr_db_plain": r["plain"]["snr_db"],
                         "snr_db_learned": r["learned"]["snr_db"], "snr_gap_db": r["snr_gap_db"],
@@ -781,6 +782,10 @@ def run_ours(a) -> int:
             enc_mlp = gear_leg("mlp", a.enc_mlp_batches, "784-128-10, N=2^13, L=4")
             enc_cnn = gear_leg("cnn", max(4, a.enc_mlp_batches // 2),
                                "conv 5x5x8 s2 + x^2 + 2x2 avg-pool + FC 288->10, N=2^13, L=5")
+            enc_mlp_c = gear_leg("mlp_compressible", a.enc_mlp_batches,
+                                 "784-128-10 with trained-like compressible hidden weights (4x4 block scales "
+                                 "log-normal, sigma 2), integer pipe (a gear's dropped blocks are skipped), "
+                                 "N=2^13, L=4")
         decoded = measure_decoded(dev, a.log_n, a.levels, a.batch) if not a.no_decoded else None
         batch = measure_batch(dev, a.batch_items) if not a.no_batch and ws == 1 else None
         cpu = None
@@ -810,6 +815,7 @@ def run_ours(a) -> int:
             "convgap": convgap,
             "enc_mlp": enc_mlp,
             "enc_cnn": enc_cnn,
+            "enc_mlp_compressible": enc_mlp_c,
             "stage_ms_per_step": {names[s]: stages[s][0] / max(1, prof_steps) for s in active},
             "stage_timing": (f"library event profiler over {prof_steps} identical steps right after the timed "
                              "region, each kernel launched alone over the whole batch"),

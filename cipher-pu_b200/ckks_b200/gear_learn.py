@@ -251,6 +251,20 @@ def gen_traces(ev, n_traces: int, seed: int = 0, batch: int = 256, progress=None
 
 
 # ------------------------------------------------------------------ controllers
+def neuron_signal_weights(W: np.ndarray, b: np.ndarray, stats: dict, act: str) -> np.ndarray:
+    """Expected output energy of each neuron from the layer input's mean and
+    spread alone: pre-activation y = w.x + b has mean mu = w.1 mean + b and
+    variance v = |w|^2 std^2 (independent inputs); E[y^2] = mu^2 + v, and
+    for the square activation E[y^4] = mu^4 + 6 mu^2 v + 3 v^2 (Gaussian
+    moments).  These weight the per-neuron NSRs into the layer NSR the
+    decrypt-based probe measures (total error energy over total signal)."""
+    mu = W @ np.full(W.shape[1], stats["mean"]) + b
+    v = (W ** 2).sum(1) * stats["std"] ** 2
+    if act == "square":
+        return mu ** 4 + 6 * mu ** 2 * v + 3 * v ** 2 + 1e-300
+    return mu ** 2 + v + 1e-300
+
+
 def layer_snr_from_neurons(snr_db: np.ndarray, sig_weight: np.ndarray | None = None) -> np.ndarray:
     """[O, G] per-neuron SNR -> [G] layer SNR (signal-weighted NSR average)."""
     nsr = 10.0 ** (-np.clip(np.asarray(snr_db), *SNR_CLIP) / 10.0)
@@ -327,8 +341,10 @@ class LearnedController:
         hit = self.pred.get(li)
         if hit is None or hit[0] != key:
             st = self.stats[li]
+            L = self.m.layers[li]
             feats = layer_features(self.m, li, None, st, info["level"], info["scale"])
-            hit = (key, layer_snr_from_neurons(self.net.predict(feats)))
+            w = neuron_signal_weights(L.W, L.b, st, L.act)
+            hit = (key, layer_snr_from_neurons(self.net.predict(feats), w))
             self.pred[li] = hit
         return hit[1]
 

@@ -3,6 +3,10 @@
 * ``mlp_784_128_10``: 784-128-10 MLP, weights N(0, 1/fan_in) with 50 %
   structured 4x4 block sparsity, square activation (the encrypted MLP
   workload: N = 2^13, L = 4, batch 1024).
+* ``mlp_784_128_10_compressible``: the same shape with the weight statistics
+  of a trained network: each 4x4 block of the hidden layer scaled by
+  exp(N(0, spread^2)) (rows renormalised), so the smallest blocks hold a small
+  share of a row's energy and a sparse gear can meet the SNR target.
 * ``cnn_28x28``: conv 5x5x8 stride 2 (28x28x1 -> 12x12x8) as a sparse linear
   map, square activation, 2x2 average pool folded into the 288 -> 10 FC
   (the encrypted CNN workload: N = 2^13, L = 5).
@@ -24,6 +28,17 @@ from .mlp import EncryptedMLP, Layer, make_block_sparse
 def mlp_784_128_10(seed: int = 0, sparsity: float = 0.5) -> list:
     rng = np.random.default_rng(seed)
     W1 = make_block_sparse(rng.standard_normal((128, 784)) / math.sqrt(784), sparsity, seed + 1)
+    W2 = make_block_sparse(rng.standard_normal((10, 128)) / math.sqrt(128), sparsity, seed + 2)
+    return [Layer(W1, rng.standard_normal(128) * 0.1, "square"),
+            Layer(W2, rng.standard_normal(10) * 0.1, "none")]
+
+
+def mlp_784_128_10_compressible(seed: int = 0, sparsity: float = 0.5, spread: float = 2.0) -> list:
+    rng = np.random.default_rng(seed)
+    W1 = rng.standard_normal((128, 784)) / math.sqrt(784)
+    scales = np.exp(rng.normal(0.0, spread, (32, 196)))
+    W1 = W1 * np.repeat(np.repeat(scales, 4, 0), 4, 1)
+    W1 = make_block_sparse(W1 / np.sqrt((W1 ** 2).sum(1, keepdims=True)), sparsity, seed + 1)
     W2 = make_block_sparse(rng.standard_normal((10, 128)) / math.sqrt(128), sparsity, seed + 2)
     return [Layer(W1, rng.standard_normal(128) * 0.1, "square"),
             Layer(W2, rng.standard_normal(10) * 0.1, "none")]

@@ -2,7 +2,7 @@
 
     python -m ckks_b200.train_gear train   [--traces 200000] [--epochs 40] [--out PATH]
     torchrun --nproc-per-node G -m ckks_b200.train_gear train ...   (data-parallel)
-    python -m ckks_b200.train_gear compare [--net PATH] [--model mlp|cnn] [--batches 8]
+    python -m ckks_b200.train_gear compare [--net PATH] [--model mlp|cnn|mlp_compressible] [--batches 8]
 
 train: generates noise-monitor traces by running random encrypted layers of
 the encrypted-MLP family (N = 2^13, L = 4) at every gear, trains the
@@ -55,13 +55,17 @@ def compare(net_path: Path = DEFAULT_NET, model: str = "mlp", batches: int = 8, 
     from .evaluator import Evaluator
     from .gear_learn import GearNet, LearnedController, PlainController
     from .mlp import EncryptedMLP
-    from .models import cnn_28x28, mlp_784_128_10, run_stream
+    from .models import cnn_28x28, mlp_784_128_10, mlp_784_128_10_compressible, run_stream
     from .params import CkksParams
-    levels = 4 if model == "mlp" else 5
+    if model not in ("mlp", "cnn", "mlp_compressible"):
+        raise ValueError(f"model={model!r}")
+    levels = 5 if model == "cnn" else 4
     ev = Evaluator(CkksParams.standard(13, levels, seed=seed + 7))
     ev.keygen()
-    layers = mlp_784_128_10(seed) if model == "mlp" else cnn_28x28(seed)
-    m = EncryptedMLP(ev, layers)
+    layers = {"mlp": mlp_784_128_10, "cnn": cnn_28x28, "mlp_compressible": mlp_784_128_10_compressible}[model](seed)
+    # the compressible model runs on the integer pipe, whose layer time
+    # shrinks with a gear's kept blocks (the tensor-core layer is dense)
+    m = EncryptedMLP(ev, layers, tensor_cores=model != "mlp_compressible")
     rng = np.random.default_rng(seed + 1)
     data = [rng.uniform(0, 1, (batch, 784)) for _ in range(batches)]
     # warm-up: a full batch at every gear with every probe (kernels, weight
@@ -94,6 +98,7 @@ def compare(net_path: Path = DEFAULT_NET, model: str = "mlp", batches: int = 8, 
         return h.tolist()
     drop = ("gears", "attempted_gears")
     return {"model": model, "target_db": target_db, "batch": batch, "batches": batches,
+            "engine": "tensor cores" if m.tensor_cores else "integer pipe",
             "plain": {k: v for k, v in rp.items() if k not in drop}, "plain_gears": rp["gears"],
             "learned": {k: v for k, v in rl.items() if k not in drop}, "learned_gears": rl["gears"],
             "plain_gear_histogram": hist(rp["gears"]), "learned_gear_histogram": hist(rl["gears"]),
@@ -126,7 +131,7 @@ def main(argv=None) -> int:
     t.add_argument("--out", default=str(DEFAULT_NET))
     c = sub.add_parser("compare")
     c.add_argument("--net", default=str(DEFAULT_NET))
-    c.add_argument("--model", default="mlp", choices=["mlp", "cnn"])
+    c.add_argument("--model", default="mlp", choices=["mlp", "cnn", "mlp_compressible"])
     c.add_argument("--batches", type=int, default=8)
     c.add_argument("--target-db", type=float, default=40.0)
     a = ap.parse_args(argv)

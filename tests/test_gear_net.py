@@ -151,3 +151,56 @@ def test_learned_controller_selects_sparse_gears_when_admissible(cuda):
     assert max(layer0[1:]) >= 1, (layer0, "measured", measured, "predicted", predicted)
     assert r["recomputed_layers"] == 0
     assert r["snr_db"] >= 40.0
+
+
+@pytest.mark.gpu
+def test_learned_controller_falls_back_when_its_prediction_is_wrong(cuda):
+    """A predictor that is wrong on purpose (every gear predicted at 120 dB):
+    after calibration the controller runs gear 3, the first-use probe (the
+    plain monitor, judge of the learned one) measures the layer far below the
+    target, the layer is recomputed at gear 0 and its gear capped below the
+    failed one; every later attempt is probed the same way (one gear lower
+    each batch), so the stream still meets the target with the plaintext
+    model's top-1."""
+    from ckks_b200.evaluator import Evaluator
+    from ckks_b200.gear_learn import GearNet, LearnedController
+    from ckks_b200.mlp import EncryptedMLP
+    from ckks_b200.models import mlp_784_128_10, run_stream
+    from ckks_b200.params import CkksParams
+    P = GM.unpack(GM.init(0))
+    P["W3"][:] = 0.0
+    P["b3"][:] = 1.2            # 120 dB for every gear, whatever the features
+    net = GearNet(GM.pack(P))
+    ev = Evaluator(CkksParams.standard(13, 4, seed=7))
+    ev.keygen()
+    m = EncryptedMLP(ev, mlp_784_128_10(0))
+    rng = np.random.default_rng(3)
+    data = [rng.uniform(0, 1, (1024, 784)) for _ in range(4)]
+    ctl = LearnedController(m, net, 40.0)
+    r = run_stream(m, ctl, data, fallback_db=40.0)
+    att = r["attempted_gears"]
+    assert att[0] == [0, 0]                            # calibration batch
+    assert att[1:] == [[3, 3], [2, 2], [1, 1]]         # the wrong prediction is acted on, capped lower each time
+    assert all(g == [0, 0] for g in r["gears"])        # every sparse attempt caught and recomputed
+    assert r["recomputed_layers"] == 6
+    assert r["snr_db"] >= 40.0 and r["min_batch_snr_db"] >= 40.0
+    assert r["top1_agreement"] == 1.0
+
+
+@pytest.mark.gpu
+def test_compressible_mlp_learned_arm_runs_sparse_gears(cuda):
+    """784-128-10 with trained-like compressible hidden weights on the integer
+    pipe (a gear's dropped blocks are skipped, so sparse gears are faster):
+    the learned controller runs the hidden layer at a sparse gear once
+    calibrated, with no recompute, meets the 40 dB target and is faster than
+    the plain arm, which (the RTL policy) only ever re-attempts gear 3 and
+    falls back to gear 0."""
+    from ckks_b200.train_gear import compare
+    r = compare(NET, "mlp_compressible", batches=8, batch=1024)
+    assert r["engine"] == "integer pipe"
+    assert sum(r["learned_gear_histogram"][0][1:]) >= 6
+    assert r["learned"]["recomputed_layers"] == 0
+    assert r["learned"]["snr_db"] >= 40.0 and r["learned"]["min_batch_snr_db"] >= 40.0
+    assert r["plain"]["snr_db"] >= 40.0
+    assert r["learned"]["top1_agreement"] >= 0.999
+    assert r["speedup"] >= 1.1, r
