@@ -468,7 +468,7 @@ def measure_batch(dev, n_items: int = 4096, steps: int = 10, warmup: int = 3) ->
     level uniform in 2..8 (45-bit primes).  Reference outputs come from the
     eager per-bucket path (one batched launch sequence per same-shape
     bucket); the persistent plan (one kernel launch per graph replay) is
-    checked bit-exact against them, its lag and CTAs per SM tuned, then
+    checked bit-exact against them, its lag tuned, then
     timed as graph replays; the per-bucket graph (default launch shapes) is
     timed beside it."""
     import numpy as np
@@ -500,7 +500,7 @@ def measure_batch(dev, n_items: int = 4096, steps: int = 10, warmup: int = 3) ->
            "workload": f"{n_items} items ({ctct} ct x ct + relin + rescale, {n_items - ctct} ct x pt + rescale), "
                        "N uniform in {2^12, 2^13}, level uniform in 2..8, 45-bit primes, seed 0",
            "buckets": len(ex.buckets), "units_per_step": info["units"], "grid": info["grid"],
-           "lag_percent": info["lag_percent"], "ctas_per_sm": info["ctas_per_sm"],
+           "slots_per_step": info["slots"], "lag_percent": info["lag_percent"],
            "persistent_sweep_ms": tune["sweep"],
            "launches_per_step": {"kernels": 1, "memsets": 1},
            "bit_exact_vs_eager_per_bucket": bool(exact and exact_graph), "incomplete_items": n_bad,

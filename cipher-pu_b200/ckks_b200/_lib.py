@@ -105,13 +105,13 @@ SIGNATURES: dict[str, tuple] = {
     "ckks_gear_ctrl_init": (_i32, [_vp, C.POINTER(_u64), C.POINTER(_u64), _i32]),
     "ckks_gear_ctrl_raw": (_i32, [_vp, _u64, _u64]),
     "ckks_gear_ctrl_flush": (_i32, [_vp, _u64, _u64, _i32, _i32, _i32]),
-    "ckks_batch_plan_create": (_i32, [C.POINTER(BatchBucket), _i32, _i32, _i32, C.POINTER(_vp)]),
+    "ckks_batch_plan_create": (_i32, [C.POINTER(BatchBucket), _i32, _i32, C.POINTER(_vp)]),
     "ckks_batch_plan_run": (_i32, [_vp, C.c_longlong, _i32, _vp]),
     "ckks_batch_plan_incomplete": (_i32, [_vp, C.POINTER(_i32), _vp]),
-    "ckks_batch_plan_info": (_i32, [_vp, C.POINTER(C.c_longlong), C.POINTER(_i32), C.POINTER(_i32),
-                                     C.POINTER(_sz)]),
+    "ckks_batch_plan_info": (_i32, [_vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(_i32),
+                                     C.POINTER(_i32), C.POINTER(_sz)]),
     "ckks_batch_plan_destroy": (None, [_vp]),
-    "ckks_batch_schedule": (_i32, [_i32, _vp, _vp, _vp, _vp, C.c_longlong, _vp, C.POINTER(C.c_longlong)]),
+    "ckks_batch_schedule": (_i32, [_i32, _vp, _vp, _vp, _vp, _vp, C.c_longlong, _vp, C.POINTER(C.c_longlong)]),
     "ckks_profile_enable": (_i32, [_i32]),
     "ckks_profile_reset": (_i32, []),
     "ckks_profile_read": (_i32, [_i32, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),

@@ -19,9 +19,8 @@ The autotuner times every bucket alone under each launch shape (per-thread
 radix 2^K, K = 2..5, balanced or tight register budget, limbs / work units
 per CTA, the persistent TMA-fed tensor kernel, chunking of the bucket into
 launches) and keeps the fastest, then times the persistent plan under each
-lag (how far a dependent stage is listed after its producers) and CTAs per
-SM, and keeps whichever execution is faster; the choice is baked into the
-graph at capture time.
+lag (how far a dependent stage is listed after its producers); the choice
+is baked into the graph at capture time.
 
 The reference's batching is time multiplexing of four poly-mult instances on
 one FPGA (rtl/m4/e2e_ckks_mult_ctrl_m4.sv:368-482, TIME_MULT = 4 in
@@ -96,7 +95,7 @@ class PersistentPlan:
     and allocates its device memory, lists the work units), then run any
     number of times; ``run`` is capturable into a CUDA graph."""
 
-    def __init__(self, evs: dict, buckets: list, lag_percent: int = 200, ctas_per_sm: int = 1):
+    def __init__(self, evs: dict, buckets: list, lag_percent: int = 400):
         arr = (_lib.BatchBucket * max(1, len(buckets)))()
         for i, bk in enumerate(buckets):
             ev = evs[bk.shape.log_n]
@@ -105,11 +104,10 @@ class PersistentPlan:
                                       bk.shape.level, 0 if ctct else 1, bk.a.data_ptr(), bk.b.data_ptr(),
                                       bk.out.data_ptr(), ev.rlk.data_ptr() if ctct else None)
         h = ctypes.c_void_p()
-        _lib.call("ckks_batch_plan_create", arr, len(buckets), int(lag_percent), int(ctas_per_sm), ctypes.byref(h))
+        _lib.call("ckks_batch_plan_create", arr, len(buckets), int(lag_percent), ctypes.byref(h))
         self.handle = h
         self.buckets = buckets
         self.lag_percent = lag_percent
-        self.ctas_per_sm = ctas_per_sm
 
     def run(self, wait_cycles: int = 0, flags: int = 0, stream=None):
         st = (stream or torch.cuda.current_stream()).cuda_stream
@@ -123,11 +121,12 @@ class PersistentPlan:
         return n.value, [bool(flags[i]) for i in range(len(self.buckets))]
 
     def info(self) -> dict:
-        nu, grid, smem, nb = ctypes.c_longlong(), ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
-        _lib.call("ckks_batch_plan_info", self.handle, ctypes.byref(nu), ctypes.byref(grid), ctypes.byref(smem),
-                  ctypes.byref(nb))
-        return {"units": nu.value, "grid": grid.value, "smem_bytes": smem.value, "device_bytes": nb.value,
-                "lag_percent": self.lag_percent, "ctas_per_sm": self.ctas_per_sm}
+        nu, ns = ctypes.c_longlong(), ctypes.c_longlong()
+        grid, smem, nb = ctypes.c_int(), ctypes.c_int(), ctypes.c_size_t()
+        _lib.call("ckks_batch_plan_info", self.handle, ctypes.byref(nu), ctypes.byref(ns), ctypes.byref(grid),
+                  ctypes.byref(smem), ctypes.byref(nb))
+        return {"units": nu.value, "slots": ns.value, "grid": grid.value, "smem_bytes": smem.value,
+                "device_bytes": nb.value, "lag_percent": self.lag_percent}
 
     def close(self):
         if self.handle:
@@ -183,12 +182,12 @@ class BatchExecutor:
         self._mode = m
         self.graph = None               # a captured step belongs to one mode
 
-    def persistent_plan(self, lag_percent: int = 200, ctas_per_sm: int = 1) -> PersistentPlan:
-        if self.plan is not None and (self.plan.lag_percent, self.plan.ctas_per_sm) == (lag_percent, ctas_per_sm):
+    def persistent_plan(self, lag_percent: int = 400) -> PersistentPlan:
+        if self.plan is not None and self.plan.lag_percent == lag_percent:
             return self.plan
         if self.plan is not None:
             self.plan.close()
-        self.plan = PersistentPlan(self.evs, self.buckets, lag_percent, ctas_per_sm)
+        self.plan = PersistentPlan(self.evs, self.buckets, lag_percent)
         self.graph = None
         return self.plan
 
@@ -326,34 +325,30 @@ class BatchExecutor:
         self.graph = None
         return choices
 
-    def autotune_persistent(self, reps: int = 3, lags=(100, 200, 400), ctas=(1, 2)) -> dict:
-        """Time the persistent plan under each lag and CTAs-per-SM choice
-        (2 only where every bucket is N = 2^12); keep the fastest plan."""
+    def autotune_persistent(self, reps: int = 3, lags=(200, 400, 800)) -> dict:
+        """Time the persistent plan under each lag (how far a dependent stage
+        is listed after its producers, in % of a wave); keep the fastest."""
         sweep = {}
         best = None
-        only12 = all(b.shape.log_n == 12 for b in self.buckets)
         for lag in lags:
-            for c in ctas:
-                if c == 2 and not only12:
-                    continue
-                plan = PersistentPlan(self.evs, self.buckets, lag, c)
+            plan = PersistentPlan(self.evs, self.buckets, lag)
+            plan.run()
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(reps):
                 plan.run()
-                torch.cuda.synchronize()
-                e0 = torch.cuda.Event(enable_timing=True)
-                e1 = torch.cuda.Event(enable_timing=True)
-                e0.record()
-                for _ in range(reps):
-                    plan.run()
-                e1.record()
-                torch.cuda.synchronize()
-                t = e0.elapsed_time(e1) / reps
-                sweep[f"lag{lag}/c{c}"] = round(t, 4)
-                if best is None or t < best[0]:
-                    if best is not None:
-                        best[1].close()
-                    best = (t, plan)
-                else:
-                    plan.close()
+            e1.record()
+            torch.cuda.synchronize()
+            t = e0.elapsed_time(e1) / reps
+            sweep[f"lag{lag}"] = round(t, 4)
+            if best is None or t < best[0]:
+                if best is not None:
+                    best[1].close()
+                best = (t, plan)
+            else:
+                plan.close()
         if self.plan is not None:
             self.plan.close()
         self.plan = best[1]

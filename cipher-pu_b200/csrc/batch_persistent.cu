@@ -10,8 +10,13 @@
 // unit comes after the units it depends on, and places a dependent stage a
 // configurable number of units (the lag) after its producers so that by the
 // time a CTA takes it, the producers have usually finished; ct x pt units,
-// which depend on nothing, fill the tail.  CTAs take units in list order from
-// one atomic ticket (the next ticket is fetched while the current unit runs).
+// which depend on nothing, fill the tail.  The list is cut into slots: one
+// N = 2^13 unit (radix 2^4: all 512 threads of the CTA), or two consecutive
+// N = 2^12 units (radix 2^4: 256 threads each, run side by side by the two
+// halves of the CTA on their own named barriers and shared-memory halves, as
+// two CTAs of the per-shape kernels share an SM).  CTAs take slots in list
+// order from one atomic ticket (the next ticket is fetched while the current
+// slot runs).
 //
 // Dependencies are per-item counters: a tensor unit adds 1 to its pair's
 // counter when its stores are done (every thread fences, the CTA syncs, one
@@ -43,8 +48,13 @@
 
 namespace {
 
-constexpr int PB_THREADS = 512;  // N / 2^K for (2^12, K = 3) and (2^13, K = 4)
+constexpr int PB_THREADS = 512;  // one N = 2^13 unit at radix 2^4, or two N = 2^12 units
+constexpr int PB_HALF = 256;     // threads of one N = 2^12 unit at radix 2^4
+// shared memory of one N = 2^12 unit (the largest: ModUp / ModDown accumulators)
+constexpr int PB_SM12_WORDS = NttShape<12, 4>::SMEM_WORDS + 2 * 4096;
+constexpr int PB_SM13_WORDS = NttShape<13, 4>::SMEM_WORDS + 2 * 8192;
 enum { PB_TENSOR = 0, PB_MODUP = 1, PB_DOWN = 2, PB_CTPT = 3 };
+constexpr unsigned PB_NONE = 0xFFFFFFFFu;
 
 struct PbBucket {
   int op;        // CKKS_BATCH_CT_CT or CKKS_BATCH_CT_PT
@@ -66,8 +76,12 @@ struct PbBucket {
 };
 
 // One work unit: x = bucket << 8 | stage << 6 | sub (limb, target prime or
-// output polynomial), y = item.
+// output polynomial), y = item.  A slot is one or two units (u[1].x =
+// PB_NONE: one).
 using PbJob = uint2;
+struct PbSlot {
+  PbJob u[2];
+};
 
 // The bucket table travels as a kernel parameter (constant bank): the units
 // then read their descriptors' fields as operands instead of holding them in
@@ -132,62 +146,78 @@ __device__ __forceinline__ void pb_run_unit(const PbBucket& B, int stage, int su
   }
 }
 
+// One unit on one thread group (the whole CTA for N = 2^13, a half for
+// 2^12; tid = the thread's index in its group, grp = the group): wait for its
+// inputs if it has any, run it, publish it.  False when the wait gave up.
+template <int LOGN, int K>
+__device__ __forceinline__ void pb_unit(const PbTable& tab, PbJob jb, u64* sm, int tid, int grp, unsigned* ctl,
+                                        long long wait_limit, int unmet_bucket, int* s_ok) {
+  constexpr int T = NttShape<LOGN, K>::T;
+  const int bi = (int)(jb.x >> 8), stage = (int)(jb.x >> 6) & 3, sub = (int)(jb.x & 63);
+  const long long item = jb.y;
+  const PbBucket& B = tab.b[bi];
+  const int n_ct = B.n_ct;
+  if (stage == PB_MODUP || stage == PB_DOWN) {
+    if (tid == 0) {
+      const unsigned* c = stage == PB_MODUP ? B.cnt + item : B.cnt + n_ct + item;
+      unsigned target = stage == PB_MODUP ? (unsigned)B.level : (unsigned)B.level + 1;
+      if (stage == PB_MODUP && bi == unmet_bucket && item == 0) target += 1;
+      s_ok[grp] = pb_wait(c, target, ctl + 2, wait_limit);
+    }
+    group_sync<T>();
+    if (!s_ok[grp]) return;
+  }
+  pb_run_unit<LOGN, K>(B, stage, sub, item, sm, tid);
+  // publish: every thread's stores, then one release add for the group
+  __threadfence();
+  group_sync<T>();
+  if (tid == 0) {
+    unsigned* c = stage == PB_TENSOR ? B.cnt + item
+                  : stage == PB_MODUP ? B.cnt + n_ct + item
+                  : stage == PB_DOWN  ? B.cnt + 2 * (size_t)n_ct + item
+                                      : B.cnt + item;
+    red_release_add(c, 1u);
+  }
+}
+
 // ctl[0..1]: the 64-bit ticket, ctl[2]: the abort flag (zeroed before every
 // launch).
 // unmet_bucket >= 0 is a test hook: the ModUp units of item 0 of that
 // bucket wait for one tensor unit more than exist, so their wait can only
 // end by its limit.
-template <int MAXLOGN, int MINB>
-__global__ void __launch_bounds__(PB_THREADS, MINB)
-    k_batch_persistent(const __grid_constant__ PbTable tab, const PbJob* __restrict__ jobs, long long n_jobs,
+template <int MAXLOGN>
+__global__ void __launch_bounds__(PB_THREADS, 1)
+    k_batch_persistent(const __grid_constant__ PbTable tab, const PbSlot* __restrict__ slots, long long n_slots,
                        unsigned* ctl, long long wait_limit, int unmet_bucket) {
   extern __shared__ u64 sm[];
   __shared__ long long s_ticket;
-  __shared__ int s_ok;
+  __shared__ int s_ok[2];
   const int tid = threadIdx.x;
   unsigned long long next = 0;
   if (tid == 0) next = atomicAdd(reinterpret_cast<unsigned long long*>(ctl), 1ull);
   for (;;) {
     if (tid == 0) {
       const unsigned long long t = next;
-      const bool go = (long long)t < n_jobs && !ld_volatile_u32(ctl + 2);
-      // fetch the following ticket now; it is used once this unit is done
+      const bool go = (long long)t < n_slots && !ld_volatile_u32(ctl + 2);
+      // fetch the following ticket now; it is used once this slot is done
       if (go) next = atomicAdd(reinterpret_cast<unsigned long long*>(ctl), 1ull);
       s_ticket = go ? (long long)t : -1;
     }
     __syncthreads();
     const long long t = s_ticket;
     if (t < 0) return;
-    const PbJob jb = jobs[t];
-    const int bi = (int)(jb.x >> 8), stage = (int)(jb.x >> 6) & 3, sub = (int)(jb.x & 63);
-    const long long item = jb.y;
-    const PbBucket& B = tab.b[bi];
-    const int n_ct = B.n_ct;
-    if (stage == PB_MODUP || stage == PB_DOWN) {
-      if (tid == 0) {
-        const unsigned* c = stage == PB_MODUP ? B.cnt + item : B.cnt + n_ct + item;
-        unsigned target = stage == PB_MODUP ? (unsigned)B.level : (unsigned)B.level + 1;
-        if (stage == PB_MODUP && bi == unmet_bucket && item == 0) target += 1;
-        s_ok = pb_wait(c, target, ctl + 2, wait_limit);
-      }
-      __syncthreads();
-      if (!s_ok) return;
+    const PbJob j0 = slots[t].u[0];
+    bool big = false;
+    if constexpr (MAXLOGN >= 13) big = tab.b[j0.x >> 8].log_n == 13;
+    if (big) {
+      if constexpr (MAXLOGN >= 13) pb_unit<13, 4>(tab, j0, sm, tid, 0, ctl, wait_limit, unmet_bucket, s_ok);
+    } else {
+      const int h = tid / PB_HALF;  // uniform within each half
+      const PbJob jh = slots[t].u[h];
+      if (jh.x != PB_NONE)
+        pb_unit<12, 4>(tab, jh, sm + h * PB_SM12_WORDS, tid % PB_HALF, h, ctl, wait_limit, unmet_bucket, s_ok);
     }
-    if (B.log_n == 12) {
-      pb_run_unit<12, 3>(B, stage, sub, item, sm, tid);
-    } else if constexpr (MAXLOGN >= 13) {
-      pb_run_unit<13, 4>(B, stage, sub, item, sm, tid);
-    }
-    // publish: every thread's stores, then one release add for the CTA
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) {
-      unsigned* c = stage == PB_TENSOR ? B.cnt + item
-                    : stage == PB_MODUP ? B.cnt + n_ct + item
-                    : stage == PB_DOWN  ? B.cnt + 2 * (size_t)n_ct + item
-                                        : B.cnt + item;
-      red_release_add(c, 1u);
-    }
+    __syncthreads();  // both halves done: the shared memory is free for the next slot
   }
 }
 
@@ -208,16 +238,16 @@ int ckks_batch_status_take(unsigned* n) {
 struct ckks_batch_plan {
   int device = 0;
   int max_log_n = 12;
-  int minb = 1;
   int grid = 0;
   int smem = 0;
-  long long n_jobs = 0;
+  long long n_units = 0;
+  long long n_slots = 0;
   int n_buckets = 0;
   unsigned char* mem = nullptr;  // one device allocation
   size_t mem_bytes = 0;
   size_t zero_bytes = 0;         // ctl + counters, at the start of mem
   unsigned* ctl = nullptr;
-  PbJob* d_jobs = nullptr;
+  PbSlot* d_slots = nullptr;
   std::vector<PbBucket> h_buckets;
   PbTable* table = nullptr;      // host copy passed at every launch
   std::vector<size_t> cnt_off;   // per bucket, in counters
@@ -227,16 +257,16 @@ struct ckks_batch_plan {
 
 namespace {
 
-template <int MAXLOGN, int MINB>
+template <int MAXLOGN>
 int pb_launch(ckks_batch_plan* p, long long wait_limit, int unmet_bucket, cudaStream_t st) {
-  k_batch_persistent<MAXLOGN, MINB><<<p->grid, PB_THREADS, p->smem, st>>>(*p->table, p->d_jobs, p->n_jobs, p->ctl,
-                                                                         wait_limit, unmet_bucket);
+  k_batch_persistent<MAXLOGN><<<p->grid, PB_THREADS, p->smem, st>>>(*p->table, p->d_slots, p->n_slots, p->ctl,
+                                                                   wait_limit, unmet_bucket);
   return ckks_check_launch("ckks_batch_plan_run");
 }
 
-template <int MAXLOGN, int MINB>
+template <int MAXLOGN>
 int pb_configure(ckks_batch_plan* p, const char* fn) {
-  auto k = k_batch_persistent<MAXLOGN, MINB>;
+  auto k = k_batch_persistent<MAXLOGN>;
   // raise the kernel's dynamic shared-memory cap, never lower it: plans of
   // other shapes may launch the same kernel with more
   cudaFuncAttributes fa{};
@@ -319,34 +349,60 @@ static void pb_schedule(int n_buckets, const int* op, const int* n_ct, const int
   }
 }
 
-// The work list on the host alone (no device, no context): jobs gets
-// 2 x uint32 per unit, (bucket << 8 | stage << 6 | sub, item) with stage 0
-// tensor, 1 ModUp, 2 ModDown, 3 ct x pt.  n_units (in/out): capacity in, units
-// listed out.  `cost` ranks the buckets (costliest first); `lag` in units.
+// Cut the unit list into slots: an N = 2^13 unit alone; N = 2^12 units two
+// by two in list order (a 2^12 unit waiting for its partner may be passed by
+// 2^13 slots: it only moves later, after its own producers).  Returns the
+// slot count; slots must hold n_units entries.
+static long long pb_slots(const PbJob* jobs, long long n_units, const int* log_n, PbSlot* slots) {
+  long long ns = 0;
+  long long pending = -1;
+  for (long long i = 0; i < n_units; ++i) {
+    if (log_n[jobs[i].x >> 8] == 13) {
+      slots[ns++] = PbSlot{{jobs[i], PbJob{PB_NONE, 0}}};
+    } else if (pending >= 0) {
+      slots[ns++] = PbSlot{{jobs[pending], jobs[i]}};
+      pending = -1;
+    } else {
+      pending = i;
+    }
+  }
+  if (pending >= 0) slots[ns++] = PbSlot{{jobs[pending], PbJob{PB_NONE, 0}}};
+  return ns;
+}
+
+// The work list on the host alone (no device, no context): slots gets 4 x
+// uint32 per slot, two units (bucket << 8 | stage << 6 | sub, item) with
+// stage 0 tensor, 1 ModUp, 2 ModDown, 3 ct x pt, the second 0xFFFFFFFF, 0 in
+// a slot of one unit.  n_slots (in/out): capacity in (at least the number of
+// units), slots listed out.  `cost` ranks the buckets (costliest first); `lag`
+// in units.
 extern "C" int ckks_batch_schedule(int n_buckets, const int* op, const int* n_ct, const int* level,
-                                   const double* cost, long long lag, uint32_t* jobs, long long* n_units) {
+                                   const int* log_n, const double* cost, long long lag, uint32_t* slots,
+                                   long long* n_slots) {
   const char* fn = "ckks_batch_schedule";
-  CKKS_REQUIRE(n_units != nullptr, "%s: n_units is NULL", fn);
+  CKKS_REQUIRE(n_slots != nullptr, "%s: n_slots is NULL", fn);
   CKKS_REQUIRE(n_buckets >= 0 && n_buckets <= PB_MAX_BUCKETS, "%s: n_buckets=%d outside [0, %d]", fn, n_buckets,
                PB_MAX_BUCKETS);
-  CKKS_REQUIRE(n_buckets == 0 || (op && n_ct && level && cost), "%s: NULL pointer argument", fn);
+  CKKS_REQUIRE(n_buckets == 0 || (op && n_ct && level && log_n && cost), "%s: NULL pointer argument", fn);
   CKKS_REQUIRE(lag >= 0, "%s: lag < 0", fn);
   long long total = 0;
   for (int b = 0; b < n_buckets; ++b) {
     CKKS_REQUIRE(op[b] == CKKS_BATCH_CT_CT || op[b] == CKKS_BATCH_CT_PT, "%s: bucket %d: op=%d", fn, b, op[b]);
     CKKS_REQUIRE(n_ct[b] >= 0 && level[b] >= 2 && level[b] <= 62, "%s: bucket %d: n_ct=%d level=%d", fn, b, n_ct[b],
                  level[b]);
+    CKKS_REQUIRE(log_n[b] == 12 || log_n[b] == 13, "%s: bucket %d: log_n=%d (12 or 13)", fn, b, log_n[b]);
     total += (long long)n_ct[b] * (op[b] == CKKS_BATCH_CT_CT ? 2 * level[b] + 3 : 2);
   }
-  CKKS_REQUIRE(jobs != nullptr || total == 0, "%s: jobs is NULL", fn);
-  CKKS_REQUIRE(*n_units >= total, "%s: capacity %lld < %lld units", fn, *n_units, total);
-  pb_schedule(n_buckets, op, n_ct, level, cost, lag, reinterpret_cast<PbJob*>(jobs));
-  *n_units = total;
+  CKKS_REQUIRE(slots != nullptr || total == 0, "%s: slots is NULL", fn);
+  CKKS_REQUIRE(*n_slots >= total, "%s: capacity %lld < %lld units", fn, *n_slots, total);
+  std::vector<PbJob> jobs((size_t)total);
+  pb_schedule(n_buckets, op, n_ct, level, cost, lag, jobs.data());
+  *n_slots = pb_slots(jobs.data(), total, log_n, reinterpret_cast<PbSlot*>(slots));
   return CKKS_OK;
 }
 
 extern "C" int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_buckets, int lag_percent,
-                                      int ctas_per_sm, ckks_batch_plan** out) {
+                                      ckks_batch_plan** out) {
   const char* fn = "ckks_batch_plan_create";
   CKKS_REQUIRE(out != nullptr, "%s: out is NULL", fn);
   *out = nullptr;
@@ -354,7 +410,6 @@ extern "C" int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_bu
                PB_MAX_BUCKETS);
   CKKS_REQUIRE(n_buckets == 0 || buckets != nullptr, "%s: buckets is NULL", fn);
   CKKS_REQUIRE(lag_percent >= 0 && lag_percent <= 10000, "%s: lag_percent=%d outside [0, 10000]", fn, lag_percent);
-  CKKS_REQUIRE(ctas_per_sm >= 0 && ctas_per_sm <= 2, "%s: ctas_per_sm=%d outside [0, 2]", fn, ctas_per_sm);
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: no current device", fn);
   auto p = new ckks_batch_plan();
@@ -392,7 +447,9 @@ extern "C" int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_bu
       if (!ctx->has_nega[i])
         return fail(ckks_set_error(CKKS_EINVAL, "%s: bucket %d: prime %d has no 2N-th root", fn, b, i));
     const int N = ctx->n;
-    const int words_sm = ctx->log_n == 12 ? NttShape<12, 3>::SMEM_WORDS : NttShape<13, 4>::SMEM_WORDS;
+    // an N = 2^13 unit uses the whole CTA's shared memory; 2^12 units run two
+    // side by side, each in a fixed half of PB_SM12_WORDS
+    smem = std::max(smem, ctx->log_n == 13 ? PB_SM13_WORDS * 8 : 2 * PB_SM12_WORDS * 8);
     if (B.op == CKKS_BATCH_CT_CT) {
       if (ctx->n_special != 1)
         return fail(ckks_set_error(CKKS_EINVAL, "%s: bucket %d: context needs exactly one special prime", fn, b));
@@ -405,13 +462,11 @@ extern "C" int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_bu
         return fail(ckks_set_error(CKKS_EINVAL, "%s: bucket %d: primes must satisfy max < 2 min", fn, b));
       scratch_words += (size_t)B.n_ct * (6 * B.level + 2) * N;
       n_units += (long long)B.n_ct * (2 * B.level + 3);
-      smem = std::max(smem, (words_sm + 2 * N) * 8);
     } else {
       for (int i = 0; i < B.level - 1; ++i)
         if (!(ctx->primes[B.level - 1] < 2 * ctx->primes[i]))
           return fail(ckks_set_error(CKKS_EINVAL, "%s: bucket %d: q_%d must be < 2 q_%d", fn, b, B.level - 1, i));
       n_units += 2ll * B.n_ct;
-      smem = std::max(smem, (words_sm + N) * 8);
     }
     p->max_log_n = std::max(p->max_log_n, ctx->log_n);
   }
@@ -419,11 +474,8 @@ extern "C" int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_bu
     return fail(ckks_set_error(CKKS_EUNSUPPORTED, "%s: %d B of shared memory per CTA exceed the device's limit", fn,
                                smem));
   p->smem = std::max(smem, 1024);
-  p->n_jobs = n_units;
-  p->minb = (ctas_per_sm == 2 && p->max_log_n == 12) ? 2 : 1;
-  int rc = p->max_log_n == 13 ? pb_configure<13, 1>(p, fn)
-           : p->minb == 2     ? pb_configure<12, 2>(p, fn)
-                              : pb_configure<12, 1>(p, fn);
+  p->n_units = n_units;
+  int rc = p->max_log_n == 13 ? pb_configure<13>(p, fn) : pb_configure<12>(p, fn);
   if (rc) return fail(rc);
 
   // ---- counters and device layout
@@ -437,8 +489,8 @@ extern "C" int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_bu
   const size_t off_ctl = 0;
   const size_t off_cnt = 256;
   p->zero_bytes = align256(off_cnt + n_cnt * sizeof(unsigned));
-  const size_t off_jobs = p->zero_bytes;
-  const size_t off_scr = align256(off_jobs + (size_t)n_units * sizeof(PbJob));
+  const size_t off_slots = p->zero_bytes;
+  const size_t off_scr = align256(off_slots + (size_t)n_units * sizeof(PbSlot));
   p->mem_bytes = off_scr + scratch_words * sizeof(u64);
   cudaError_t e = cudaMalloc(&p->mem, p->mem_bytes);
   if (e != cudaSuccess) {
@@ -447,7 +499,7 @@ extern "C" int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_bu
   }
   p->ctl = reinterpret_cast<unsigned*>(p->mem + off_ctl);
   unsigned* cnt = reinterpret_cast<unsigned*>(p->mem + off_cnt);
-  p->d_jobs = reinterpret_cast<PbJob*>(p->mem + off_jobs);
+  p->d_slots = reinterpret_cast<PbSlot*>(p->mem + off_slots);
   u64* scr = reinterpret_cast<u64*>(p->mem + off_scr);
   p->h_buckets.resize(n_buckets);
   for (int b = 0; b < n_buckets; ++b) {
@@ -481,21 +533,25 @@ extern "C" int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_bu
     }
   }
 
-  std::vector<int> ops(n_buckets), cts(n_buckets), lvls(n_buckets);
+  std::vector<int> ops(n_buckets), cts(n_buckets), lvls(n_buckets), logs(n_buckets);
   std::vector<double> costs(n_buckets);
   for (int b = 0; b < n_buckets; ++b) {
     ops[b] = buckets[b].op;
     cts[b] = buckets[b].n_ct;
     lvls[b] = buckets[b].level;
+    logs[b] = buckets[b].ctx->log_n;
     costs[b] = (double)buckets[b].ctx->n * (2 * buckets[b].level + 3);
   }
+  // a wave: every CTA on one slot, two units each (N = 2^12)
   std::vector<PbJob> jobs((size_t)n_units);
   pb_schedule(n_buckets, ops.data(), cts.data(), lvls.data(), costs.data(),
-              (long long)p->grid * lag_percent / 100, jobs.data());
+              (long long)p->grid * 2 * lag_percent / 100, jobs.data());
+  std::vector<PbSlot> slots((size_t)n_units);
+  p->n_slots = pb_slots(jobs.data(), n_units, logs.data(), slots.data());
   p->table = new PbTable();
   for (int b = 0; b < n_buckets; ++b) p->table->b[b] = p->h_buckets[b];
-  if (n_units)
-    e = cudaMemcpy(p->d_jobs, jobs.data(), (size_t)n_units * sizeof(PbJob), cudaMemcpyHostToDevice);
+  if (p->n_slots)
+    e = cudaMemcpy(p->d_slots, slots.data(), (size_t)p->n_slots * sizeof(PbSlot), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail(ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e)));
   *out = p;
   return CKKS_OK;
@@ -511,7 +567,7 @@ extern "C" int ckks_batch_plan_run(ckks_batch_plan* p, long long wait_cycles, in
   cudaStream_t st = as_stream(stream);
   cudaError_t e = cudaMemsetAsync(p->mem, 0, p->zero_bytes, st);
   if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
-  if (p->n_jobs == 0) return CKKS_OK;
+  if (p->n_slots == 0) return CKKS_OK;
   int unmet = -1;
   if (flags & CKKS_BATCH_RUN_UNMET_WAIT) {
     for (int b = 0; b < p->n_buckets && unmet < 0; ++b)
@@ -520,8 +576,7 @@ extern "C" int ckks_batch_plan_run(ckks_batch_plan* p, long long wait_cycles, in
   }
   const long long limit = wait_cycles > 0 ? wait_cycles : 2147483647ll;
   ProfSpan span(CKKS_STAGE_BATCH, st);
-  if (p->max_log_n == 13) return pb_launch<13, 1>(p, limit, unmet, st);
-  return p->minb == 2 ? pb_launch<12, 2>(p, limit, unmet, st) : pb_launch<12, 1>(p, limit, unmet, st);
+  return p->max_log_n == 13 ? pb_launch<13>(p, limit, unmet, st) : pb_launch<12>(p, limit, unmet, st);
 }
 
 extern "C" int ckks_batch_plan_incomplete(ckks_batch_plan* p, int* n_incomplete, uint8_t* bucket_complete) {
@@ -545,10 +600,11 @@ extern "C" int ckks_batch_plan_incomplete(ckks_batch_plan* p, int* n_incomplete,
   return CKKS_OK;
 }
 
-extern "C" int ckks_batch_plan_info(const ckks_batch_plan* p, long long* n_units, int* grid, int* smem_bytes,
-                                    size_t* device_bytes) {
+extern "C" int ckks_batch_plan_info(const ckks_batch_plan* p, long long* n_units, long long* n_slots, int* grid,
+                                    int* smem_bytes, size_t* device_bytes) {
   CKKS_REQUIRE(p != nullptr, "ckks_batch_plan_info: plan is NULL");
-  if (n_units) *n_units = p->n_jobs;
+  if (n_units) *n_units = p->n_units;
+  if (n_slots) *n_slots = p->n_slots;
   if (grid) *grid = p->grid;
   if (smem_bytes) *smem_bytes = p->smem;
   if (device_bytes) *device_bytes = p->mem_bytes;

@@ -57,6 +57,20 @@ struct NttShape {
 
 __device__ __forceinline__ int padix(int p, int sh) { return p + (p >> sh); }
 
+// Barrier of the T threads that run one transform.  Every kernel but one
+// launches exactly T threads per CTA, where this is a CTA-wide barrier; the
+// persistent batch kernel runs two N = 2^12 transforms (T = 256) side by side
+// in a 512-thread CTA, each group on its own named barrier 1 + threadIdx.x / T.
+// Below one warp (T < 32, tiny rings) the hardware needs the CTA barrier.
+template <int T>
+__device__ __forceinline__ void group_sync() {
+  if constexpr (T < 32) {
+    __syncthreads();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + (int)(threadIdx.x / T)), "n"(T) : "memory");
+  }
+}
+
 // position of register (c, r) of a pass that starts at stage S0 with KP stages
 template <int LOGN, int K, int S0, int KP>
 __device__ __forceinline__ int pass_pos(int tid, int c, int r) {
@@ -241,9 +255,9 @@ struct FwdRest {
     using S = NttShape<LOGN, K>;
     if constexpr (P <= S::NP) {
       sm_store<LOGN, K, S::s0(P - 1), S::kp(P - 1)>(x, sm, tid);
-      __syncthreads();
+      group_sync<S::T>();
       sm_load<LOGN, K, S::s0(P), S::kp(P)>(x, sm, tid);
-      __syncthreads();
+      group_sync<S::T>();
       fwd_pass<LOGN, K, S::s0(P), S::kp(P)>(x, tid, tw, qd);
       FwdRest<LOGN, K, P + 1>::run(x, sm, tid, tw, qd);
     }
@@ -258,9 +272,9 @@ struct InvRest {
     if constexpr (P >= 1) {
       inv_pass<LOGN, K, S::s0(P), S::kp(P)>(x, tid, itw, qd);
       sm_store<LOGN, K, S::s0(P), S::kp(P)>(x, sm, tid);
-      __syncthreads();
+      group_sync<S::T>();
       sm_load<LOGN, K, S::s0(P - 1), S::kp(P - 1)>(x, sm, tid);
-      __syncthreads();
+      group_sync<S::T>();
       InvRest<LOGN, K, P - 1>::run(x, sm, tid, itw, qd);
     }
   }
@@ -368,10 +382,10 @@ __device__ __forceinline__ void z_to_c(V (&x)[1 << K], u64* sm, int tid) {
   V* sv = reinterpret_cast<V*>(sm);
 #pragma unroll
   for (int e = 0; e < (1 << K); ++e) sv[padix(posZ<LOGN, K>(tid, e), S::PADSH)] = x[e];
-  __syncthreads();
+  group_sync<S::T>();
 #pragma unroll
   for (int e = 0; e < (1 << K); ++e) x[e] = sv[padix(posC<LOGN, K>(tid, e), S::PADSH)];
-  __syncthreads();
+  group_sync<S::T>();
 }
 template <int LOGN, int K, typename V>
 __device__ __forceinline__ void c_to_z(V (&x)[1 << K], u64* sm, int tid) {
@@ -379,10 +393,10 @@ __device__ __forceinline__ void c_to_z(V (&x)[1 << K], u64* sm, int tid) {
   V* sv = reinterpret_cast<V*>(sm);
 #pragma unroll
   for (int e = 0; e < (1 << K); ++e) sv[padix(posC<LOGN, K>(tid, e), S::PADSH)] = x[e];
-  __syncthreads();
+  group_sync<S::T>();
 #pragma unroll
   for (int e = 0; e < (1 << K); ++e) x[e] = sv[padix(posZ<LOGN, K>(tid, e), S::PADSH)];
-  __syncthreads();
+  group_sync<S::T>();
 }
 
 // Dynamic shared memory bytes needed by one transform.

@@ -677,10 +677,10 @@ int ckks_ct_mul_relin_rescale_noalloc(const ckks_ctx* ctx, uint64_t* out, const 
  * counters) and lists every work unit (a pair's tensor limbs, ModUp target
  * primes, ModDown polynomials; a ct x pt item's two polynomials) in a
  * dependency-respecting order, each dependent stage lag_percent % of one
- * wave of CTAs after its producers (0..10000; 200 is a good default).
- * ctas_per_sm: 0 or 1 = one 512-thread CTA per SM (128 registers a thread),
- * 2 = two (64 registers; for plans of N = 2^12 only).  The buckets' device
- * pointers are baked into the plan: they must stay valid while it is used.
+ * wave after its producers (0..10000; 400 is a good default), cut into
+ * slots: one N = 2^13 unit for a whole 512-thread CTA, or two N = 2^12 units
+ * that the CTA's halves run side by side.  The buckets' device pointers are
+ * baked into the plan: they must stay valid while it is used.
  *
  * ckks_batch_plan_run zeroes the plan's counters (one memset) and launches
  * the persistent kernel on `stream`: CTAs take units from one atomic ticket;
@@ -715,24 +715,25 @@ typedef struct ckks_batch_bucket {
   const uint64_t* key;
 } ckks_batch_bucket;
 typedef struct ckks_batch_plan ckks_batch_plan;
-int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_buckets, int lag_percent, int ctas_per_sm,
+int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_buckets, int lag_percent,
                            ckks_batch_plan** plan);
 int ckks_batch_plan_run(ckks_batch_plan* plan, long long wait_cycles, int flags, void* stream);
 int ckks_batch_plan_incomplete(ckks_batch_plan* plan, int* n_incomplete, uint8_t* bucket_complete);
-int ckks_batch_plan_info(const ckks_batch_plan* plan, long long* n_units, int* grid, int* smem_bytes,
-                         size_t* device_bytes);
+int ckks_batch_plan_info(const ckks_batch_plan* plan, long long* n_units, long long* n_slots, int* grid,
+                         int* smem_bytes, size_t* device_bytes);
 void ckks_batch_plan_destroy(ckks_batch_plan* plan);
 /*
  * The plan's work list computed on the host alone (no device): for buckets
- * described by op, n_ct, level and a cost that ranks them (costliest first),
- * with dependent stages `lag` units after their producers, writes two
- * uint32 per unit, (bucket << 8 | stage << 6 | sub, item): stage 0 tensor
- * (sub = limb), 1 ModUp (sub = target prime, level = the special prime),
- * 2 ModDown (sub = output polynomial), 3 ct x pt (sub = output polynomial).
- * *n_units: capacity in, units written out.
+ * described by op, n_ct, level, log_n (12 or 13) and a cost that ranks them
+ * (costliest first), with dependent stages `lag` units after their
+ * producers, writes 4 x uint32 per slot: two units (bucket << 8 | stage << 6
+ * | sub, item), stage 0 tensor (sub = limb), 1 ModUp (sub = target prime,
+ * level = the special prime), 2 ModDown (sub = output polynomial), 3 ct x pt
+ * (sub = output polynomial); the second unit is (0xFFFFFFFF, 0) in a slot of
+ * one.  *n_slots: capacity in (at least the number of units), slots out.
  */
-int ckks_batch_schedule(int n_buckets, const int* op, const int* n_ct, const int* level, const double* cost,
-                        long long lag, uint32_t* jobs, long long* n_units);
+int ckks_batch_schedule(int n_buckets, const int* op, const int* n_ct, const int* level, const int* log_n,
+                        const double* cost, long long lag, uint32_t* slots, long long* n_slots);
 
 /*
  * Per-kernel device timing (tracing).  When enabled, the multi-kernel entry

@@ -1,9 +1,11 @@
 """The persistent batch kernel (ckks_batch_plan_*): one launch drains a work
 list of mixed-N, mixed-level ct x ct and ct x pt work units with per-item
-dependency counters.  Its outputs are bit-identical to the eager per-bucket
-path (integer results: tolerance zero) under every lag and CTAs-per-SM
-choice, inside a CUDA graph too; a wait that nothing satisfies ends at its
-limit with CKKS_ETIMEOUT and the unfinished items reported incomplete."""
+dependency counters; N = 2^13 units take a whole 512-thread CTA, N = 2^12
+units run two side by side in its halves.  Its outputs are bit-identical to
+the eager per-bucket path (integer results: tolerance zero) under every lag,
+for one ring size or both, inside a CUDA graph too; a wait that nothing
+satisfies ends at its limit with CKKS_ETIMEOUT and the unfinished items
+reported incomplete."""
 import numpy as np
 import pytest
 
@@ -55,6 +57,10 @@ def test_persistent_equals_eager_and_oracle(mixed):
     info = plan.info()
     assert info["units"] == sum(b.count * ((2 * b.shape.level + 3) if b.shape.op == "ctct" else 2)
                                 for b in ex.buckets)
+    units13 = sum(b.count * ((2 * b.shape.level + 3) if b.shape.op == "ctct" else 2)
+                  for b in ex.buckets if b.shape.log_n == 13)
+    # every 2^13 unit alone, the 2^12 units two by two (at most one alone)
+    assert info["slots"] - units13 == (info["units"] - units13 + 1) // 2
     assert {b.shape.log_n for b in ex.buckets} == {12, 13}
     _clear(ex)
     plan.run()
@@ -104,7 +110,7 @@ def test_persistent_graph_replay(mixed):
     ex, ref = mixed
     ex.mode = "persistent"
     try:
-        ex.persistent_plan(200, 1)
+        ex.persistent_plan(400)
         _clear(ex)
         ex.capture()
         for _ in range(3):
@@ -116,18 +122,20 @@ def test_persistent_graph_replay(mixed):
         ex.mode = "streams"
 
 
-def test_persistent_two_ctas_per_sm(cuda):
-    """N = 2^12 only: the 64-register, two-CTAs-per-SM build."""
+@pytest.mark.parametrize("log_n", [12, 13])
+def test_persistent_one_ring_size(cuda, log_n):
+    """Plans of one ring size: N = 2^12 only (every slot two half-CTA units,
+    the 2^12-only kernel build) and N = 2^13 only (whole-CTA units)."""
     import torch
     from ckks_b200.batch import PersistentPlan
-    ex, ref = _executor(64, seed=6, log_ns=(12,))
-    for c in (1, 2):
-        plan = PersistentPlan(ex.evs, ex.buckets, ctas_per_sm=c)
-        assert plan.info()["ctas_per_sm"] == c
+    ex, ref = _executor(64, seed=6 + log_n, log_ns=(log_n,))
+    for lag in (0, 400):
+        plan = PersistentPlan(ex.evs, ex.buckets, lag_percent=lag)
         _clear(ex)
         plan.run()
         torch.cuda.synchronize()
-        assert all(_same(ex, ref)), c
+        assert plan.incomplete()[0] == 0
+        assert all(_same(ex, ref)), lag
         plan.close()
 
 
@@ -173,7 +181,7 @@ def test_plan_refusals(cuda):
     from ckks_b200.params import CkksParams
     h = ctypes.c_void_p()
     # empty plan: valid, runs nothing
-    _lib.call("ckks_batch_plan_create", None, 0, 200, 1, ctypes.byref(h))
+    _lib.call("ckks_batch_plan_create", None, 0, 200, ctypes.byref(h))
     _lib.call("ckks_batch_plan_run", h, 0, 0, None)
     _lib.raw("ckks_batch_plan_destroy")(h)
     P11 = CkksParams.standard(11, 3)
@@ -181,14 +189,14 @@ def test_plan_refusals(cuda):
     arr = (_lib.BatchBucket * 1)()
     arr[0] = _lib.BatchBucket(ctx11.handle, _lib.BATCH_CT_PT, 1, 3, 1, 16, 16, 16, None)
     with pytest.raises(CkksError, match="built for 12 and 13"):
-        _lib.call("ckks_batch_plan_create", arr, 1, 200, 1, ctypes.byref(h))
+        _lib.call("ckks_batch_plan_create", arr, 1, 200, ctypes.byref(h))
     P12 = CkksParams.standard(12, 3)
     ctx12 = Context.get(12, P12.primes, n_special=1)
     arr[0] = _lib.BatchBucket(ctx12.handle, _lib.BATCH_CT_PT, 1, 4, 1, 16, 16, 16, None)
     with pytest.raises(CkksError, match="level=4"):
-        _lib.call("ckks_batch_plan_create", arr, 1, 200, 1, ctypes.byref(h))
+        _lib.call("ckks_batch_plan_create", arr, 1, 200, ctypes.byref(h))
     arr[0] = _lib.BatchBucket(ctx12.handle, _lib.BATCH_CT_CT, 1, 3, 0, 16, 16, 16, None)
     with pytest.raises(CkksError, match="NULL"):
-        _lib.call("ckks_batch_plan_create", arr, 1, 200, 1, ctypes.byref(h))
+        _lib.call("ckks_batch_plan_create", arr, 1, 200, ctypes.byref(h))
     with pytest.raises(CkksError, match="n_buckets"):
-        _lib.call("ckks_batch_plan_create", arr, 129, 200, 1, ctypes.byref(h))
+        _lib.call("ckks_batch_plan_create", arr, 129, 200, ctypes.byref(h))
