@@ -294,9 +294,9 @@ size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 // ---------------------------------------------------------------- the work list
 // A greedy list schedule.  A ct x ct pair's ModUp units go in once `lag`
 // units have been listed after its last tensor unit, its ModDown units `lag`
-// after its last ModUp unit; otherwise the next pair's tensor units go in
-// (pairs of the costliest buckets first), then ct x pt units; with nothing
-// else left, a pending stage goes in early.  Every unit is listed once and
+// after its last ModUp unit; otherwise the next pairs' tensor units go in
+// (pairs of the costliest buckets first, two at a time), then ct x pt
+// units; with nothing else left, a pending stage goes in early.  Every unit is listed once and
 // after the units it depends on.  jobs must hold sum(n_ct (2 level + 3)) +
 // sum(2 n_ct) entries (ct x ct, ct x pt buckets).
 static void pb_schedule(int n_buckets, const int* op, const int* n_ct, const int* level, const double* cost,
@@ -311,10 +311,14 @@ static void pb_schedule(int n_buckets, const int* op, const int* n_ct, const int
   std::stable_sort(pt_order.begin(), pt_order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
   long long total = 0;
   for (int b = 0; b < n_buckets; ++b) total += (long long)n_ct[b] * (op[b] == CKKS_BATCH_CT_CT ? 2 * level[b] + 3 : 2);
+  // Pairs go in two at a time (items `item` and item + 1 of one bucket when
+  // n_items = 2), their units interleaved, so consecutive units have the same
+  // stage and length: two of them share a slot without one half idling.
   struct Pending {
     long long ready;
     int b, stage;
     long long item;
+    int n_items;
   };
   std::deque<Pending> pend;
   size_t cb = 0, pb = 0;
@@ -323,10 +327,12 @@ static void pb_schedule(int n_buckets, const int* op, const int* n_ct, const int
     const Pending q = pend.front();
     pend.pop_front();
     if (q.stage == PB_MODUP) {
-      for (int ti = level[q.b]; ti >= 0; --ti) jobs[pos++] = job(q.b, PB_MODUP, ti, q.item);  // special prime first
-      pend.push_back({pos + lag, q.b, PB_DOWN, q.item});
+      for (int ti = level[q.b]; ti >= 0; --ti)  // special prime first
+        for (int i = 0; i < q.n_items; ++i) jobs[pos++] = job(q.b, PB_MODUP, ti, q.item + i);
+      pend.push_back({pos + lag, q.b, PB_DOWN, q.item, q.n_items});
     } else {
-      for (int k = 0; k < 2; ++k) jobs[pos++] = job(q.b, PB_DOWN, k, q.item);
+      for (int k = 0; k < 2; ++k)
+        for (int i = 0; i < q.n_items; ++i) jobs[pos++] = job(q.b, PB_DOWN, k, q.item + i);
     }
   };
   while (pos < total) {
@@ -336,9 +342,11 @@ static void pb_schedule(int n_buckets, const int* op, const int* n_ct, const int
       emit_pending();
     } else if (cb < cm_order.size()) {
       const int b = cm_order[cb];
-      for (int j = 0; j < level[b]; ++j) jobs[pos++] = job(b, PB_TENSOR, j, ci);
-      pend.push_back({pos + lag, b, PB_MODUP, ci});
-      ++ci;
+      const int m = ci + 1 < n_ct[b] ? 2 : 1;
+      for (int j = 0; j < level[b]; ++j)
+        for (int i = 0; i < m; ++i) jobs[pos++] = job(b, PB_TENSOR, j, ci + i);
+      pend.push_back({pos + lag, b, PB_MODUP, ci, m});
+      ci += m;
     } else if (pb < pt_order.size()) {
       const int b = pt_order[pb];
       for (int k = 0; k < 2; ++k) jobs[pos++] = job(b, PB_CTPT, k, pi);

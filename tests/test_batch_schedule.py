@@ -108,8 +108,9 @@ def test_schedule_mixed_workload():
 def test_schedule_lag_extremes(lag, logs):
     _, _, gaps = _check([CT_CT, CT_PT, CT_CT], [5, 3, 4], [3, 2, 8], [1.0, 1.0, 2.0], lag, logs)
     if lag == 0:
-        # with no lag every pair's stages follow each other directly
-        assert max(gaps) == 0
+        # with no lag every pair's stages follow each other directly (pairs
+        # go in two at a time, interleaved: at most the partner's unit between)
+        assert max(gaps) <= 1
 
 
 def test_schedule_empty_and_refusals():
