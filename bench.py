@@ -292,9 +292,63 @@ def measure_transforms(ctx, dev, hbm_peak: float, reps: int = 20) -> dict:
     byts = 3 * 8 * n * (npoly // 2) * nl
     res["poly_mul"] = {"products_per_s": npoly // 2 * nl / s, "GBps": byts / s / 1e9,
                        "frac_hbm": byts / s / 1e9 / hbm_peak}
+    res["poly_mul_batch1"] = measure_poly_mul_batch1(ctx, dev)
     res["shape"] = f"N=2^{logn}, 45-bit primes, {npoly} polys x {nl} limbs per launch, 4 rotating buffers"
     res["linear_mlp"] = measure_linear(dev, reps=reps, hbm_peak=hbm_peak)
     return res
+
+
+def measure_poly_mul_batch1(ctx, dev, calls: int = 200) -> dict:
+    """Config 1 at its stated batch of 1: one negacyclic product NTT ->
+    pointwise modmul -> INTT of two polynomials (N = 2^12, the context's
+    first 45-bit prime).  device_us: one call alone (events around it, a
+    synchronize between calls, median); back_to_back_us: per call over
+    `calls` calls issued back to back (launch-bound); e2e_us: through the
+    drop-in golden API (`golden_bridge.poly_mult`: Python ints in, Python
+    ints out, copies included), median host time per call."""
+    import statistics
+    import time
+    import numpy as np
+    import torch
+    from ckks_b200 import golden_bridge as GB
+    n = ctx.n
+    q = int(ctx.primes[0])
+    rng = np.random.default_rng(1)
+    a = torch.from_numpy(rng.integers(0, q, n, dtype=np.uint64).view(np.int64)).to(dev).view(torch.uint64)
+    b = torch.from_numpy(rng.integers(0, q, n, dtype=np.uint64).view(np.int64)).to(dev).view(torch.uint64)
+    a, b = a.reshape(1, 1, n), b.reshape(1, 1, n)
+    out = torch.empty_like(a)
+    for _ in range(10):
+        _lib_call_poly_mul(ctx, out, a, b, 1)
+    torch.cuda.synchronize()
+    single = []
+    for _ in range(50):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        _lib_call_poly_mul(ctx, out, a, b, 1)
+        e1.record()
+        torch.cuda.synchronize()
+        single.append(e0.elapsed_time(e1) * 1000.0)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(calls):
+        _lib_call_poly_mul(ctx, out, a, b, 1)
+    e1.record()
+    torch.cuda.synchronize()
+    b2b = e0.elapsed_time(e1) * 1000.0 / calls
+    la = [int(v) for v in rng.integers(0, q, n, dtype=np.uint64)]
+    lb = [int(v) for v in rng.integers(0, q, n, dtype=np.uint64)]
+    GB.poly_mult(la, lb, q)
+    e2e = []
+    for _ in range(30):
+        t0 = time.perf_counter()
+        GB.poly_mult(la, lb, q)
+        e2e.append((time.perf_counter() - t0) * 1e6)
+    return {"device_us": statistics.median(single), "back_to_back_us": b2b,
+            "e2e_us": statistics.median(e2e), "q": q, "n": n,
+            "note": "batch 1: one product of two polynomials per call"}
 
 
 def measure_convgap(dev, hbm_peak: float, with_cpu: bool, reps: int = 20) -> dict:

@@ -34,6 +34,7 @@
 #include <mutex>
 
 #include "ctmul.hpp"
+#include "ctmul_modup_tm.cuh"
 #include "ctmul_units.cuh"
 #include "dispatch.cuh"
 #include "profile.hpp"
@@ -616,8 +617,18 @@ static int cm_launch_one(const ckks_ctx* ctx, uint64_t* out, const uint64_t* ct_
     {
       ProfSpan span(CKKS_STAGE_CM_MODUP, st);
       const long long nu_b = (long long)n_ct * (level + 1);
-      kb<<<grid1d((nu_b + upc - 1) / upc), Sh::T, smem_bc, st>>>(
-          S, reinterpret_cast<const double*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct, nu_b, upc);
+      bool tm = false;
+      if constexpr (ModupTm<L, K>::BUILT) {
+        if (ctx->tune_cm_tmem != 2) {
+          // accumulators in TMEM: the CTA needs only its transform buffer
+          k_cm_modup_tm<L, K><<<grid1d((nu_b + upc - 1) / upc), Sh::T, smem_a, st>>>(
+              S, reinterpret_cast<const double*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct, nu_b, upc);
+          tm = true;
+        }
+      }
+      if (!tm)
+        kb<<<grid1d((nu_b + upc - 1) / upc), Sh::T, smem_bc, st>>>(
+            S, reinterpret_cast<const double*>(key), level, ctx->n_q, ctx->d_pi, ctx->d_tw, n_ct, nu_b, upc);
     }
     if (int rc = ckks_check_launch(fn)) return rc;
     {

@@ -302,6 +302,11 @@ extern "C" int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value) {
                    "ckks_ctx_set_tuning: ct-mult path must be 0 (auto), 1 (fused) or 2 (three kernels)");
       ctx->tune_cm_fused = value;
       return CKKS_OK;
+    case CKKS_TUNE_CM_MODUP_TMEM:
+      CKKS_REQUIRE(value >= 0 && value <= 2,
+                   "ckks_ctx_set_tuning: ModUp accumulators must be 0 (auto), 1 (TMEM) or 2 (shared memory)");
+      ctx->tune_cm_tmem = value;
+      return CKKS_OK;
     case CKKS_TUNE_WAIT_CYCLES:
       CKKS_REQUIRE(value >= 0, "ckks_ctx_set_tuning: wait limit must be >= 0 SM cycles");
       ctx->tune_wait_cycles = value;

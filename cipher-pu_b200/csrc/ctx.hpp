@@ -24,6 +24,7 @@ struct ckks_ctx {
   int tune_cm_tma = 0;   // ct-mult tensor kernel: 1 = persistent TMA-fed, 2 = one CTA per unit (0 = default)
   int tune_wait_cycles = 0;  // limit of every bounded device wait, SM cycles (0 = default, ~1 s)
   int tune_cm_fused = 0;     // ct-mult: 0 = fused kernel where built, 1 = fused required, 2 = three kernels
+  int tune_cm_tmem = 0;      // ct-mult ModUp accumulators: 0 = default, 1 = TMEM where built, 2 = shared memory
   std::vector<u64> primes, psi, omega;
   std::vector<int> has_nega;
   std::vector<PrimeInfo> h_pi;

@@ -102,6 +102,12 @@ int ckks_ctx_destroy(ckks_ctx* ctx);
  *   work-queue flag); on expiry a kernel records it for ckks_device_status,
  *   lets its own copies in flight land and returns.  0 = default
  *   (2^31 - 1 cycles, about 1.1 s at 1965 MHz).
+ *   CKKS_TUNE_CM_MODUP_TMEM: where the three-kernel ct-mult's ModUp keeps
+ *   its key inner-product accumulators: 1 = Tensor Memory (the CTA then
+ *   needs only its transform buffer in shared memory and three 256-thread
+ *   CTAs share an SM; built for radix 2^4 at N = 2^12, where it measured
+ *   2.7-5.6 % faster), 2 = shared memory; 0 = default (TMEM where built).
+ *   Results are identical.
  *   CKKS_TUNE_NTT_LOG_ELEMS: K of ckks_ntt, ckks_ct_mul_plain_rescale and
  *   ckks_mul_plain_multi, in [2, 5] for log N in [6, 14] with
  *   N / 2^K <= 1024 (0 = default: min(4, log N)).
@@ -116,7 +122,8 @@ enum {
   CKKS_TUNE_CM_UNITS_PER_CTA = 4,
   CKKS_TUNE_CM_TENSOR_TMA = 5,
   CKKS_TUNE_WAIT_CYCLES = 6,
-  CKKS_TUNE_CM_FUSED = 7
+  CKKS_TUNE_CM_FUSED = 7,
+  CKKS_TUNE_CM_MODUP_TMEM = 8
 };
 int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value);
 

@@ -14,6 +14,7 @@ pytestmark = pytest.mark.gpu
 # ckks_ctx_set_tuning parameters
 CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC, CM_TMA = 0, 1, 2, 3, 4, 5
 CM_FUSED = 7  # 0 = fused kernel where built (default), 2 = the three-kernel path these shapes tune
+CM_TMEM = 8   # ModUp accumulators: 1 = TMEM (default where built: N = 2^12, K = 4), 2 = shared memory
 
 
 def _rand(rng, shape, basis):
@@ -32,7 +33,7 @@ def ck(cuda):
 
 
 def _reset(_lib, ctx):
-    for p in (CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC, CM_TMA, CM_FUSED):
+    for p in (CM_K, CM_MINB, CM_SPLIT, NTT_K, CM_UPC, CM_TMA, CM_FUSED, CM_TMEM):
         _lib.call("ckks_ctx_set_tuning", ctx.handle, p, 0)
 
 
@@ -259,3 +260,38 @@ def test_tma_tensor_kernel_identical(ck, log_n, n_ct, level):
     assert _lib.raw("ckks_device_status")() == 0
     sub = ksk[:level][:, :, list(range(level)) + [4]]
     assert np.array_equal(base[:1], R.ct_mul_relin_rescale(a[:1], b[:1], sub, qs[:level], P.special))
+
+
+@pytest.mark.parametrize("level,n_ct,upc", [(2, 33, 1), (3, 300, 1), (5, 17, 2), (8, 9, 4)])
+def test_modup_tmem_accumulators_identical(ck, level, n_ct, upc):
+    """The ModUp with its key inner-product accumulators in TMEM (three
+    256-thread CTAs per SM) against the shared-memory ModUp and the oracle at
+    N = 2^12: ragged batches, several levels, several units per CTA."""
+    ops, _lib, Context = ck
+    from ckks_b200.params import CkksParams
+    P = CkksParams.standard(12, 8)
+    ctx = Context.get(12, P.primes, n_special=1)
+    qs = list(P.q)
+    rng = np.random.default_rng(100 + level)
+    a = _rand(rng, (n_ct, 2, level, 4096), qs[:level])
+    b = _rand(rng, (n_ct, 2, level, 4096), qs[:level])
+    a[0, :, :, :] = np.asarray(qs[:level], dtype=np.uint64)[None, :, None] - 1
+    ksk = _rand(rng, (8, 2, 9, 4096), qs + [P.special])
+    key = ops.relin_key_prepare(ctx, ops.to_device(ksk))
+    da, db = ops.to_device(a), ops.to_device(b)
+    got = {}
+    try:
+        _three_kernels(_lib, ctx)
+        _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_UPC, upc)
+        for tm in (1, 2):
+            _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_TMEM, tm)
+            got[tm] = ops.to_host(ops.ct_mul_relin_rescale(ctx, da, db, key))
+    finally:
+        _reset(_lib, ctx)
+    assert np.array_equal(got[1], got[2])
+    sub = ksk[:level][:, :, list(range(level)) + [8]]
+    idx = [0, n_ct - 1]
+    assert np.array_equal(got[1][idx], R.ct_mul_relin_rescale(a[idx], b[idx], sub, qs[:level], P.special))
+    from ckks_b200._lib import CkksError
+    with pytest.raises(CkksError, match="ModUp accumulators"):
+        _lib.call("ckks_ctx_set_tuning", ctx.handle, CM_TMEM, 3)
