@@ -777,7 +777,9 @@ def run_ours(a) -> int:
         peak_src = "measured" if hbm else "fallback"
         hbm = hbm or 6650.0
         dom = max(STAGES, key=lambda s: stages[s][0])
-        names = STAGES
+        names = dict(STAGES)
+        if n == 4096:
+            names[1] = "k_cm_modup_tm"   # the ModUp with TMEM accumulators, the default at N = 2^12
         active = [s for s in STAGES if stages[s][1] > 0]
         per_launch_ms = stages[dom][0] / max(1, stages[dom][1])
         # a call may run its batch as concurrent sub-batches: pairs per launch
