@@ -309,7 +309,7 @@ class PlainController:
 class LearnedController:
     """Predict each gear's layer SNR from features; take the sparsest gear
     predicted >= target + margin.  The decrypt-based probe (the plain monitor)
-    stays as judge and fallback: it runs on the first use of a (layer, gear),
+    stays as arbiter and fallback: it runs on the first use of a (layer, gear),
     every `audit_every`-th batch, and whenever the prediction lies within
     `band_db` of the target; a measurement below the target caps the layer's
     gear and triggers the recompute."""

@@ -213,7 +213,7 @@ class EncryptedMLP:
         X: the batch already encrypted (else it is encrypted here).
         fallback_db: when a probe measures less than this at a gear > 0, the
         layer is recomputed at gear 0 before its result is used (the probe is
-        both the judge and the fallback trigger).
+        both the arbiter and the fallback trigger).
         Returns logits [B, O_last] (numpy), the probe records and the number of
         recomputed layers."""
         B = x.shape[0]

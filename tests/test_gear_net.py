@@ -157,7 +157,7 @@ def test_learned_controller_selects_sparse_gears_when_admissible(cuda):
 def test_learned_controller_falls_back_when_its_prediction_is_wrong(cuda):
     """A predictor that is wrong on purpose (every gear predicted at 120 dB):
     after calibration the controller runs gear 3, the first-use probe (the
-    plain monitor, judge of the learned one) measures the layer far below the
+    plain monitor, arbiter of the learned one) measures the layer far below the
     target, the layer is recomputed at gear 0 and its gear capped below the
     failed one; every later attempt is probed the same way (one gear lower
     each batch), so the stream still meets the target with the plaintext
