@@ -89,6 +89,15 @@ __device__ __forceinline__ bool tc_mbar_wait(uint32_t bar, uint32_t parity, long
 }
 constexpr long long kTcDrainCycles = 4000000000ll;
 
+// one bulk asynchronous copy global -> shared (16-byte aligned addresses, a
+// multiple of 16 bytes), completing as transaction bytes on `bar`
+__device__ __forceinline__ void tc_bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
 // shared-memory matrix descriptor: no swizzle, version 1 (sm_100)
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
@@ -153,17 +162,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   extern __shared__ __align__(1024) unsigned char smem[];
   __shared__ uint32_t tmem_slot;
   __shared__ __align__(8) unsigned long long bars[2];
+  __shared__ __align__(8) unsigned long long wbars[2];  // weight image of a stage landed
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int mt = blockIdx.y;
   const long long npos = (2ll * level) << log_n;
   const long long p0 = (long long)blockIdx.x * TC_N;
   const int nchunk = (n_in + TC_KC - 1) / TC_KC;
   const uint32_t bar[2] = {s_u32(&bars[0]), s_u32(&bars[1])};
+  const uint32_t wbar[2] = {s_u32(&wbars[0]), s_u32(&wbars[1])};
 
   if (warp == 0) tmem_alloc_warp(&tmem_slot, 512);
   if (tid == 32) {
     tc_mbar_init(bar[0]);
     tc_mbar_init(bar[1]);
+    tc_mbar_init(wbar[0]);
+    tc_mbar_init(wbar[1]);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   tmem_fence_before_sync();
@@ -173,6 +186,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
   // commits issued / waited for per stage (the k-th completion has parity k & 1)
   int n_commit[2] = {0, 0}, n_waited[2] = {0, 0};
+  // thread 0: a weight copy issued and not yet seen landed (stage, parity), or -1
+  int w_pending = -1;
   bool ok = true;
 #pragma unroll 1
   for (int kc = 0; kc < nchunk; ++kc) {
@@ -185,12 +200,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const bool need_wait = n_waited[s] < n_commit[s];
     bool expired = false;
     if (tid < TC_LOADERS && need_wait) expired = !tc_mbar_wait(bar[s], n_waited[s] & 1, wait_limit);
+    const uint32_t wpar = (uint32_t)(kc >> 1) & 1u;  // this stage's use number kc / 2, mod 2
     if (tid < TC_LOADERS && !expired) {
-      // weight limbs: the packed image of (tile mt, chunk kc), 16-byte copies
-      const uint4* wsrc = reinterpret_cast<const uint4*>(wpk + ((size_t)mt * nchunk + kc) * TC_WL * TC_A_IMG);
-      uint4 wv[TC_WL * TC_A_IMG / 16 / TC_LOADERS];
-  #pragma unroll
-      for (int i = 0; i < TC_WL * TC_A_IMG / 16 / TC_LOADERS; ++i) wv[i] = __ldg(wsrc + tid + i * TC_LOADERS);
+      // weight limbs: the packed image of (tile mt, chunk kc), already in the
+      // UMMA layout, as one bulk asynchronous copy (the stage is free: this
+      // thread has just seen its previous MMAs complete)
+      if (tid == 0) {
+        tc_bulk_load(s_u32(A), wpk + ((size_t)mt * nchunk + kc) * TC_WL * TC_A_IMG, TC_WL * TC_A_IMG, wbar[s]);
+        w_pending = s * 2 + (int)wpar;
+      }
       // residue limbs: 64 tasks (8 position x 8 feature groups), 4 per warp;
       // lane = 8 fq + pl takes position pb + pl and features fb + 4 fq .. + 3,
       // so a warp's 4-byte image stores hit 32 distinct banks.  Every load of
@@ -207,9 +225,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           xv[it][t] = (f + t < n_in) ? ld_stream(in + (size_t)(f + t) * npos + p0 + p) : 0ull;
       }
   #pragma unroll
-      for (int i = 0; i < TC_WL * TC_A_IMG / 16 / TC_LOADERS; ++i)
-        reinterpret_cast<uint4*>(A)[tid + i * TC_LOADERS] = wv[i];
-  #pragma unroll
       for (int it = 0; it < TPW; ++it) {
         const int task = warp * TPW + it;
         const int p = (task & 7) * 8 + (lane & 7);
@@ -222,6 +237,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         for (int a = 0; a < TC_XL; ++a) *reinterpret_cast<uint32_t*>(Bm + a * TC_B_IMG + off) = pl[a];
       }
     }
+    // the weight image has landed (bounded wait)
+    if (tid == 0 && w_pending >= 0) {
+      if (tc_mbar_wait(wbar[s], wpar, wait_limit)) w_pending = -1;
+      else expired = true;
+    }
     // make the generic-proxy stores visible to the tensor cores, then issue
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (__syncthreads_or(expired)) {
@@ -231,6 +251,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (need_wait) ++n_waited[s];
     if (tid == TC_ISSUER) {
       tmem_fence_after_sync();
+      // observe the weight copy's completion here too (already complete:
+      // thread 0 saw it before the barrier), ordering it before the MMAs
+      tc_mbar_wait(wbar[s], wpar, wait_limit);
       // descriptors of the stage's first operand rows; later ones differ only
       // in the start-address field (byte offset / 16, no carry below 256 KB)
       const uint64_t da = umma_desc(s_u32(A), 128, 8 * TC_KC);
@@ -263,6 +286,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (__syncthreads_or(!w)) ok = false;
     else ++n_waited[s];
   }
+  if (!ok && tid == 0 && w_pending >= 0 && !tc_mbar_wait(wbar[w_pending >> 1], w_pending & 1, kTcDrainCycles))
+    atomicAdd(&g_tc_wait_expiries, 1u);  // a weight copy still in flight after the drain limit
   if (!ok && tid == TC_ISSUER) {
     atomicAdd(&g_tc_wait_expiries, 1u);
     for (int st = 0; st < 2; ++st)
