@@ -283,6 +283,21 @@ def measure_transforms(ctx, dev, hbm_peak: float, reps: int = 20) -> dict:
         res["intt" if inv else "ntt"] = {
             "limb_transforms_per_s": npoly * nl / s, "GBps": byts / s / 1e9, "frac_hbm": byts / s / 1e9 / hbm_peak,
             "Gbutterfly_s": npoly * nl * (n // 2) * logn / s / 1e9}
+    if logn == 12:
+        # the same forward transform on the tensor cores (int8 byte-limb
+        # four-step, ckks_ntt_tc), with a bit-identity check against ckks_ntt
+        s = timed(lambda i: ops.ntt_tc(ctx, bufs[i % nbuf], n_limbs=nl))
+        byts = 2 * 8 * n * npoly * nl
+        a, b = bufs[0].clone(), bufs[0].clone()
+        ops.ntt(ctx, a, n_limbs=nl)
+        ops.ntt_tc(ctx, b, n_limbs=nl)
+        res["ntt_tc"] = {
+            "limb_transforms_per_s": npoly * nl / s, "GBps": byts / s / 1e9, "frac_hbm": byts / s / 1e9 / hbm_peak,
+            "vs_fp64_ntt": (npoly * nl / s) / res["ntt"]["limb_transforms_per_s"],
+            "bit_identical_to_ntt": bool(torch.equal(a, b)),
+            "int8_tops": npoly * nl * 2 * 36 * 64 ** 3 * 2 / s / 1e12,
+            "engine": "tcgen05.mma kind::i8, 64 x 64 four-step, 72 MMAs of 128x32x32 per step and polynomial"}
+        del a, b
     outs = [torch.empty((npoly // 2, nl, n), dtype=torch.uint64, device=dev) for _ in range(nbuf)]
 
     def pm(i):

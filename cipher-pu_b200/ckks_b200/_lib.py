@@ -40,6 +40,7 @@ SIGNATURES: dict[str, tuple] = {
     "ckks_ctx_set_tuning": (_i32, [_vp, _i32, _i32]),
     "ckks_device_status": (_i32, []),
     "ckks_ntt": (_i32, [_vp, _u64p, _i32, _i32, _i32, _i32, _i32, _vp]),
+    "ckks_ntt_tc": (_i32, [_vp, _u64p, _i32, _i32, _i32, _vp]),
     "ckks_bitrev_permute": (_i32, [_vp, _u64p, _u64p, _i32, _vp]),
     "ckks_pointwise_mul": (_i32, [_vp, _u64p, _u64p, _u64p, _i32, _i32, _i32, _vp]),
     "ckks_vec_addsub": (_i32, [_u64p, _u64p, _u64p, _i64, _u64, _i32, _vp]),

@@ -58,6 +58,14 @@ def ntt(ctx: Context, x: torch.Tensor, prime_begin: int = 0, inverse: bool = Fal
     return x
 
 
+def ntt_tc(ctx: Context, x: torch.Tensor, prime_begin: int = 0, n_limbs: int | None = None) -> torch.Tensor:
+    """In-place forward negacyclic NTT of x [..., n_limbs, N] on the tensor
+    cores (N = 2^12 only): the same results and order as ``ntt``."""
+    npoly, nl = _polys_limbs(x, ctx.n, n_limbs)
+    _lib.call("ckks_ntt_tc", ctx.handle, _p(x), npoly, prime_begin, nl, _stream())
+    return x
+
+
 def bitrev_permute(ctx: Context, x: torch.Tensor) -> torch.Tensor:
     out = torch.empty_like(x)
     _lib.call("ckks_bitrev_permute", ctx.handle, _p(out), _p(x), x.numel() // ctx.n, _stream())

@@ -372,9 +372,10 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T, MINB)
 // expiries of the tensor-core linear layer's waits (linear_tc.cu), read and cleared
 int ckks_linear_tc_status_take(unsigned int* n);
 int ckks_batch_status_take(unsigned int* n);
+int ckks_ntt_tc_status_take(unsigned int* n);
 
 extern "C" int ckks_device_status(void) {
-  unsigned int n = 0, n_tc = 0, n_pb = 0;
+  unsigned int n = 0, n_tc = 0, n_pb = 0, n_nt = 0;
   cudaError_t e = cudaMemcpyFromSymbol(&n, g_cm_wait_expiries, sizeof(n));
   if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "ckks_device_status: %s", cudaGetErrorString(e));
   if (n) {
@@ -384,8 +385,10 @@ extern "C" int ckks_device_status(void) {
   }
   if (int rc = ckks_linear_tc_status_take(&n_tc)) return rc;
   if (int rc = ckks_batch_status_take(&n_pb)) return rc;
-  if (n + n_tc + n_pb == 0) return CKKS_OK;
-  return ckks_set_error(CKKS_ETIMEOUT, "ckks_device_status: %u bounded device waits expired", n + n_tc + n_pb);
+  if (int rc = ckks_ntt_tc_status_take(&n_nt)) return rc;
+  const unsigned int total = n + n_tc + n_pb + n_nt;
+  if (total == 0) return CKKS_OK;
+  return ckks_set_error(CKKS_ETIMEOUT, "ckks_device_status: %u bounded device waits expired", total);
 }
 
 // ---------------------------------------------------------------- kernel B

@@ -117,6 +117,7 @@ static void free_ctx(ckks_ctx* c) {
   cudaFree(c->d_tw);
   cudaFree(c->d_pinv);
   cudaFree(c->d_qtinv);
+  cudaFree(c->d_ntt_tc);
   delete c;
 }
 

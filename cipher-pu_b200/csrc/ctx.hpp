@@ -33,6 +33,7 @@ struct ckks_ctx {
   TwPair* d_pinv = nullptr;   // [n_q]: special^-1 mod q_i (zeros when n_special == 0)
   TwPair* d_qtinv = nullptr;  // [n_q][n_q]: q_t^-1 mod q_i at [t][i], i < t
   TwPair* d_misc = nullptr;   // [n_primes][4]: (1, one_s) helpers; slot 1: R mod q
+  unsigned char* d_ntt_tc = nullptr;  // tensor-core transform tables (ntt_tc.cu), built on first use
   std::vector<std::vector<u64>> h_qtinv;  // host copies
   std::vector<u64> h_pinv;
 };

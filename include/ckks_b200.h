@@ -150,6 +150,20 @@ int ckks_device_status(void);
 int ckks_ntt(const ckks_ctx* ctx, uint64_t* data, int n_polys, int prime_begin, int n_limbs,
              int inverse, int cyclic, void* stream);
 
+/*
+ * The forward negacyclic NTT of ckks_ntt (same layout, output order and
+ * results) computed on the tensor cores: N = 2^12 as a 64 x 64 four-step
+ * transform whose two 64-point stages are int8 byte-limb matrix products
+ * (tcgen05.mma kind::i8), exact through an FP64 recombination.  N = 2^12
+ * contexts only; the first call builds the context's matrix images (about
+ * 112 KB per prime, device memory freed with the context) and should come
+ * before any stream capture.  The engine the task statement conditions
+ * tensor-core use on; ckks_ntt stays the default (it is faster).
+ * Replaces tb/ref/gen_ntt_reference.py:78 ntt (forward, with the
+ * negacyclic twist), like ckks_ntt.
+ */
+int ckks_ntt_tc(ckks_ctx* ctx, uint64_t* data, int n_polys, int prime_begin, int n_limbs, void* stream);
+
 /* out[row][i] = in[row][bitrev(i)] for n_rows rows of N words (out != in).
  * Converts between the bit-reversed evaluation order and the natural order
  * of tb/ref/gen_ntt_reference.py:78 ntt (natural-order output). */
