@@ -63,6 +63,11 @@ SIGNATURES: dict[str, tuple] = {
     "ckks_ct_mul_host48_workspace_bytes": (_sz, [_vp, _i32, _i32]),
     "ckks_ct_mul_relin_rescale_host48": (_i32, [_vp, _vp, _vp, _vp, _u64p, _i32, _i32, _i32, _vp, _sz,
                                                 _vp]),
+    "ckks_ct_mul_relin_rescale_host_async": (_i32, [_vp, _vp, _vp, _vp, _u64p, _i32, _i32, _i32, _vp, _sz,
+                                                    _vp]),
+    "ckks_ct_mul_relin_rescale_host48_async": (_i32, [_vp, _vp, _vp, _vp, _u64p, _i32, _i32, _i32, _vp,
+                                                      _sz, _vp]),
+    "ckks_ct_mul_host_join": (_i32, [_vp]),
     "ckks_ct_mul_relin_rescale_noalloc": (_i32, [_vp, _u64p, _u64p, _u64p, _u64p, _i32, _i32, _vp]),
     "ckks_encode": (_i32, [_vp, _u64p, _vp, _i32, _i32, _i32, C.c_double, _vp]),
     "ckks_decode": (_i32, [_vp, _vp, _u64p, _i32, _i32, _i32, C.c_double, _vp]),

@@ -289,6 +289,32 @@ def ct_mul_relin_rescale_host48(ctx: Context, a48: torch.Tensor, b48: torch.Tens
     return out48
 
 
+def ct_mul_relin_rescale_host_async(ctx: Context, ct_a: torch.Tensor, ct_b: torch.Tensor,
+                                    key_prepared: torch.Tensor, out: torch.Tensor, chunk: int,
+                                    workspace: torch.Tensor) -> torch.Tensor:
+    """Stream-ordered form of ``ct_mul_relin_rescale_host``: enqueues the
+    pipeline and returns at once; ``ct_mul_host_join()`` then orders the
+    current stream after every call enqueued so far (synchronise it before
+    reading ``out``).  Host tensors and the workspace must stay untouched
+    until then."""
+    if ct_a.is_cuda or ct_b.is_cuda or out.is_cuda:
+        raise ValueError("ct_mul_relin_rescale_host_async takes host tensors")
+    if not (ct_a.is_contiguous() and ct_b.is_contiguous() and out.is_contiguous()):
+        raise ValueError("expected contiguous host tensors")
+    if ct_a.dtype != U64 or ct_b.dtype != U64 or out.dtype != U64:
+        raise ValueError("expected uint64 host tensors")
+    n_ct, two, level, n = ct_a.shape
+    _lib.call("ckks_ct_mul_relin_rescale_host_async", ctx.handle, out.data_ptr(), ct_a.data_ptr(),
+              ct_b.data_ptr(), _p(key_prepared), n_ct, level, chunk, _p(workspace),
+              workspace.numel() * workspace.element_size(), _stream())
+    return out
+
+
+def ct_mul_host_join() -> None:
+    """Order the current stream after every async host-buffer ct-mult enqueued so far."""
+    _lib.call("ckks_ct_mul_host_join", _stream())
+
+
 # ------------------------------------------------------------------ encode / decode
 def _f64(t: torch.Tensor) -> int:
     if not t.is_cuda or t.dtype not in (torch.float64, torch.complex128) or not t.is_contiguous():

@@ -2,7 +2,8 @@
 // call a binding makes when its ciphertexts live in host memory (numpy arrays
 // behind ctypes, a JVM direct buffer, a cgo slice).
 //
-// The batch is cut into chunks; chunk i runs on pipeline stream i mod 3 as
+// The batch is cut into chunks; chunk i runs on pipeline stream i mod 3 (the
+// rotation continues from the previous call's last stream) as
 // H2D(a, b) -> the three ct-mult kernels -> D2H(out), so the host->device copy
 // of one chunk, the kernels of the previous one and the device->host copy of
 // the one before that overlap (B200 has separate copy engines per direction).
@@ -12,6 +13,14 @@
 // in host memory.  Host buffers should be page-locked (cudaHostAlloc /
 // torch pin_memory) for the copies to run asynchronously; pageable buffers
 // give the same results with serialised copies.
+//
+// The _async entries enqueue the same pipeline and return at once; a later
+// ckks_ct_mul_host_join(stream) makes the caller's stream wait for every
+// chunk enqueued so far.  Back-to-back async calls keep the host->device copy
+// engine busy across calls: the next call's first input copies run while the
+// previous call's last chunks compute and copy back, which the blocking call
+// cannot do (it drains the pipeline before returning).
+#include <atomic>
 #include <mutex>
 
 #include "ctmul.hpp"
@@ -28,6 +37,8 @@ struct Pipe {
   bool ready = false;
   cudaStream_t s[kPipe];
   cudaEvent_t start;
+  cudaEvent_t done[kPipe];        // join points of the pipeline streams
+  std::atomic<unsigned> next{0};  // stream of the next chunk: the rotation continues across calls
 };
 
 std::mutex g_pipe_mu;
@@ -47,6 +58,7 @@ int pipe_for_device(Pipe** out, const char* fn) {
     for (int i = 0; i < kPipe && e == cudaSuccess; ++i)
       e = cudaStreamCreateWithFlags(&p.s[i], cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&p.start, cudaEventDisableTiming);
+    for (int i = 0; i < kPipe && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&p.done[i], cudaEventDisableTiming);
     if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
     p.ready = true;
   }
@@ -86,7 +98,7 @@ extern "C" size_t ckks_ct_mul_host48_workspace_bytes(const ckks_ctx* ctx, int ch
 
 static int host_pipeline(const ckks_ctx* ctx, void* out_host, const void* a_host, const void* b_host,
                          const uint64_t* key, int n_ct, int level, int chunk, void* workspace,
-                         size_t workspace_bytes, void* stream, bool packed, const char* fn) {
+                         size_t workspace_bytes, void* stream, bool packed, bool wait, const char* fn) {
   CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
   CKKS_REQUIRE(n_ct >= 0, "%s: n_ct < 0", fn);
   CKKS_REQUIRE(chunk >= 1, "%s: chunk=%d must be >= 1", fn, chunk);
@@ -112,10 +124,16 @@ static int host_pipeline(const ckks_ctx* ctx, void* out_host, const void* a_host
   const unsigned char* bh = reinterpret_cast<const unsigned char*>(b_host);
   unsigned char* oh = reinterpret_cast<unsigned char*>(out_host);
   int rc = CKKS_OK;
+  // chunk i of this call runs on stream (first + i) mod 3 with that stream's
+  // workspace slot, so back-to-back stream-ordered calls spread over all three
+  // streams even when a call has fewer chunks than streams
+  const unsigned n_chunks = (unsigned)((n_ct + chunk - 1) / chunk);
+  const unsigned first = p->next.fetch_add(n_chunks) % kPipe;
   for (int c0 = 0, i = 0; c0 < n_ct && rc == CKKS_OK; c0 += chunk, ++i) {
     const int m = n_ct - c0 < chunk ? n_ct - c0 : chunk;
-    cudaStream_t st = p->s[i % kPipe];
-    unsigned char* base = reinterpret_cast<unsigned char*>(workspace) + (size_t)(i % kPipe) * sl.total_bytes;
+    const unsigned si = (first + (unsigned)i) % kPipe;
+    cudaStream_t st = p->s[si];
+    unsigned char* base = reinterpret_cast<unsigned char*>(workspace) + (size_t)si * sl.total_bytes;
     uint64_t* da = reinterpret_cast<uint64_t*>(base);
     uint64_t* db = da + sl.a_words;
     uint64_t* dout = db + sl.a_words;
@@ -148,7 +166,7 @@ static int host_pipeline(const ckks_ctx* ctx, void* out_host, const void* a_host
     e = cudaMemcpyAsync(oh + (size_t)c0 * out_ct * wb, so, out_words * wb, cudaMemcpyDeviceToHost, st);
     if (e != cudaSuccess) rc = ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
   }
-  for (int i = 0; i < kPipe; ++i) {
+  for (int i = 0; wait && i < kPipe; ++i) {
     const cudaError_t es = cudaStreamSynchronize(p->s[i]);
     if (es != cudaSuccess && rc == CKKS_OK)
       rc = ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(es));
@@ -162,7 +180,7 @@ extern "C" int ckks_ct_mul_relin_rescale_host(const ckks_ctx* ctx, uint64_t* out
                                               void* workspace, size_t workspace_bytes,
                                               void* stream) {
   return host_pipeline(ctx, out_host, a_host, b_host, key, n_ct, level, chunk, workspace, workspace_bytes,
-                       stream, false, "ckks_ct_mul_relin_rescale_host");
+                       stream, false, true, "ckks_ct_mul_relin_rescale_host");
 }
 
 extern "C" int ckks_ct_mul_relin_rescale_host48(const ckks_ctx* ctx, void* out_host, const void* a_host,
@@ -170,5 +188,34 @@ extern "C" int ckks_ct_mul_relin_rescale_host48(const ckks_ctx* ctx, void* out_h
                                                 int level, int chunk, void* workspace,
                                                 size_t workspace_bytes, void* stream) {
   return host_pipeline(ctx, out_host, a_host, b_host, key, n_ct, level, chunk, workspace, workspace_bytes,
-                       stream, true, "ckks_ct_mul_relin_rescale_host48");
+                       stream, true, true, "ckks_ct_mul_relin_rescale_host48");
+}
+
+extern "C" int ckks_ct_mul_relin_rescale_host_async(const ckks_ctx* ctx, uint64_t* out_host,
+                                                    const uint64_t* a_host, const uint64_t* b_host,
+                                                    const uint64_t* key, int n_ct, int level, int chunk,
+                                                    void* workspace, size_t workspace_bytes, void* stream) {
+  return host_pipeline(ctx, out_host, a_host, b_host, key, n_ct, level, chunk, workspace, workspace_bytes,
+                       stream, false, false, "ckks_ct_mul_relin_rescale_host_async");
+}
+
+extern "C" int ckks_ct_mul_relin_rescale_host48_async(const ckks_ctx* ctx, void* out_host, const void* a_host,
+                                                      const void* b_host, const uint64_t* key, int n_ct,
+                                                      int level, int chunk, void* workspace,
+                                                      size_t workspace_bytes, void* stream) {
+  return host_pipeline(ctx, out_host, a_host, b_host, key, n_ct, level, chunk, workspace, workspace_bytes,
+                       stream, true, false, "ckks_ct_mul_relin_rescale_host48_async");
+}
+
+extern "C" int ckks_ct_mul_host_join(void* stream) {
+  const char* fn = "ckks_ct_mul_host_join";
+  Pipe* p = nullptr;
+  if (int rc = pipe_for_device(&p, fn)) return rc;
+  cudaError_t e = cudaSuccess;
+  for (int i = 0; i < kPipe && e == cudaSuccess; ++i) {
+    e = cudaEventRecord(p->done[i], p->s[i]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(as_stream(stream), p->done[i], 0);
+  }
+  if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
+  return CKKS_OK;
 }

@@ -648,6 +648,27 @@ int ckks_ct_mul_relin_rescale_host48(const ckks_ctx* ctx, void* out_host, const 
                                      const void* b_host, const uint64_t* key, int n_ct, int level,
                                      int chunk, void* workspace, size_t workspace_bytes, void* stream);
 
+/*
+ * Stream-ordered forms of the two host-buffer calls above: the same chunked
+ * H2D -> kernels -> D2H pipeline is enqueued (after the work already queued
+ * on `stream`) and the call returns without waiting.  ckks_ct_mul_host_join
+ * (stream) then makes `stream` wait for every chunk enqueued so far on the
+ * current device; the outputs are in host memory once `stream` has reached
+ * that point (cudaStreamSynchronize).  Host buffers and the workspace must
+ * stay valid and unmodified until then; consecutive calls may share one
+ * workspace (its slots are reused in stream order).  Back-to-back calls
+ * overlap: the next call's input copies run while the previous call's last
+ * chunks compute and copy back.  Like the blocking calls, they replace the
+ * host side of scripts/verify_e2e_mult.py:78 e2e_mult for batches.
+ */
+int ckks_ct_mul_relin_rescale_host_async(const ckks_ctx* ctx, uint64_t* out_host, const uint64_t* a_host,
+                                         const uint64_t* b_host, const uint64_t* key, int n_ct, int level,
+                                         int chunk, void* workspace, size_t workspace_bytes, void* stream);
+int ckks_ct_mul_relin_rescale_host48_async(const ckks_ctx* ctx, void* out_host, const void* a_host,
+                                           const void* b_host, const uint64_t* key, int n_ct, int level,
+                                           int chunk, void* workspace, size_t workspace_bytes, void* stream);
+int ckks_ct_mul_host_join(void* stream);
+
 /* Size of the static device scratch used by ckks_ct_mul_relin_rescale_noalloc. */
 #define CKKS_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 
