@@ -29,6 +29,7 @@ class BatchBucket(C.Structure):
 
 BATCH_CT_CT, BATCH_CT_PT = 0, 1
 BATCH_RUN_UNMET_WAIT = 1
+BATCH_RUN_PHASED = 2
 
 # name -> (restype, argtypes); must mirror include/ckks_b200.h
 SIGNATURES: dict[str, tuple] = {
@@ -118,6 +119,8 @@ SIGNATURES: dict[str, tuple] = {
                                      C.POINTER(_i32), C.POINTER(_sz)]),
     "ckks_batch_plan_destroy": (None, [_vp]),
     "ckks_batch_schedule": (_i32, [_i32, _vp, _vp, _vp, _vp, _vp, C.c_longlong, _vp, C.POINTER(C.c_longlong)]),
+    "ckks_batch_schedule_phased": (_i32, [_i32, _vp, _vp, _vp, _vp, _vp, C.c_longlong, _vp,
+                                          C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]),
     "ckks_profile_enable": (_i32, [_i32]),
     "ckks_profile_reset": (_i32, []),
     "ckks_profile_read": (_i32, [_i32, C.POINTER(C.c_double), C.POINTER(C.c_longlong)]),

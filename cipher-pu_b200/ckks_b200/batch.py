@@ -108,9 +108,15 @@ class PersistentPlan:
         self.handle = h
         self.buckets = buckets
         self.lag_percent = lag_percent
+        # True: the paired list (the default: N = 2^12 units two per slot);
+        # False: the phased list (N = 2^13 whole-CTA slots, then N = 2^12 units
+        # taken by each half on its own)
+        self.paired = True
 
     def run(self, wait_cycles: int = 0, flags: int = 0, stream=None):
         st = (stream or torch.cuda.current_stream()).cuda_stream
+        if not self.paired:
+            flags |= _lib.BATCH_RUN_PHASED
         _lib.call("ckks_batch_plan_run", self.handle, int(wait_cycles), int(flags), st)
 
     def incomplete(self) -> tuple[int, list]:
@@ -126,7 +132,8 @@ class PersistentPlan:
         _lib.call("ckks_batch_plan_info", self.handle, ctypes.byref(nu), ctypes.byref(ns), ctypes.byref(grid),
                   ctypes.byref(smem), ctypes.byref(nb))
         return {"units": nu.value, "slots": ns.value, "grid": grid.value, "smem_bytes": smem.value,
-                "device_bytes": nb.value, "lag_percent": self.lag_percent}
+                "device_bytes": nb.value, "lag_percent": self.lag_percent,
+                "list": "paired" if self.paired else "phased"}
 
     def close(self):
         if self.handle:
@@ -327,26 +334,33 @@ class BatchExecutor:
 
     def autotune_persistent(self, reps: int = 3, lags=(200, 400, 800)) -> dict:
         """Time the persistent plan under each lag (how far a dependent stage
-        is listed after its producers, in % of a wave); keep the fastest."""
+        is listed after its producers, in % of a wave) and both of its unit
+        lists (phased, paired); keep the fastest."""
         sweep = {}
         best = None
         for lag in lags:
             plan = PersistentPlan(self.evs, self.buckets, lag)
-            plan.run()
-            torch.cuda.synchronize()
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            for _ in range(reps):
+            keep = False
+            for paired in (True, False):
+                plan.paired = paired
                 plan.run()
-            e1.record()
-            torch.cuda.synchronize()
-            t = e0.elapsed_time(e1) / reps
-            sweep[f"lag{lag}"] = round(t, 4)
-            if best is None or t < best[0]:
-                if best is not None:
-                    best[1].close()
-                best = (t, plan)
+                torch.cuda.synchronize()
+                e0 = torch.cuda.Event(enable_timing=True)
+                e1 = torch.cuda.Event(enable_timing=True)
+                e0.record()
+                for _ in range(reps):
+                    plan.run()
+                e1.record()
+                torch.cuda.synchronize()
+                t = e0.elapsed_time(e1) / reps
+                sweep[f"{'paired' if paired else 'phased'}/lag{lag}"] = round(t, 4)
+                if best is None or t < best[0]:
+                    if best is not None and best[1] is not plan:
+                        best[1].close()
+                    best = (t, plan, paired)
+                    keep = True
+            if keep:
+                plan.paired = best[2]
             else:
                 plan.close()
         if self.plan is not None:

@@ -16,7 +16,13 @@
 // halves of the CTA on their own named barriers and shared-memory halves, as
 // two CTAs of the per-shape kernels share an SM).  CTAs take slots in list
 // order from one atomic ticket (the next ticket is fetched while the current
-// slot runs).
+// slot runs).  That paired list couples the halves: both must finish before
+// the CTA takes its next slot.  The phased list (an option) avoids it: the
+// N = 2^13 units come first, one per whole-CTA slot; then every N = 2^12
+// unit is a half slot of its own, and each half of each CTA takes half slots
+// from a second ticket as soon as its previous unit is done.  Each ring
+// size is scheduled on its own (no item spans both), so the dependency and
+// no-deadlock arguments below hold in each phase.
 //
 // Dependencies are per-item counters: a tensor unit adds 1 to its pair's
 // counter when its stores are done (every thread fences, the CTA syncs, one
@@ -180,8 +186,13 @@ __device__ __forceinline__ void pb_unit(const PbTable& tab, PbJob jb, u64* sm, i
   }
 }
 
-// ctl[0..1]: the 64-bit ticket, ctl[2]: the abort flag (zeroed before every
-// launch).
+// ctl[0..1]: the 64-bit ticket of the whole-CTA slots, ctl[2]: the abort
+// flag, ctl[4..5]: the 64-bit ticket of the half slots (all zeroed before
+// every launch).
+// slots[0, n_slots): whole-CTA slots (one N = 2^13 unit, or in the paired
+// list two N = 2^12 units side by side); slots[n_slots, n_slots + n_half):
+// half slots, one N = 2^12 unit each, which each 256-thread half of every CTA
+// takes from its own ticket once the CTA has run out of whole-CTA slots.
 // unmet_bucket >= 0 is a test hook: the ModUp units of item 0 of that
 // bucket wait for one tensor unit more than exist, so their wait can only
 // end by its limit.
@@ -221,6 +232,52 @@ __global__ void __launch_bounds__(PB_THREADS, 1)
   }
 }
 
+// The phased list: slots[0, n_whole) are N = 2^13 units, one per whole-CTA
+// slot; slots[n_whole, n_whole + n_half) are N = 2^12 units, which each
+// 256-thread half takes from the second ticket (ctl[4..5]) on its own once
+// the CTA has run out of whole-CTA slots (its own named barrier and
+// shared-memory half from then on).  One call site per unit shape.
+template <int MAXLOGN>
+__global__ void __launch_bounds__(PB_THREADS, 1)
+    k_batch_phased(const __grid_constant__ PbTable tab, const PbSlot* __restrict__ slots, long long n_whole,
+                   long long n_half, unsigned* ctl, long long wait_limit, int unmet_bucket) {
+  extern __shared__ u64 sm[];
+  __shared__ long long s_whole;     // phase 1 ticket (whole CTA)
+  __shared__ long long s_half[2];   // phase 2 tickets (one per half)
+  __shared__ int s_ok[2];
+  const int tid = threadIdx.x;
+  if constexpr (MAXLOGN >= 13) {
+    unsigned long long next = 0;
+    if (tid == 0 && n_whole > 0) next = atomicAdd(reinterpret_cast<unsigned long long*>(ctl), 1ull);
+    for (;;) {
+      if (tid == 0) {
+        const unsigned long long t = next;
+        const bool go = n_whole > 0 && (long long)t < n_whole && !ld_volatile_u32(ctl + 2);
+        if (go) next = atomicAdd(reinterpret_cast<unsigned long long*>(ctl), 1ull);
+        s_whole = go ? (long long)t : -1;
+      }
+      __syncthreads();
+      const long long t = s_whole;
+      if (t < 0) break;
+      pb_unit<13, 4>(tab, slots[t].u[0], sm, tid, 0, ctl, wait_limit, unmet_bucket, s_ok);
+      __syncthreads();  // the CTA's shared memory is free for the next unit
+    }
+  }
+  const int h = tid / PB_HALF, ht = tid % PB_HALF;  // h is uniform within each half
+  for (;;) {
+    if (ht == 0) {
+      const bool live = !ld_volatile_u32(ctl + 2);
+      const unsigned long long t = live ? atomicAdd(reinterpret_cast<unsigned long long*>(ctl + 4), 1ull) : 0ull;
+      s_half[h] = live && (long long)t < n_half ? (long long)t : -1;
+    }
+    group_sync<PB_HALF>();
+    const long long t = s_half[h];
+    if (t < 0) return;
+    pb_unit<12, 4>(tab, slots[n_whole + t].u[0], sm + h * PB_SM12_WORDS, ht, h, ctl, wait_limit, unmet_bucket, s_ok);
+    group_sync<PB_HALF>();  // the half's shared memory and ticket word are free again
+  }
+}
+
 // Expiries of the persistent batch kernel's waits, read and cleared by
 // ckks_device_status.
 int ckks_batch_status_take(unsigned* n) {
@@ -241,7 +298,9 @@ struct ckks_batch_plan {
   int grid = 0;
   int smem = 0;
   long long n_units = 0;
-  long long n_slots = 0;
+  long long n_slots = 0;   // paired list (the default): whole-CTA slots
+  long long n_whole = 0;   // phased list: N = 2^13 whole-CTA slots, then
+  long long n_half = 0;    // N = 2^12 half slots (stored after the paired list)
   int n_buckets = 0;
   unsigned char* mem = nullptr;  // one device allocation
   size_t mem_bytes = 0;
@@ -258,28 +317,40 @@ struct ckks_batch_plan {
 namespace {
 
 template <int MAXLOGN>
-int pb_launch(ckks_batch_plan* p, long long wait_limit, int unmet_bucket, cudaStream_t st) {
-  k_batch_persistent<MAXLOGN><<<p->grid, PB_THREADS, p->smem, st>>>(*p->table, p->d_slots, p->n_slots, p->ctl,
-                                                                   wait_limit, unmet_bucket);
+int pb_launch(ckks_batch_plan* p, bool paired, long long wait_limit, int unmet_bucket, cudaStream_t st) {
+  if (paired)
+    k_batch_persistent<MAXLOGN><<<p->grid, PB_THREADS, p->smem, st>>>(*p->table, p->d_slots, p->n_slots, p->ctl,
+                                                                     wait_limit, unmet_bucket);
+  else
+    k_batch_phased<MAXLOGN><<<p->grid, PB_THREADS, p->smem, st>>>(
+        *p->table, p->d_slots + p->n_slots, p->n_whole, p->n_half, p->ctl, wait_limit, unmet_bucket);
   return ckks_check_launch("ckks_batch_plan_run");
+}
+
+template <typename KernelT>
+cudaError_t pb_raise_smem(KernelT k, int smem) {
+  // raise the kernel's dynamic shared-memory cap, never lower it: plans of
+  // other shapes may launch the same kernel with more
+  cudaFuncAttributes fa{};
+  cudaError_t e = cudaFuncGetAttributes(&fa, k);
+  if (e == cudaSuccess && smem > fa.maxDynamicSharedSizeBytes)
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  return e;
 }
 
 template <int MAXLOGN>
 int pb_configure(ckks_batch_plan* p, const char* fn) {
   auto k = k_batch_persistent<MAXLOGN>;
-  // raise the kernel's dynamic shared-memory cap, never lower it: plans of
-  // other shapes may launch the same kernel with more
-  cudaFuncAttributes fa{};
-  cudaError_t e0 = cudaFuncGetAttributes(&fa, k);
+  auto kp = k_batch_phased<MAXLOGN>;
+  cudaError_t e0 = pb_raise_smem(k, p->smem);
+  if (e0 == cudaSuccess) e0 = pb_raise_smem(kp, p->smem);
   if (e0 != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e0));
-  if (p->smem > fa.maxDynamicSharedSizeBytes) {
-    e0 = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, p->smem);
-    if (e0 != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e0));
-  }
-  int per_sm = 0, n_sm = 0;
+  int per_sm = 0, per_sm_p = 0, n_sm = 0;
   cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, p->device);
   cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, PB_THREADS, p->smem);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_p, kp, PB_THREADS, p->smem);
   if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
+  per_sm = std::min(per_sm, per_sm_p);
   if (per_sm < 1)
     return ckks_set_error(CKKS_EUNSUPPORTED, "%s: the persistent kernel does not fit on an SM with %d B of shared memory",
                           fn, p->smem);
@@ -378,6 +449,30 @@ static long long pb_slots(const PbJob* jobs, long long n_units, const int* log_n
   return ns;
 }
 
+// The phased list: the N = 2^13 buckets scheduled alone, one unit per
+// whole-CTA slot, then the N = 2^12 buckets scheduled alone, one unit per
+// half slot (u[1] = none).  Returns the whole-CTA slot count; *n_half gets
+// the half-slot count.  slots must hold every unit.
+static long long pb_phased(int n_buckets, const int* op, const int* n_ct, const int* level, const int* log_n,
+                           const double* cost, long long lag_whole, long long lag_half, PbSlot* slots,
+                           long long* n_half) {
+  std::vector<int> c13(n_buckets), c12(n_buckets);
+  long long t13 = 0, t12 = 0;
+  for (int b = 0; b < n_buckets; ++b) {
+    const long long u = (long long)n_ct[b] * (op[b] == CKKS_BATCH_CT_CT ? 2 * level[b] + 3 : 2);
+    c13[b] = log_n[b] == 13 ? n_ct[b] : 0;
+    c12[b] = log_n[b] == 13 ? 0 : n_ct[b];
+    (log_n[b] == 13 ? t13 : t12) += u;
+  }
+  std::vector<PbJob> jobs((size_t)std::max(t13, t12));
+  pb_schedule(n_buckets, op, c13.data(), level, cost, lag_whole, jobs.data());
+  for (long long i = 0; i < t13; ++i) slots[i] = PbSlot{{jobs[i], PbJob{PB_NONE, 0}}};
+  pb_schedule(n_buckets, op, c12.data(), level, cost, lag_half, jobs.data());
+  for (long long i = 0; i < t12; ++i) slots[t13 + i] = PbSlot{{jobs[i], PbJob{PB_NONE, 0}}};
+  *n_half = t12;
+  return t13;
+}
+
 // The work list on the host alone (no device, no context): slots gets 4 x
 // uint32 per slot, two units (bucket << 8 | stage << 6 | sub, item) with
 // stage 0 tensor, 1 ModUp, 2 ModDown, 3 ct x pt, the second 0xFFFFFFFF, 0 in
@@ -406,6 +501,36 @@ extern "C" int ckks_batch_schedule(int n_buckets, const int* op, const int* n_ct
   std::vector<PbJob> jobs((size_t)total);
   pb_schedule(n_buckets, op, n_ct, level, cost, lag, jobs.data());
   *n_slots = pb_slots(jobs.data(), total, log_n, reinterpret_cast<PbSlot*>(slots));
+  return CKKS_OK;
+}
+
+// The phased list on the host alone: *n_whole whole-CTA slots (one
+// N = 2^13 unit each, dependent stages lag units apart), then the half slots
+// (one N = 2^12 unit each, 2 lag units apart: two halves per CTA); the slot
+// format of ckks_batch_schedule, every second unit (0xFFFFFFFF, 0).
+extern "C" int ckks_batch_schedule_phased(int n_buckets, const int* op, const int* n_ct, const int* level,
+                                          const int* log_n, const double* cost, long long lag, uint32_t* slots,
+                                          long long* n_slots, long long* n_whole) {
+  const char* fn = "ckks_batch_schedule_phased";
+  CKKS_REQUIRE(n_slots != nullptr && n_whole != nullptr, "%s: NULL count argument", fn);
+  CKKS_REQUIRE(n_buckets >= 0 && n_buckets <= PB_MAX_BUCKETS, "%s: n_buckets=%d outside [0, %d]", fn, n_buckets,
+               PB_MAX_BUCKETS);
+  CKKS_REQUIRE(n_buckets == 0 || (op && n_ct && level && log_n && cost), "%s: NULL pointer argument", fn);
+  CKKS_REQUIRE(lag >= 0, "%s: lag < 0", fn);
+  long long total = 0;
+  for (int b = 0; b < n_buckets; ++b) {
+    CKKS_REQUIRE(op[b] == CKKS_BATCH_CT_CT || op[b] == CKKS_BATCH_CT_PT, "%s: bucket %d: op=%d", fn, b, op[b]);
+    CKKS_REQUIRE(n_ct[b] >= 0 && level[b] >= 2 && level[b] <= 62, "%s: bucket %d: n_ct=%d level=%d", fn, b, n_ct[b],
+                 level[b]);
+    CKKS_REQUIRE(log_n[b] == 12 || log_n[b] == 13, "%s: bucket %d: log_n=%d (12 or 13)", fn, b, log_n[b]);
+    total += (long long)n_ct[b] * (op[b] == CKKS_BATCH_CT_CT ? 2 * level[b] + 3 : 2);
+  }
+  CKKS_REQUIRE(slots != nullptr || total == 0, "%s: slots is NULL", fn);
+  CKKS_REQUIRE(*n_slots >= total, "%s: capacity %lld < %lld units", fn, *n_slots, total);
+  long long n_half = 0;
+  *n_whole = pb_phased(n_buckets, op, n_ct, level, log_n, cost, lag, 2 * lag, reinterpret_cast<PbSlot*>(slots),
+                       &n_half);
+  *n_slots = *n_whole + n_half;
   return CKKS_OK;
 }
 
@@ -498,7 +623,7 @@ extern "C" int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_bu
   const size_t off_cnt = 256;
   p->zero_bytes = align256(off_cnt + n_cnt * sizeof(unsigned));
   const size_t off_slots = p->zero_bytes;
-  const size_t off_scr = align256(off_slots + (size_t)n_units * sizeof(PbSlot));
+  const size_t off_scr = align256(off_slots + 2 * (size_t)n_units * sizeof(PbSlot));  // both lists
   p->mem_bytes = off_scr + scratch_words * sizeof(u64);
   cudaError_t e = cudaMalloc(&p->mem, p->mem_bytes);
   if (e != cudaSuccess) {
@@ -550,16 +675,22 @@ extern "C" int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_bu
     logs[b] = buckets[b].ctx->log_n;
     costs[b] = (double)buckets[b].ctx->n * (2 * buckets[b].level + 3);
   }
-  // a wave: every CTA on one slot, two units each (N = 2^12)
+  // paired list (a wave: every CTA on one slot, two units each at N = 2^12)
   std::vector<PbJob> jobs((size_t)n_units);
   pb_schedule(n_buckets, ops.data(), cts.data(), lvls.data(), costs.data(),
               (long long)p->grid * 2 * lag_percent / 100, jobs.data());
-  std::vector<PbSlot> slots((size_t)n_units);
+  std::vector<PbSlot> slots(2 * (size_t)n_units);
   p->n_slots = pb_slots(jobs.data(), n_units, logs.data(), slots.data());
+  // phased list, stored after it (a wave: one N = 2^13 unit per CTA, then
+  // one N = 2^12 unit per half)
+  p->n_whole = pb_phased(n_buckets, ops.data(), cts.data(), lvls.data(), logs.data(), costs.data(),
+                         (long long)p->grid * lag_percent / 100, (long long)p->grid * 2 * lag_percent / 100,
+                         slots.data() + p->n_slots, &p->n_half);
   p->table = new PbTable();
   for (int b = 0; b < n_buckets; ++b) p->table->b[b] = p->h_buckets[b];
-  if (p->n_slots)
-    e = cudaMemcpy(p->d_slots, slots.data(), (size_t)p->n_slots * sizeof(PbSlot), cudaMemcpyHostToDevice);
+  const long long n_all = p->n_slots + p->n_whole + p->n_half;
+  if (n_all)
+    e = cudaMemcpy(p->d_slots, slots.data(), (size_t)n_all * sizeof(PbSlot), cudaMemcpyHostToDevice);
   if (e != cudaSuccess) return fail(ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e)));
   *out = p;
   return CKKS_OK;
@@ -568,14 +699,15 @@ extern "C" int ckks_batch_plan_create(const ckks_batch_bucket* buckets, int n_bu
 extern "C" int ckks_batch_plan_run(ckks_batch_plan* p, long long wait_cycles, int flags, void* stream) {
   const char* fn = "ckks_batch_plan_run";
   CKKS_REQUIRE(p != nullptr, "%s: plan is NULL", fn);
-  CKKS_REQUIRE((flags & ~CKKS_BATCH_RUN_UNMET_WAIT) == 0, "%s: unknown flags 0x%x", fn, flags);
+  CKKS_REQUIRE((flags & ~(CKKS_BATCH_RUN_UNMET_WAIT | CKKS_BATCH_RUN_PHASED)) == 0, "%s: unknown flags 0x%x", fn,
+               flags);
   int dev = 0;
   cudaGetDevice(&dev);
   CKKS_REQUIRE(dev == p->device, "%s: plan of device %d, current device %d", fn, p->device, dev);
   cudaStream_t st = as_stream(stream);
   cudaError_t e = cudaMemsetAsync(p->mem, 0, p->zero_bytes, st);
   if (e != cudaSuccess) return ckks_set_error(CKKS_ECUDA, "%s: %s", fn, cudaGetErrorString(e));
-  if (p->n_slots == 0) return CKKS_OK;
+  if (p->n_units == 0) return CKKS_OK;
   int unmet = -1;
   if (flags & CKKS_BATCH_RUN_UNMET_WAIT) {
     for (int b = 0; b < p->n_buckets && unmet < 0; ++b)
@@ -584,7 +716,8 @@ extern "C" int ckks_batch_plan_run(ckks_batch_plan* p, long long wait_cycles, in
   }
   const long long limit = wait_cycles > 0 ? wait_cycles : 2147483647ll;
   ProfSpan span(CKKS_STAGE_BATCH, st);
-  return p->max_log_n == 13 ? pb_launch<13>(p, limit, unmet, st) : pb_launch<12>(p, limit, unmet, st);
+  const bool paired = (flags & CKKS_BATCH_RUN_PHASED) == 0;
+  return p->max_log_n == 13 ? pb_launch<13>(p, paired, limit, unmet, st) : pb_launch<12>(p, paired, limit, unmet, st);
 }
 
 extern "C" int ckks_batch_plan_incomplete(ckks_batch_plan* p, int* n_incomplete, uint8_t* bucket_complete) {
@@ -612,7 +745,7 @@ extern "C" int ckks_batch_plan_info(const ckks_batch_plan* p, long long* n_units
                                     int* smem_bytes, size_t* device_bytes) {
   CKKS_REQUIRE(p != nullptr, "ckks_batch_plan_info: plan is NULL");
   if (n_units) *n_units = p->n_units;
-  if (n_slots) *n_slots = p->n_slots;
+  if (n_slots) *n_slots = p->n_slots;  // the default (paired) list
   if (grid) *grid = p->grid;
   if (smem_bytes) *smem_bytes = p->smem;
   if (device_bytes) *device_bytes = p->mem_bytes;

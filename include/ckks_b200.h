@@ -11,9 +11,10 @@
  *    cudaStream_t passed as void* (NULL = legacy default stream).
  *  - All data pointers are DEVICE pointers owned by the caller; calls are
  *    stream-ordered and never synchronise the host.  Device memory is
- *    allocated only by ckks_ctx_create (tables) and, once per thread and
- *    device, by ckks_sample_dgauss (its CDF table); every other entry uses
- *    caller buffers.
+ *    allocated only by ckks_ctx_create (tables), once per thread and
+ *    device by ckks_sample_dgauss (its CDF table), once per context by the
+ *    first ckks_ntt_tc call (its matrix images) and by ckks_batch_plan_create
+ *    (the plan); every other entry uses caller buffers.
  *  - Polynomials are uint64 coefficient arrays, limb-major:
  *    [batch][poly][limb][N]; limb l of a call with prime_begin b uses the
  *    context prime b + l.  Values are canonical residues in [0, q).
@@ -130,7 +131,7 @@ int ckks_ctx_set_tuning(ckks_ctx* ctx, int param, int value);
 /*
  * Device-side status of the kernels that wait with a bounded spin (the
  * TMA-fed ct-mult tensor kernel on its copies, the tensor-core linear
- * layer on its MMA completions, the persistent batch kernel on its work
+ * layer and transform on their MMA completions, the persistent batch kernel on its work
  * queue's dependency counters): CKKS_ETIMEOUT (and the
  * count in ckks_last_error) when any such wait on the current device expired
  * since the last call, which leaves those outputs incomplete; CKKS_OK
@@ -731,9 +732,21 @@ int ckks_ct_mul_relin_rescale_noalloc(const ckks_ctx* ctx, uint64_t* out, const 
  * the kernel records it for ckks_device_status (CKKS_ETIMEOUT), stops every
  * CTA, and leaves the unfinished items incomplete.  Both calls of a run may
  * be captured into a CUDA graph (one memset node, one kernel node).  flags:
- * 0, or CKKS_BATCH_RUN_UNMET_WAIT (a test hook: the ModUp units of the first
- * ct x ct item wait for one tensor unit more than exist, so that wait ends
- * only by its limit).
+ * 0, CKKS_BATCH_RUN_PHASED (run the phased list instead of the paired one,
+ * below), and / or CKKS_BATCH_RUN_UNMET_WAIT (a test hook: the ModUp units of
+ * the first ct x ct item wait for one tensor unit more than exist, so that
+ * wait ends only by its limit).
+ *
+ * The plan holds two lists of the same units.  The paired list (the
+ * default): both ring sizes interleaved, N = 2^12 units two per slot, so the
+ * two halves of a CTA finish together before it takes its next slot.  The
+ * phased list: the N = 2^13 units first, one per whole-CTA slot, then every
+ * N = 2^12 unit in a half slot of its own, which each half of each CTA takes
+ * from a second ticket independently of the other half (its kernel is a
+ * separate build; on B200 it measured 1-3 % slower at lags 200-800, the cost
+ * of its larger register spills in the N = 2^13 units outweighing the
+ * decoupled halves).  ckks_batch_plan_info reports the paired list's slot
+ * count.
  *
  * ckks_batch_plan_incomplete synchronises the device and counts the items
  * of the last run whose output is not complete (bucket_complete, if not
@@ -744,7 +757,7 @@ int ckks_ct_mul_relin_rescale_noalloc(const ckks_ctx* ctx, uint64_t* out, const 
  * of the uneven-shape work list.
  */
 enum { CKKS_BATCH_CT_CT = 0, CKKS_BATCH_CT_PT = 1 };
-enum { CKKS_BATCH_RUN_UNMET_WAIT = 1 };
+enum { CKKS_BATCH_RUN_UNMET_WAIT = 1, CKKS_BATCH_RUN_PHASED = 2 };
 typedef struct ckks_batch_bucket {
   const ckks_ctx* ctx;
   int32_t op;
@@ -776,6 +789,13 @@ void ckks_batch_plan_destroy(ckks_batch_plan* plan);
  */
 int ckks_batch_schedule(int n_buckets, const int* op, const int* n_ct, const int* level, const int* log_n,
                         const double* cost, long long lag, uint32_t* slots, long long* n_slots);
+/* The phased list (CKKS_BATCH_RUN_PHASED) on the host alone: *n_whole
+ * whole-CTA slots of one N = 2^13 unit each (dependent stages `lag` units
+ * apart), then half slots of one N = 2^12 unit each (2 lag units apart); the
+ * slot format above, every second unit (0xFFFFFFFF, 0). */
+int ckks_batch_schedule_phased(int n_buckets, const int* op, const int* n_ct, const int* level, const int* log_n,
+                               const double* cost, long long lag, uint32_t* slots, long long* n_slots,
+                               long long* n_whole);
 
 /*
  * Per-kernel device timing (tracing).  When enabled, the multi-kernel entry

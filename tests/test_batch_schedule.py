@@ -142,3 +142,61 @@ def test_schedule_empty_and_refusals():
     l[0] = 1
     with pytest.raises(CkksError, match="level=1"):
         call(100)
+
+
+def _phased(ops, cts, lvls, costs, lag, log_ns):
+    from ckks_b200 import _lib
+    nb = len(ops)
+    total = sum(c * (2 * l + 3 if o == CT_CT else 2) for o, c, l in zip(ops, cts, lvls))
+    slots = np.zeros((max(1, total), 4), dtype=np.uint32)
+    n, whole = C.c_longlong(total), C.c_longlong(-1)
+    a = lambda v, t: np.ascontiguousarray(np.asarray(v, dtype=t))
+    o, c, l, g, w = (a(ops, np.int32), a(cts, np.int32), a(lvls, np.int32), a(log_ns, np.int32),
+                     a(costs, np.float64))
+    _lib.call("ckks_batch_schedule_phased", nb, o.ctypes.data, c.ctypes.data, l.ctypes.data, g.ctypes.data,
+              w.ctypes.data, lag, slots.ctypes.data, C.byref(n), C.byref(whole))
+    return slots[:n.value], whole.value, total
+
+
+@pytest.mark.parametrize("lag", [0, 5, 296])
+def test_phased_schedule(lag):
+    """The plan's default list: every unit once in a slot of its own, the
+    N = 2^13 units first (whole-CTA slots), then the N = 2^12 units (half
+    slots); within each phase every unit after its producers, and with ct x pt
+    filler to spare the dependent stages keep `lag` (whole) / 2 lag (half)
+    units of distance."""
+    rng = np.random.default_rng(2)
+    ops, cts, lvls, costs, logs = [], [], [], [], []
+    for op in (CT_CT, CT_PT):
+        for log_n in (12, 13):
+            for lvl in range(2, 9):
+                ops.append(op)
+                cts.append(int(rng.integers(0, 40)))
+                lvls.append(lvl)
+                logs.append(log_n)
+                costs.append(float((1 << log_n) * (2 * lvl + 3)))
+    slots, whole, total = _phased(ops, cts, lvls, costs, lag, logs)
+    assert len(slots) == total
+    assert all(int(x1) == NONE for x1 in slots[:, 2])
+    sizes = [logs[int(x) >> 8] for x in slots[:, 0]]
+    assert sizes == [13] * whole + [12] * (total - whole)
+    assert whole == sum(c * (2 * l + 3 if o == CT_CT else 2)
+                        for o, c, l, g in zip(ops, cts, lvls, logs) if g == 13)
+    pos = {}
+    for i, (x, y) in enumerate(zip(slots[:, 0].tolist(), slots[:, 1].tolist())):
+        key = (x >> 8, (x >> 6) & 3, x & 63, y)
+        assert key not in pos
+        pos[key] = i
+    gaps = []
+    for b, (o, c, l, g) in enumerate(zip(ops, cts, lvls, logs)):
+        if o != CT_CT:
+            continue
+        for it in range(c):
+            last_t = max(pos[(b, TENSOR, j, it)] for j in range(l))
+            mods = [pos[(b, MODUP, t, it)] for t in range(l + 1)]
+            downs = [pos[(b, DOWN, k, it)] for k in range(2)]
+            assert last_t < min(mods) and max(mods) < min(downs)
+            need = lag if g == 13 else 2 * lag
+            gaps += [min(mods) - last_t - 1 >= need, min(downs) - max(mods) - 1 >= need]
+    if lag:
+        assert sum(gaps) >= 0.8 * len(gaps)

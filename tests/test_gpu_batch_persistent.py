@@ -1,7 +1,8 @@
 """The persistent batch kernel (ckks_batch_plan_*): one launch drains a work
 list of mixed-N, mixed-level ct x ct and ct x pt work units with per-item
 dependency counters; N = 2^13 units take a whole 512-thread CTA, N = 2^12
-units run two side by side in its halves.  Its outputs are bit-identical to
+units run in its halves (phased list: each half takes its own units after
+the 2^13 phase; paired list: two per slot, side by side).  Both lists' outputs are bit-identical to
 the eager per-bucket path (integer results: tolerance zero) under every lag,
 for one ring size or both, inside a CUDA graph too; a wait that nothing
 satisfies ends at its limit with CKKS_ETIMEOUT and the unfinished items
@@ -59,15 +60,18 @@ def test_persistent_equals_eager_and_oracle(mixed):
                                 for b in ex.buckets)
     units13 = sum(b.count * ((2 * b.shape.level + 3) if b.shape.op == "ctct" else 2)
                   for b in ex.buckets if b.shape.log_n == 13)
-    # every 2^13 unit alone, the 2^12 units two by two (at most one alone)
-    assert info["slots"] - units13 == (info["units"] - units13 + 1) // 2
+    # paired list (the default): every 2^13 unit alone, the 2^12 units two by
+    # two (at most one alone); the phased list gives every unit its own slot
+    assert info["slots"] - units13 == (info["units"] - units13 + 1) // 2 and info["list"] == "paired"
     assert {b.shape.log_n for b in ex.buckets} == {12, 13}
-    _clear(ex)
-    plan.run()
-    torch.cuda.synchronize()
-    assert _lib.load().ckks_device_status() == 0
-    assert plan.incomplete() == (0, [True] * len(ex.buckets))
-    assert all(_same(ex, ref))
+    for paired in (True, False):
+        plan.paired = paired
+        _clear(ex)
+        plan.run()
+        torch.cuda.synchronize()
+        assert _lib.load().ckks_device_status() == 0
+        assert plan.incomplete() == (0, [True] * len(ex.buckets))
+        assert all(_same(ex, ref)), paired
     # the last item of a few buckets against the oracle
     for bk in [b for b in ex.buckets if b.count][::7]:
         ev = ex.evs[bk.shape.log_n]
@@ -86,15 +90,17 @@ def test_persistent_equals_eager_and_oracle(mixed):
     plan.close()
 
 
+@pytest.mark.parametrize("paired", [False, True])
 @pytest.mark.parametrize("lag", [0, 100, 10000])
-def test_persistent_any_lag_same_results(mixed, lag):
+def test_persistent_any_lag_same_results(mixed, lag, paired):
     """lag 0 lists each dependent stage right after its producers (most
     units wait), 10000 only after every other unit (the work list degenerates
-    to stage order): the same bits either way."""
+    to stage order): the same bits either way, on either unit list."""
     import torch
     from ckks_b200.batch import PersistentPlan
     ex, ref = mixed
     plan = PersistentPlan(ex.evs, ex.buckets, lag_percent=lag)
+    plan.paired = paired
     _clear(ex)
     plan.run()
     torch.cuda.synchronize()
@@ -131,11 +137,13 @@ def test_persistent_one_ring_size(cuda, log_n):
     ex, ref = _executor(64, seed=6 + log_n, log_ns=(log_n,))
     for lag in (0, 400):
         plan = PersistentPlan(ex.evs, ex.buckets, lag_percent=lag)
-        _clear(ex)
-        plan.run()
-        torch.cuda.synchronize()
-        assert plan.incomplete()[0] == 0
-        assert all(_same(ex, ref)), lag
+        for paired in (False, True):
+            plan.paired = paired
+            _clear(ex)
+            plan.run()
+            torch.cuda.synchronize()
+            assert plan.incomplete()[0] == 0
+            assert all(_same(ex, ref)), (lag, paired)
         plan.close()
 
 
