@@ -21,6 +21,7 @@ from .context import Context
 from .params import CkksParams
 
 U64 = torch.uint64
+KEYS_SCHEMA = 1  # version of the key checkpoint written by Evaluator.save_keys
 
 
 @dataclass
@@ -141,6 +142,52 @@ class Evaluator:
             self._scratch = torch.empty((need + 7) // 8, dtype=U64, device=self.device)
         r = ops.rotate(self.ctx, ct.data, gk, nu, scratch=self._scratch, out=out)
         return Ciphertext(r, ct.scale)
+
+    # ---------------------------------------------------------------- checkpoint
+    def save_keys(self, path) -> None:
+        """Write the key material to an .npz (schema KEYS_SCHEMA): the
+        parameter set (ring, primes, scale, sigma, seed), the sampler's stream
+        counter (so a resumed evaluator draws the same randomness next), the
+        ternary secret in the coefficient domain, the raw relinearisation key
+        and every raw Galois key.  Twiddle tables are not stored: a context is
+        a pure function of (N, primes) and is rebuilt on load."""
+        if self.sk is None:
+            raise ValueError("no keys to save: call keygen() first")
+        host = lambda t: t.contiguous().view(torch.int64).cpu().numpy()
+        P = self.params
+        rec = {"schema": np.int64(KEYS_SCHEMA), "log_n": np.int64(P.log_n),
+               "q": np.asarray(P.q, dtype=np.uint64), "special": np.uint64(P.special),
+               "scale": np.float64(P.scale), "sigma": np.float64(P.sigma), "seed": np.int64(P.seed),
+               "stream_id": np.int64(self._stream_id), "s_coef": host(self.sk.s_coef),
+               "ksk": host(self.ksk), "galois_nu": np.asarray(sorted(self.galois), dtype=np.int64)}
+        for nu in sorted(self.galois):
+            rec[f"galois_{nu}"] = host(self.galois[nu][0])
+        np.savez(path, **rec)
+
+    def load_keys(self, path) -> SecretKey:
+        """Restore what save_keys wrote into this evaluator (same parameter
+        set required): the secret, the relinearisation key and the Galois
+        keys (re-prepared on the device), and the sampler's stream counter."""
+        z = np.load(path)
+        if int(z["schema"]) != KEYS_SCHEMA:
+            raise ValueError(f"key checkpoint schema {int(z['schema'])}, expected {KEYS_SCHEMA}")
+        P = self.params
+        same = (int(z["log_n"]) == P.log_n and [int(x) for x in z["q"]] == list(P.q)
+                and int(z["special"]) == P.special and float(z["scale"]) == P.scale
+                and float(z["sigma"]) == P.sigma and int(z["seed"]) == P.seed)
+        if not same:
+            raise ValueError("key checkpoint was written for another parameter set")
+        dev = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(self.device)
+        s_coef = dev(z["s_coef"]).to(torch.int64)
+        self.sk = SecretKey(s_coef, self._int_poly_to_eval(s_coef, len(P.primes)))
+        self.ksk = dev(z["ksk"]).view(U64).contiguous()
+        self.rlk = ops.relin_key_prepare(self.ctx, self.ksk)
+        self.galois = {}
+        for nu in z["galois_nu"].tolist():
+            raw = dev(z[f"galois_{nu}"]).view(U64).contiguous()
+            self.galois[int(nu)] = (raw, ops.relin_key_prepare(self.ctx, raw))
+        self._stream_id = int(z["stream_id"])
+        return self.sk
 
     # ---------------------------------------------------------------- polynomials
     def drop_to(self, ct: Ciphertext, level: int) -> Ciphertext:

@@ -1,6 +1,7 @@
 // aux.cu - noise monitor reductions, slot SNR, block sparsity, RNS split /
 // merge and the energy-threshold gear controller.
 #include "dispatch.cuh"
+#include "profile.hpp"
 
 // ---------------------------------------------------------------- noise energy
 // Per row: exact 128-bit sum of min(c, q - c)^2 (rtl/m4/noise_monitor.sv:42-78).
@@ -44,6 +45,7 @@ __global__ void k_noise_energy(unsigned long long* __restrict__ out, const u64* 
 
 extern "C" int ckks_noise_energy(uint64_t* out_sum, const uint64_t* in, int n_rows, int row_len,
                                  uint64_t q, void* stream) {
+  ProfSpan span(CKKS_STAGE_OTHER, as_stream(stream), "ckks noise monitor");
   CKKS_REQUIRE(n_rows >= 0 && row_len >= 0, "ckks_noise_energy: negative size");
   CKKS_REQUIRE(q >= 2 && q < (1ull << 62), "ckks_noise_energy: q outside [2, 2^62)");
   if (n_rows == 0) return CKKS_OK;
@@ -166,6 +168,7 @@ __global__ void k_snr(double* __restrict__ out, const double* __restrict__ dec,
 
 extern "C" int ckks_snr_sums(double* out, const double* dec, const double* ref, int n_rows,
                              int row_len, int complex_vals, void* stream) {
+  ProfSpan span(CKKS_STAGE_OTHER, as_stream(stream), "ckks SNR probe sums");
   CKKS_REQUIRE(n_rows >= 0 && row_len >= 0, "ckks_snr_sums: negative size");
   if (n_rows == 0) return CKKS_OK;
   k_snr<<<grid1d(n_rows), 256, 0, as_stream(stream)>>>(out, dec, ref, row_len, complex_vals);

@@ -107,7 +107,7 @@ extern "C" int ckks_mul_plain_multi(const ckks_ctx* ctx, uint64_t* out, const ui
     auto kern = k_mul_plain_multi<L, K>;
     if (int rc = require_smem(S::SMEM_WORDS * 8, L, fn)) return rc;
     ensure_smem(kern, S::SMEM_WORDS * 8);
-    ProfSpan span(CKKS_STAGE_OTHER, st);
+    ProfSpan span(CKKS_STAGE_OTHER, st, "ckks conv + GAP: products per filter");
     kern<<<grid1d(2ll * n_ct), S::T, S::SMEM_WORDS * 8, st>>>(reinterpret_cast<u64*>(out),
                                                               reinterpret_cast<const u64*>(ct),
                                                               reinterpret_cast<const u64*>(w_hat), n_w,

@@ -766,7 +766,7 @@ extern "C" int ckks_rotate(const ckks_ctx* ctx, uint64_t* out, const uint64_t* c
     ensure_smem(kb, smem_b);
     ensure_smem(kc, smem_c);
     {
-      ProfSpan span(CKKS_STAGE_OTHER, st);
+      ProfSpan span(CKKS_STAGE_OTHER, st, "ckks rotation: automorphism + digits");
       const long long nu_a = (long long)n_ct * level;
       ka<<<grid1d((nu_a + upc - 1) / upc), Sh::T, smem_a, st>>>(reinterpret_cast<const u64*>(ct), S, level,
                                                                 nu2n, ctx->d_pi, ctx->d_tw, n_ct, nu_a, upc);

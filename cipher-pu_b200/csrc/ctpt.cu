@@ -46,7 +46,7 @@ extern "C" int ckks_ct_mul_plain_rescale(const ckks_ctx* ctx, uint64_t* out, con
     const int smem = (Sh::SMEM_WORDS + Sh::N) * 8;
     if (int rc = require_smem(smem, L, fn)) return rc;
     ensure_smem(k_ctpt_rescale<L, K>, smem);
-    ProfSpan span(CKKS_STAGE_OTHER, st);
+    ProfSpan span(CKKS_STAGE_OTHER, st, "ckks ct x pt + rescale");
     k_ctpt_rescale<L, K><<<grid1d(2ll * n_ct), Sh::T, smem, st>>>(
         reinterpret_cast<u64*>(out), reinterpret_cast<const u64*>(ct), reinterpret_cast<const u64*>(pt),
         pt_per_ct ? 1 : 0, level, ctx->d_pi, ctx->d_tw, ctx->d_qtinv, ctx->n_q);

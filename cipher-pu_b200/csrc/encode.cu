@@ -10,6 +10,7 @@
 //           V[k] = sum_j x_j Phi^j e^{+2 pi i jk / N}.
 // The FFT is an in-shared-memory radix-2 transform, one CTA per polynomial.
 #include "dispatch.cuh"
+#include "profile.hpp"
 
 struct cplx {
   double re, im;
@@ -194,6 +195,7 @@ static int dispatch_fft(int log_n, F&& f, const char* fn) {
 
 extern "C" int ckks_encode(const ckks_ctx* ctx, uint64_t* out, const double* slots, int n_polys,
                            int n_slots, int level, double scale, void* stream) {
+  ProfSpan span(CKKS_STAGE_OTHER, as_stream(stream), "ckks encode");
   const char* fn = "ckks_encode";
   CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
   CKKS_REQUIRE(n_slots >= 0 && n_slots <= ctx->n / 2, "%s: n_slots=%d outside [0, N/2]", fn, n_slots);
@@ -217,6 +219,7 @@ extern "C" int ckks_encode(const ckks_ctx* ctx, uint64_t* out, const double* slo
 
 extern "C" int ckks_decode(const ckks_ctx* ctx, double* slots, const uint64_t* in_coef, int n_polys,
                            int n_slots, int level, double scale, void* stream) {
+  ProfSpan span(CKKS_STAGE_OTHER, as_stream(stream), "ckks decode");
   const char* fn = "ckks_decode";
   CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
   CKKS_REQUIRE(n_slots >= 0 && n_slots <= ctx->n / 2, "%s: n_slots=%d outside [0, N/2]", fn, n_slots);
@@ -443,6 +446,7 @@ extern "C" int ckks_dare_refresh(const ckks_ctx* ctx, uint64_t* out, const uint6
                                  const uint64_t* s_eval, const uint64_t* a_fresh,
                                  const int64_t* e_fresh, int n_ct, int level_in, int level_out,
                                  int shift_bits, void* scratch, size_t scratch_bytes, void* stream) {
+  ProfSpan span(CKKS_STAGE_OTHER, as_stream(stream), "ckks DARE refresh");
   const char* fn = "ckks_dare_refresh";
   CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
   CKKS_REQUIRE(level_in >= 1 && level_in <= 16 && level_in <= ctx->n_primes,

@@ -16,6 +16,7 @@
 // input column block that no row block of the CTA keeps is never loaded, so
 // both the multiplies and the input traffic scale with the kept fraction.
 #include "dispatch.cuh"
+#include "profile.hpp"
 
 constexpr int LIN_ROWB = 8;                  // 4-row blocks per CTA (one per warp)
 constexpr int LIN_OT = 4 * LIN_ROWB;         // outputs per CTA
@@ -215,6 +216,7 @@ extern "C" int ckks_linear_plain_weights(const ckks_ctx* ctx, uint64_t* out, con
                                          const int32_t* w, const int64_t* bias,
                                          const uint8_t* block_keep, int n_out, int n_in, int level,
                                          void* stream) {
+  ProfSpan span(CKKS_STAGE_OTHER, as_stream(stream), "ckks linear layer (integer pipe)");
   const char* fn = "ckks_linear_plain_weights";
   CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
   CKKS_REQUIRE(n_in >= 1 && n_in <= LIN_MAX_IN, "%s: n_in=%d outside [1, %d]", fn, n_in, LIN_MAX_IN);

@@ -35,6 +35,7 @@
 #include "dispatch.cuh"
 #include "tmem.cuh"
 #include "umma.cuh"
+#include "profile.hpp"
 
 namespace {
 
@@ -331,6 +332,7 @@ int ckks_linear_tc_status_take(unsigned int* n) {
 extern "C" int ckks_linear_plain_weights_tc(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in,
                                             const void* packed, const int64_t* bias, int n_out, int n_in,
                                             int level, void* stream) {
+  ProfSpan span(CKKS_STAGE_OTHER, as_stream(stream), "ckks linear layer (tensor cores)");
   const char* fn = "ckks_linear_plain_weights_tc";
   CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
   CKKS_REQUIRE(n_in >= 1 && n_in <= TC_MAX_IN, "%s: n_in=%d outside [1, %d]", fn, n_in, TC_MAX_IN);

@@ -45,6 +45,7 @@
 #include "dispatch.cuh"
 #include "tmem.cuh"
 #include "umma.cuh"
+#include "profile.hpp"
 
 namespace {
 
@@ -334,6 +335,7 @@ int ckks_ntt_tc_status_take(unsigned int* n) {
 
 extern "C" int ckks_ntt_tc(ckks_ctx* ctx, uint64_t* data, int n_polys, int prime_begin, int n_limbs,
                            void* stream) {
+  ProfSpan span(CKKS_STAGE_OTHER, as_stream(stream), "ckks NTT (tensor cores)");
   const char* fn = "ckks_ntt_tc";
   CKKS_REQUIRE(ctx != nullptr, "%s: ctx is NULL", fn);
   CKKS_REQUIRE(ctx->log_n == 12, "%s: built for N = 2^12 only (context has N = 2^%d)", fn, ctx->log_n);

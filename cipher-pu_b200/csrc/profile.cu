@@ -7,6 +7,8 @@
 #include <unordered_map>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "profile.hpp"
 
 namespace {
@@ -38,7 +40,16 @@ cudaEvent_t take_event() {
 
 bool prof_on() { return g_on; }
 
-ProfSpan::ProfSpan(int stage, cudaStream_t s) : stage_(stage), s_(s) {
+// NVTX range names of the stages (index = stage id)
+const char* const kStageNames[CKKS_PROFILE_STAGES] = {
+    "ckks ct-mult: tensor product + d2 INTT", "ckks ct-mult: ModUp + key inner product",
+    "ckks ct-mult: ModDown + rescale",       "ckks NTT",
+    "ckks other",                            "ckks ct-mult: fused cluster kernel",
+    "ckks batch: persistent kernel",         "ckks stage 7"};
+
+ProfSpan::ProfSpan(int stage, cudaStream_t s, const char* nvtx_name) : stage_(stage), s_(s) {
+  nvtxRangePushA(nvtx_name ? nvtx_name
+                           : (stage >= 0 && stage < CKKS_PROFILE_STAGES ? kStageNames[stage] : "ckks"));
   if (!g_on) return;
   std::lock_guard<std::mutex> lk(g_mu);
   a_ = take_event();
@@ -48,10 +59,12 @@ ProfSpan::ProfSpan(int stage, cudaStream_t s) : stage_(stage), s_(s) {
 }
 
 ProfSpan::~ProfSpan() {
-  if (!active_) return;
-  std::lock_guard<std::mutex> lk(g_mu);
-  cudaEventRecord(b_, s_);
-  g_pending.push_back({stage_, a_, b_});
+  if (active_) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    cudaEventRecord(b_, s_);
+    g_pending.push_back({stage_, a_, b_});
+  }
+  nvtxRangePop();
 }
 
 extern "C" int ckks_profile_enable(int on) {

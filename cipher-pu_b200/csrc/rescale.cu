@@ -1,6 +1,7 @@
 // rescale.cu - the golden single-modulus rescales (exact and scaled) and the
 // RNS drop-last-limb rescale.
 #include "dispatch.cuh"
+#include "profile.hpp"
 
 // round(c * q_out / q_in) mod q_out, round half up (scripts/verify_rescale.py:38).
 __global__ void k_rescale_exact(u64* __restrict__ out, const u64* __restrict__ in, long long n,
@@ -110,6 +111,7 @@ __global__ void __launch_bounds__(NttShape<LOGN, K>::T)
 
 extern "C" int ckks_rescale_rns(const ckks_ctx* ctx, uint64_t* out, const uint64_t* in,
                                 int n_polys, int level, void* stream) {
+  ProfSpan span(CKKS_STAGE_OTHER, as_stream(stream), "ckks RNS rescale");
   CKKS_REQUIRE(ctx != nullptr, "ckks_rescale_rns: ctx is NULL");
   CKKS_REQUIRE(level >= 2 && level <= ctx->n_q, "ckks_rescale_rns: level=%d outside [2, %d]",
                level, ctx->n_q);
