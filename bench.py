@@ -72,6 +72,8 @@ def parse():
                     help="skip the decoded-slot error check of the ct-mult (real keys)")
     ap.add_argument("--no-e2e", action="store_true",
                     help="skip the host-buffer end-to-end legs (profiling runs)")
+    ap.add_argument("--jsonl", default=None,
+                    help="also append the JSON line, with a UTC timestamp and the command line, to this run log")
     ap.add_argument("--e2e-async-chunk", type=int, default=128,
                     help="pairs per pipeline chunk of the stream-ordered host-buffer calls (e2e)")
     ap.add_argument("--e2e-chunk", type=int, default=48,
@@ -87,6 +89,16 @@ def config(a) -> dict:
             "ct_mult_path": a.ct_mult_path,
             "l2": "inputs larger than L2: 4 distinct input batches rotate between steps",
             "parallelism": f"replicas x{max(1, a.gpus)} (ciphertext batch sharded, no collective)"}
+
+
+def emit(line: dict, a) -> None:
+    """Print the run's one JSON line; with --jsonl, also append it (plus the
+    time and command line) to a JSON-lines run log."""
+    print(json.dumps(line), flush=True)
+    if getattr(a, "jsonl", None):
+        rec = dict(line, logged_utc=time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()), argv=sys.argv[1:])
+        with open(a.jsonl, "a") as f:
+            f.write(json.dumps(rec) + "\n")
 
 
 def dist_env():
@@ -121,7 +133,7 @@ def run_reference(a) -> int:
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line), flush=True)
+    emit(line, a)
     return 0
 
 
@@ -1002,7 +1014,7 @@ def run_ours(a) -> int:
                                   f"unsplit ({launches_per_step:g} per step)",
             "clocks": clocks,
         }
-        print(json.dumps(line), flush=True)
+        emit(line, a)
     if ws > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
