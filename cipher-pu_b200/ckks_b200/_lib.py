@@ -27,6 +27,14 @@ class BatchBucket(C.Structure):
                 ("pt_per_ct", C.c_int32), ("a", _vp), ("b", _vp), ("out", _vp), ("key", _vp)]
 
 
+class CkksParamsC(C.Structure):
+    """ckks_params: the parameter set as one POD struct (ckks_ctx_create_params)."""
+    _fields_ = [("log_n", C.c_int32), ("n_primes", C.c_int32), ("n_special", C.c_int32),
+                ("reserved", C.c_int32), ("primes", C.POINTER(C.c_uint64)), ("psi", C.POINTER(C.c_uint64)),
+                ("omega", C.POINTER(C.c_uint64)), ("scale", C.c_double), ("sigma", C.c_double),
+                ("seed", C.c_uint64)]
+
+
 BATCH_CT_CT, BATCH_CT_PT = 0, 1
 BATCH_RUN_UNMET_WAIT = 1
 BATCH_RUN_PHASED = 2
@@ -35,6 +43,8 @@ BATCH_RUN_PHASED = 2
 SIGNATURES: dict[str, tuple] = {
     "ckks_abi_version": (_i32, []),
     "ckks_last_error": (C.c_char_p, []),
+    "ckks_ctx_create_params": (_i32, [C.POINTER(CkksParamsC), C.POINTER(_vp)]),
+    "ckks_ctx_get_params": (_i32, [_vp, C.POINTER(CkksParamsC)]),
     "ckks_ctx_create": (_i32, [_i32, _i32, _i32, C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64),
                                C.POINTER(_vp)]),
     "ckks_ctx_destroy": (_i32, [_vp]),

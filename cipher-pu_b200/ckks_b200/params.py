@@ -114,6 +114,18 @@ class CkksParams:
     def n(self) -> int:
         return 1 << self.log_n
 
+    def to_c(self):
+        """(ckks_params struct, the primes array it points to): the C mirror of
+        this set (all primes with the special one last; roots left to the
+        library, which derives them as this module does).  Keep the array
+        alive while the struct is used."""
+        import ctypes
+        from ._lib import CkksParamsC
+        arr = (ctypes.c_uint64 * len(self.primes))(*self.primes)
+        st = CkksParamsC(self.log_n, len(self.primes), 1, 0, arr, None, None, float(self.scale),
+                         float(self.sigma), int(self.seed))
+        return st, arr
+
     @property
     def levels(self) -> int:
         return len(self.q)

@@ -260,6 +260,84 @@ extern "C" int ckks_ctx_create(int log_n, int n_primes, int n_special, const uin
   return CKKS_OK;
 }
 
+namespace {
+// smallest generator of (Z/qZ)^* (q prime): q - 1 = 2^k m with m < 2^47, its
+// distinct prime factors by trial division, then the first g with
+// g^((q-1)/f) != 1 for every factor f
+u64 smallest_generator(u64 q) {
+  std::vector<u64> fs;
+  u64 m = q - 1;
+  for (u64 d = 2; d * d <= m; d += (d == 2 ? 1 : 2))
+    if (m % d == 0) {
+      fs.push_back(d);
+      while (m % d == 0) m /= d;
+    }
+  if (m > 1) fs.push_back(m);
+  for (u64 g = 2;; ++g) {
+    bool ok = true;
+    for (u64 f : fs) ok = ok && h_powmod(g, (q - 1) / f, q) != 1;
+    if (ok) return g;
+  }
+}
+}  // namespace
+
+extern "C" int ckks_ctx_create_params(const ckks_params* p, ckks_ctx** out) {
+  const char* fn = "ckks_ctx_create_params";
+  CKKS_REQUIRE(p != nullptr && out != nullptr, "%s: NULL argument", fn);
+  *out = nullptr;
+  CKKS_REQUIRE(p->reserved == 0, "%s: reserved field must be 0", fn);
+  CKKS_REQUIRE(p->log_n >= 1 && p->log_n <= 14, "%s: log_n=%d outside [1, 14]", fn, p->log_n);
+  CKKS_REQUIRE(p->n_primes >= 1 && p->n_primes <= 64, "%s: n_primes=%d outside [1, 64]", fn, p->n_primes);
+  CKKS_REQUIRE(p->primes != nullptr, "%s: primes is NULL", fn);
+  const u64 n = 1ull << p->log_n;
+  std::vector<uint64_t> psi(p->n_primes), om(p->n_primes);
+  for (int i = 0; i < p->n_primes; ++i) {
+    const u64 q = p->primes[i];
+    CKKS_REQUIRE(q >= 3 && q < (1ull << 47) && is_prime_u64(q), "%s: primes[%d]=%llu is not a prime in [3, 2^47)",
+                 fn, i, (unsigned long long)q);
+    CKKS_REQUIRE((q - 1) % n == 0, "%s: N=%llu does not divide primes[%d]-1", fn, (unsigned long long)n, i);
+    u64 g = 0;
+    if (p->psi && p->psi[i]) {
+      psi[i] = p->psi[i];
+    } else if ((q - 1) % (2 * n) == 0) {
+      g = smallest_generator(q);
+      psi[i] = h_powmod(g, (q - 1) / (2 * n), q);
+    } else {
+      psi[i] = 0;
+    }
+    if (p->omega && p->omega[i]) {
+      om[i] = p->omega[i];
+    } else if (psi[i]) {
+      om[i] = h_mulmod(psi[i], psi[i], q);
+    } else {
+      if (!g) g = smallest_generator(q);
+      om[i] = h_powmod(g, (q - 1) / n, q);
+    }
+  }
+  ckks_ctx* c = nullptr;
+  if (int rc = ckks_ctx_create(p->log_n, p->n_primes, p->n_special, p->primes, psi.data(), om.data(), &c)) return rc;
+  c->scale = p->scale;
+  c->sigma = p->sigma;
+  c->seed = p->seed;
+  *out = c;
+  return CKKS_OK;
+}
+
+extern "C" int ckks_ctx_get_params(const ckks_ctx* ctx, ckks_params* out) {
+  CKKS_REQUIRE(ctx != nullptr && out != nullptr, "ckks_ctx_get_params: NULL argument");
+  out->log_n = ctx->log_n;
+  out->n_primes = ctx->n_primes;
+  out->n_special = ctx->n_special;
+  out->reserved = 0;
+  out->primes = reinterpret_cast<const uint64_t*>(ctx->primes.data());
+  out->psi = reinterpret_cast<const uint64_t*>(ctx->psi.data());
+  out->omega = reinterpret_cast<const uint64_t*>(ctx->omega.data());
+  out->scale = ctx->scale;
+  out->sigma = ctx->sigma;
+  out->seed = ctx->seed;
+  return CKKS_OK;
+}
+
 extern "C" int ckks_ctx_destroy(ckks_ctx* ctx) {
   free_ctx(ctx);
   return CKKS_OK;

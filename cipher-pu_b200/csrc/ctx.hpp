@@ -34,6 +34,8 @@ struct ckks_ctx {
   TwPair* d_qtinv = nullptr;  // [n_q][n_q]: q_t^-1 mod q_i at [t][i], i < t
   TwPair* d_misc = nullptr;   // [n_primes][4]: (1, one_s) helpers; slot 1: R mod q
   unsigned char* d_ntt_tc = nullptr;  // tensor-core transform tables (ntt_tc.cu), built on first use
+  double scale = 0.0, sigma = 0.0;  // scheme constants of ckks_ctx_create_params (not read by kernels)
+  u64 seed = 0;
   std::vector<std::vector<u64>> h_qtinv;  // host copies
   std::vector<u64> h_pinv;
 };

@@ -65,6 +65,36 @@ int ckks_ctx_create(int log_n, int n_primes, int n_special, const uint64_t* prim
 int ckks_ctx_destroy(ckks_ctx* ctx);
 
 /*
+ * The parameter set as one plain struct (the C mirror of the Python
+ * CkksParams): ring, primes (the last n_special special), optional roots
+ * (NULL or 0 entries: derived as g^((q-1)/2N), resp. psi^2 or g^((q-1)/N),
+ * with g the smallest generator of (Z/qZ)^*, exactly as the Python side
+ * derives them), and the scheme constants a caller keeps with its keys
+ * (scale Delta, error width sigma, sampler seed; the context stores them
+ * and ckks_ctx_get_params returns them, the kernels do not read them).
+ * ckks_ctx_create_params is ckks_ctx_create from such a struct.
+ * ckks_ctx_get_params fills *out from a context; its pointers point into
+ * the context and stay valid while it lives.
+ * Replaces the parameter constants spread over scripts/gen_modulus_chain.py
+ * (argparse, :229-238), the rtl/m1/ntt_unit.sv:39-52 module parameters and
+ * the chain JSON rtl/m2/modulus_chain_chain4.json.
+ */
+typedef struct ckks_params {
+  int32_t log_n;
+  int32_t n_primes;
+  int32_t n_special;
+  int32_t reserved;  /* 0 */
+  const uint64_t* primes;
+  const uint64_t* psi;    /* NULL: derived */
+  const uint64_t* omega;  /* NULL: derived */
+  double scale;
+  double sigma;
+  uint64_t seed;
+} ckks_params;
+int ckks_ctx_create_params(const ckks_params* params, ckks_ctx** out);
+int ckks_ctx_get_params(const ckks_ctx* ctx, ckks_params* out);
+
+/*
  * Launch-shape tuning of a context (used by the autotuner).  Parameters:
  *   CKKS_TUNE_CM_LOG_ELEMS: coefficients per thread of the ct-mult and
  *   rotation kernels as log2 K (radix-2^K register passes with N / 2^K

@@ -45,3 +45,27 @@ def test_error_channel_without_gpu():
     rc = lib.ckks_rescale_exact(None, None, -1, 5, 3, None)
     assert rc == 1
     assert b"n < 0" in lib.ckks_last_error()
+
+
+def test_params_struct_layout_matches_header(tmp_path):
+    """The ctypes mirror of ckks_params has the C struct's size and field
+    offsets (a C program built against include/ckks_b200.h prints them)."""
+    import ctypes
+    import shutil
+    import subprocess
+    from pathlib import Path
+    from ckks_b200._lib import CkksParamsC
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    inc = Path(__file__).resolve().parents[1] / "include"
+    fields = [f for f, _ in CkksParamsC._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "ckks_b200.h"\nint main(void) {\n'
+                   '  printf("%zu", sizeof(ckks_params));\n'
+                   + "".join(f'  printf(" %zu", offsetof(ckks_params, {f}));\n' for f in fields)
+                   + '  printf("\\n");\n  return 0;\n}\n')
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", str(inc), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()]
+    assert got == [ctypes.sizeof(CkksParamsC)] + [getattr(CkksParamsC, f).offset for f in fields]
