@@ -915,6 +915,9 @@ def run_ours(a) -> int:
                         "speedup": r["speedup"], "snr_db_plain": r["plain"]["snr_db"],
                         "snr_db_learned": r["learned"]["snr_db"], "snr_gap_db": r["snr_gap_db"],
                         "top1_plain": r["plain"]["top1_agreement"], "top1_learned": r["learned"]["top1_agreement"],
+                        "decoded_vs_fp64": {arm: {"max_abs_err": r[arm]["max_abs_err"],
+                                                  "max_rel_err": r[arm]["max_rel_err"]}
+                                            for arm in ("plain", "learned")},
                         "probes_plain": r["plain"]["probes"], "probes_learned": r["learned"]["probes"],
                         "recomputed_layers_plain": r["plain"]["recomputed_layers"],
                         "recomputed_layers_learned": r["learned"]["recomputed_layers"],

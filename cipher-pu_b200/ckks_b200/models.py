@@ -84,6 +84,7 @@ def run_stream(m: EncryptedMLP, ctrl, batches: list, ref_layers: list | None = N
     recomputed = 0
     t_total = 0.0
     per_batch_snr = []
+    max_abs = max_ref = 0.0
     for x in batches:
         X = m.encrypt_inputs(x)
         torch.cuda.synchronize()
@@ -97,6 +98,8 @@ def run_stream(m: EncryptedMLP, ctrl, batches: list, ref_layers: list | None = N
         sig += s
         err += e
         per_batch_snr.append(10 * math.log10(s / max(e, 1e-300)))
+        max_abs = max(max_abs, float(np.abs(d - ref).max()))
+        max_ref = max(max_ref, float(np.abs(ref).max()))
         agree += int((d.argmax(1) == ref.argmax(1)).sum())
         total += len(x)
         gears.append(r["gears"])
@@ -108,4 +111,7 @@ def run_stream(m: EncryptedMLP, ctrl, batches: list, ref_layers: list | None = N
             "snr_db": 10 * math.log10(sig / max(err, 1e-300)), "top1_agreement": agree / total,
             "probes": getattr(ctrl, "probes", None), "recomputed_layers": recomputed, "gears": gears,
             "attempted_gears": attempted,
-            "min_batch_snr_db": min(per_batch_snr)}
+            "min_batch_snr_db": min(per_batch_snr),
+            # decoded logits against the FP64 plaintext model: max abs error and
+            # the normwise relative error max |d - ref| / max |ref|
+            "max_abs_err": max_abs, "max_rel_err": max_abs / max(max_ref, 1e-300)}
