@@ -55,9 +55,9 @@ __device__ __forceinline__ void cm_modup_unit_tm(const CmScratch& S, const doubl
   for (int j = 0; j < level; ++j) {
     {
       // bring the first key polynomial's limb for this digit toward L1 while
-      // the digit is transformed (both polynomials' limbs, 3 CTAs x 64 KB,
+      // the digit is transformed (both polynomials' limbs here, 3 CTAs x 64 KB,
       // would not fit the L1 left beside the shared memory: measured +1-1.6 %
-      // for the first alone, +0.7-1 % for both)
+      // for the first alone, +0.7-1 % for both; the second follows below)
       const double* kp = key + ((size_t)j * 2 * (nq + 1) + pidx) * (2 * N);
 #pragma unroll
       for (int e = 0; e < E; ++e) asm volatile("prefetch.global.L1 [%0];" ::"l"(kp + posC<LOGN, K>(tid, e)));
@@ -79,6 +79,14 @@ __device__ __forceinline__ void cm_modup_unit_tm(const CmScratch& S, const doubl
 #pragma unroll 1
     for (int kk = 0; kk < 2; ++kk) {
       const double* kp = key + (((size_t)j * 2 + kk) * (nq + 1) + pidx) * (2 * N);
+      if (kk == 0) {
+        // and the second polynomial's limb while the first one's products run
+        // (by then the first limb's lines are in use; both at the digit's
+        // start would not fit the L1 beside the shared memory)
+        const double* kp1 = kp + (size_t)(nq + 1) * (2 * N);
+#pragma unroll
+        for (int e = 0; e < E; ++e) asm volatile("prefetch.global.L1 [%0];" ::"l"(kp1 + posC<LOGN, K>(tid, e)));
+      }
 #pragma unroll
       for (int c = 0; c < E / 8; ++c) {
         const uint32_t addr = ta + (uint32_t)(kk * 2 * E + 16 * c);
