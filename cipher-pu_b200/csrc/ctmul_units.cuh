@@ -194,6 +194,20 @@ __device__ __forceinline__ void cm_down_unit(const CmScratch& S, u64* __restrict
 
   double d[Sh::E];
   u64 x[Sh::E];
+  // d_k's limbs (read after this unit's first transform) toward L2 now: the
+  // tensor kernel wrote them long before and, with four sub-batches in
+  // flight, they may have left L2 (measured +0.4 % on the whole step at
+  // N = 2^12, L = 3; prefetching the accumulators as well lost 0.3 %).  The
+  // per-shape kernel only: in the persistent batch kernel (COH) the loop
+  // costs registers that its N = 2^13 units spill.
+  if constexpr (!COH) {
+#pragma unroll 1
+    for (int i = 0; i <= t; ++i) {
+#pragma unroll
+      for (int e = 0; e < Sh::E; ++e)
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(dk + (size_t)i * N + posC<LOGN, K>(tid, e)));
+    }
+  }
   load_sc<LOGN, K, COH>(x, S.accp + (ct * 2 + k) * N, tid);
 #pragma unroll
   for (int e = 0; e < Sh::E; ++e) d[e] = u2d(x[e]);
